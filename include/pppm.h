@@ -1,0 +1,205 @@
+/*
+ * pppm.h — C ABI of the B200 (sm_100a) PPPM vortex-particle velocity
+ * evaluation.
+ *
+ * It replaces the reference's hot path, BiotSavartSolver::computeFarFieldBuffer
+ * followed by BiotSavartSolver::evaluateVelocity, together with the spatial
+ * hash and the multigrid solver underneath it.  Reference files are cited by
+ * their path inside the reference project (HFS = hybridFastSummation/
+ * hybridFastSummation, MG = multigrid/multigrid, PH = particle_hash/
+ * particle_hash).
+ *
+ * Conventions
+ *   - Every function returns a pppm_status; pppm_last_error() describes the
+ *     last failure on the calling thread.  (The reference returns bool true
+ *     and exits the process on CUDA errors through helper_cuda.)
+ *   - Pointers named *_dev are CUDA device pointers; *_host are host pointers.
+ *     Positions are float4 records (x, y, z, w; w ignored), four floats each.
+ *     Strengths and velocities are double arrays, one per component, as the
+ *     reference's GpuArrayd buffers.
+ *   - All work is enqueued on the scene's stream (cudaStream_t passed as
+ *     void*; NULL = the legacy default stream).  Calls on different scenes are
+ *     independent; one scene must not be used from two threads at once.
+ *   - Grids are cubic, n^3 cells, x-fastest ((k*n + j)*n + i), as the
+ *     reference's hash and multigrid assume.
+ */
+#ifndef PPPM_H
+#define PPPM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum pppm_status {
+    PPPM_OK = 0,
+    PPPM_ERR_INVALID = 1,   /* bad argument (NULL, size, capacity, mode)     */
+    PPPM_ERR_CUDA = 2,      /* CUDA runtime error                            */
+    PPPM_ERR_OOM = 3,       /* device allocation failed                      */
+    PPPM_ERR_STATE = 4,     /* call out of order (e.g. eval before far field) */
+    PPPM_ERR_DOMAIN = 5     /* degenerate domain (zero or non-finite extent) */
+} pppm_status;
+
+/* Domain selection.  BBOX3X is the reference's rule: edge L = 3 * largest
+ * extent of the vortex bounding box, centred on the box
+ * (HFS/BiotSavartSolverImp.cpp:379-409).  FIXED uses fixed_origin and
+ * fixed_length. */
+enum { PPPM_DOMAIN_BBOX3X = 0, PPPM_DOMAIN_FIXED = 1 };
+
+/* Poisson solve.  REFERENCE runs the reference schedule — full multigrid then
+ * one V(4,4) cycle, red-black SOR with omega = 1.43f, zero ghost values, 100
+ * Jacobi sweeps on the coarsest level (MG/MultiGrid.cpp:128-250) — in FP32,
+ * with the final V-cycle applied as an FP64 defect correction (FP64
+ * residual, FP64 accumulation of psi).  CONVERGED repeats FP64
+ * defect-correction V-cycles until ||b - A psi|| <= mg_tol * ||b||. */
+enum { PPPM_MG_REFERENCE = 0, PPPM_MG_CONVERGED = 1 };
+
+typedef struct pppm_params {
+    uint32_t n;              /* grid edge (gdx == gdy == gdz), 4..512            */
+    int32_t K;               /* near-field range in cells (m_K), -1..4; <0 = off */
+    double a;                /* smoothing radius, absolute (0.08 in the reference,
+                                HFS/GPU_kernel.cu:2306)                           */
+    int32_t domain_mode;     /* PPPM_DOMAIN_*                                     */
+    double fixed_origin[3];
+    double fixed_length;
+    int32_t mg_mode;         /* PPPM_MG_*                                         */
+    double mg_tol;           /* relative residual target for CONVERGED            */
+    int32_t mg_max_cycles;   /* cap on defect-correction cycles                   */
+} pppm_params;
+
+typedef struct pppm_scene pppm_scene;
+
+/* Grids exposed for inspection (device pointers owned by the scene). */
+enum {
+    PPPM_GRID_VORT = 0,      /* float [3][n^3]: P2M result sum(alpha)/h^3        */
+    PPPM_GRID_PSI = 1,       /* double [3][n^3]: vector potential                */
+    PPPM_GRID_FAR = 2        /* float [3][n^3]: far-field velocity               */
+};
+
+const char *pppm_last_error(void);
+const char *pppm_version(void);
+
+/* Defaults = the reference's constants: K = 1, a = 0.08, BBOX3X,
+ * PPPM_MG_REFERENCE, mg_tol 1e-10, 50 cycles; n must still be set. */
+pppm_status pppm_params_default(pppm_params *p);
+
+/* BiotSavartSolver::initializeSolver (HFS/BiotSavartSolverImp.cpp:44-229):
+ * allocates every buffer for up to cap_vort vortices and cap_eval evaluation
+ * points; later calls allocate only if a count exceeds its capacity. */
+pppm_status pppm_scene_create(const pppm_params *p, uint32_t cap_vort, uint32_t cap_eval,
+                              void *stream, pppm_scene **out);
+/* BiotSavartSolver::shutdown (HFS/BiotSavartSolverImp.cpp:230-264). */
+pppm_status pppm_scene_destroy(pppm_scene *s);
+pppm_status pppm_scene_set_stream(pppm_scene *s, void *stream);
+pppm_status pppm_scene_get_params(const pppm_scene *s, pppm_params *p);
+
+/* BiotSavartSolver::setVortParameter (HFS/BiotSavartSolverImp.cpp:318-377):
+ * copies N float4 positions and three double strength arrays (device). */
+pppm_status pppm_set_vortices(pppm_scene *s, uint32_t N, const float *pos4_dev,
+                              const double *ax_dev, const double *ay_dev, const double *az_dev);
+
+/* BiotSavartSolver::computeFarFieldBuffer (HFS/BiotSavartSolverImp.cpp:756-816):
+ * bounding box, hash + sort + cell tables + reorder, P2M, Poisson solve of the
+ * three potential components, curl, far-field correction. */
+pppm_status pppm_build_far_field(pppm_scene *s);
+
+/* BiotSavartSolver::setEvalParameter + evaluateVelocity
+ * (HFS/BiotSavartSolverImp.cpp:266-316, 410-516): far field interpolated at
+ * eval_a plus the near-field smoothed Biot-Savart correction; with
+ * is_segment = 1, vortices coinciding with eval_b (the segment's other end)
+ * are excluded.  Writes velocities in the caller's order.  eval_b may be NULL
+ * when is_segment = 0. */
+pppm_status pppm_eval(pppm_scene *s, uint32_t M, const float *eval_a4_dev,
+                      const float *eval_b4_dev, int is_segment,
+                      double *u_dev, double *v_dev, double *w_dev);
+
+/* Same evaluation with float output, interleaved (M x 3). */
+pppm_status pppm_eval_f32(pppm_scene *s, uint32_t M, const float *eval_a4_dev,
+                          const float *eval_b4_dev, int is_segment, float *uvw_dev);
+
+/* End-to-end on host buffers: copies the inputs to the device, runs
+ * set_vortices + build_far_field + eval, copies velocities back, and
+ * synchronises the stream.  eval_a4_host = NULL evaluates at the vortex
+ * positions with is_segment = 1 against themselves (each vortex excludes
+ * itself), the way the reference drives a velocity evaluation of its own
+ * particles. */
+pppm_status pppm_solve_host(pppm_scene *s, uint32_t N, const float *pos4_host,
+                            const double *ax_host, const double *ay_host, const double *az_host,
+                            uint32_t M, const float *eval_a4_host, const float *eval_b4_host,
+                            int is_segment, double *u_host, double *v_host, double *w_host);
+
+/* Accessors matching BiotSavartSolver::getOrigin / getCellh
+ * (HFS/BiotSavartSolver.h:34-35); synchronises the stream. */
+pppm_status pppm_get_domain(pppm_scene *s, double origin[3], double *length, double *cell_h);
+/* getVortStartTable / getVortEndTable (HFS/BiotSavartSolver.h:28-29): device
+ * pointers to n^3 uint32 tables (empty cells hold 0xFFFFFFFF in both). */
+pppm_status pppm_get_cell_tables(pppm_scene *s, const uint32_t **start_dev,
+                                 const uint32_t **end_dev);
+/* Sorted order of the vortices (ParticleManager's gridParticleIndex and
+ * gridParticleHash, PH/SpaceHashClass.h:87-89): device pointers, N entries. */
+pppm_status pppm_get_sorted_index(pppm_scene *s, const uint32_t **key_dev,
+                                  const uint32_t **idx_dev);
+/* getSortPos / getSortVort (HFS/BiotSavartSolver.h:25,27): gathers the
+ * vortex positions and double strengths into sorted order. */
+pppm_status pppm_get_sorted_vortices(pppm_scene *s, float *pos4_dev, double *ax_dev,
+                                     double *ay_dev, double *az_dev);
+pppm_status pppm_get_grid(pppm_scene *s, int which, const void **ptr_dev);
+/* Near-field pairs inside the axis box at the last eval with pair counting
+ * on, multigrid cycles and final relative residual of the last solve. */
+pppm_status pppm_get_stats(pppm_scene *s, uint64_t *pairs, int32_t *mg_cycles,
+                           double *mg_relres);
+/* Re-runs the last eval with pair counting on (diagnostics; not timed). */
+pppm_status pppm_count_pairs(pppm_scene *s, uint32_t M, const float *eval_a4_dev,
+                             uint64_t *pairs);
+
+/* ---- multigrid surface: gf::MultiGridSolver3DPeriod_double
+ * (MG/MultiGrid.h:188-209, MG/MultiGrid.cpp:128-250) ---------------------- */
+typedef struct pppm_mg pppm_mg;
+/* m_InitialSystem(n, n, n). */
+pppm_status pppm_mg_create(uint32_t n, void *stream, pppm_mg **out);
+pppm_status pppm_mg_destroy(pppm_mg *mg);
+/* m_FullMultiGrid(x, b, tol, residual) on FP64 device arrays of n^3: solves
+ * sum_nbr(x) - 6x = b with zero ghost values.  mode = PPPM_MG_REFERENCE runs
+ * the reference schedule (tol ignored, as in the reference); CONVERGED adds
+ * defect-correction cycles until the relative residual meets tol.
+ * *relres (may be NULL) receives ||b - A x|| / ||b||. */
+pppm_status pppm_mg_full_multigrid(pppm_mg *mg, double *x_dev, const double *b_dev,
+                                   int mode, double tol, int max_cycles, double *relres);
+
+/* ---- spatial hash surface: ParticleManager (PH/SpaceHashClass.h:10-84) and
+ * the extern "C" calcHash / sortParticles / FindCellStart / reorder / deorder
+ * of PH/SpaceHashHeader.cuh:12-47 ------------------------------------------ */
+typedef struct pppm_hasher pppm_hasher;
+/* initSpatialHash(numParticles, n, n, n). */
+pppm_status pppm_hasher_create(uint32_t cap_particles, uint32_t n, void *stream,
+                               pppm_hasher **out);
+pppm_status pppm_hasher_destroy(pppm_hasher *h);
+/* setSpatialHashGrid(n, h, origin) + doSpatialHash(pos, N): cell key
+ * floor((p - origin)/h) in FP32 per axis, wrapped mod n, stable sort of
+ * (key, index), cell start/end tables. */
+pppm_status pppm_hasher_run(pppm_hasher *h, uint32_t N, const float *pos4_dev, float cell_h,
+                            const float origin[3]);
+pppm_status pppm_hasher_tables(pppm_hasher *h, const uint32_t **key_dev, const uint32_t **idx_dev,
+                               const uint32_t **start_dev, const uint32_t **end_dev);
+/* reorderData / deorderData (PH/SpaceHashClassImp.cpp:24-34): gather
+ * out[i] = in[idx[i]] or scatter out[idx[i]] = in[i] of `stride` elements of
+ * 4 bytes (precision 1) or 8 bytes (precision 2) each. */
+pppm_status pppm_hasher_reorder(pppm_hasher *h, uint32_t N, const void *in_dev, void *out_dev,
+                                uint32_t stride, uint32_t precision);
+pppm_status pppm_hasher_deorder(pppm_hasher *h, uint32_t N, const void *in_dev, void *out_dev,
+                                uint32_t stride, uint32_t precision);
+
+/* ---- FP64 O(N*M) direct sum with the near field's smoothing kernel ------
+ * (accuracy ground truth; no reference counterpart) */
+pppm_status pppm_direct_sum_fp64(uint32_t N, const float *vort_pos4_dev, const double *ax_dev,
+                                 const double *ay_dev, const double *az_dev, uint32_t M,
+                                 const float *eval_a4_dev, const float *eval_b4_dev, int is_segment,
+                                 double a, double *u_dev, double *v_dev, double *w_dev,
+                                 void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,771 @@
+/*
+ * CPU oracle for the PPPM vortex-particle velocity evaluation — TEST
+ * INFRASTRUCTURE ONLY (see pppm_oracle.h for scope and pinning status).
+ *
+ * Build: oracle/Makefile (g++ -O3 -fopenmp -ffp-contract=off).  FP contraction
+ * is off so every expression rounds exactly as written here; where the
+ * reference mixes float and double the casts below reproduce its promotions.
+ */
+#include "pppm_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <numeric>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+struct F4 { float x, y, z, w; };
+
+inline const F4 *as_f4(const float *p) { return reinterpret_cast<const F4 *>(p); }
+
+/* __umul24: product of the low 24 bits of each operand (low 32 bits kept). */
+inline uint32_t umul24(uint32_t a, uint32_t b) {
+    return (uint32_t)((uint64_t)(a & 0xFFFFFFu) * (uint64_t)(b & 0xFFFFFFu));
+}
+
+/* The reference keeps the MG relaxation weight as the float literal 1.43f
+ * (MG/MultiGrid_kernel.cu:36) and forms (1-omega) in float before promoting. */
+const double kOmega = (double)1.43f;
+const double kOneMinusOmega = (double)(1.0f - 1.43f);
+/* Literal 4*pi of HFS/GPU_kernel.cu:12,2397,2403. */
+const double kFourPi = 12.5663706144;
+/* Diagonal self-potential factor of HFS/GPU_kernel.cu:1990-1992. */
+const double kDiagPsi = 0.250580605913965;
+
+inline size_t gidx(int i, int j, int k, int d) { return ((size_t)k * d + j) * d + i; }
+
+}  // namespace
+
+extern "C" int orc_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+/* HFS/BiotSavartSolverImp.cpp:379-409 (setDomain).  The min/max use an
+ * else-if, which is equivalent to independent min and max because min <= max
+ * holds from the first sample on. */
+extern "C" void orc_set_domain(const float *pos4, uint32_t N, double *origin3, double *length) {
+    const F4 *pos = as_f4(pos4);
+    double maxx, minx, maxy, miny, maxz, minz;
+    maxx = minx = pos[0].x;
+    maxy = miny = pos[0].y;
+    maxz = minz = pos[0].z;
+    for (uint32_t i = 1; i < N; i++) {
+        if (pos[i].x < minx) minx = pos[i].x; else if (pos[i].x > maxx) maxx = pos[i].x;
+        if (pos[i].y < miny) miny = pos[i].y; else if (pos[i].y > maxy) maxy = pos[i].y;
+        if (pos[i].z < minz) minz = pos[i].z; else if (pos[i].z > maxz) maxz = pos[i].z;
+    }
+    double L = 3 * std::max(std::max(maxx - minx, maxy - miny), maxz - minz);
+    double cx = minx + 0.5 * (maxx - minx);
+    double cy = miny + 0.5 * (maxy - miny);
+    double cz = minz + 0.5 * (maxz - minz);
+    origin3[0] = cx - 0.5 * L;
+    origin3[1] = cy - 0.5 * L;
+    origin3[2] = cz - 0.5 * L;
+    *length = L;
+}
+
+/* PH/particle_hash_kernel.cu:32-70 (calcGridPos, calcGridHash, calcHashD).
+ * Cell coordinate = floor((p - origin_f) / h_f) in FP32 with IEEE division;
+ * the int % uint wrap turns negatives into large unsigned values. */
+extern "C" void orc_calc_hash(const float *pos4, uint32_t N, uint32_t n, float h_f,
+                              const float *origin_f3, uint32_t *key, uint32_t *idx) {
+    const F4 *pos = as_f4(pos4);
+    const float ox = origin_f3[0], oy = origin_f3[1], oz = origin_f3[2];
+#pragma omp parallel for schedule(static)
+    for (int64_t t = 0; t < (int64_t)N; t++) {
+        volatile float px = pos[t].x, py = pos[t].y, pz = pos[t].z;
+        float fx = (px - ox) / h_f;
+        float fy = (py - oy) / h_f;
+        float fz = (pz - oz) / h_f;
+        int gx = (int)std::floor(fx);
+        int gy = (int)std::floor(fy);
+        int gz = (int)std::floor(fz);
+        uint32_t ux = (uint32_t)gx % n, uy = (uint32_t)gy % n, uz = (uint32_t)gz % n;
+        key[t] = umul24(umul24(uz, n), n) + umul24(uy, n) + ux;
+        idx[t] = (uint32_t)t;
+    }
+}
+
+/* PH/SpaceHashFunctional.cu:97-102: thrust::sort_by_key, a stable radix sort.
+ * A stable sort on the key reproduces its order. */
+extern "C" void orc_sort_by_key(uint32_t *key, uint32_t *idx, uint32_t N) {
+    std::vector<uint32_t> perm(N);
+    std::iota(perm.begin(), perm.end(), 0u);
+    std::stable_sort(perm.begin(), perm.end(),
+                     [&](uint32_t a, uint32_t b) { return key[a] < key[b]; });
+    std::vector<uint32_t> k2(N), i2(N);
+    for (uint32_t t = 0; t < N; t++) { k2[t] = key[perm[t]]; i2[t] = idx[perm[t]]; }
+    std::memcpy(key, k2.data(), sizeof(uint32_t) * N);
+    std::memcpy(idx, i2.data(), sizeof(uint32_t) * N);
+}
+
+/* PH/SpaceHashFunctional.cu:71-94 + PH/particle_hash_kernel.cu:74-126.
+ * Empty cells: start = 0xFFFFFFFF (the memset of :82).  The reference leaves
+ * cellEnd of empty cells stale; this restatement writes 0xFFFFFFFF there too. */
+extern "C" void orc_find_cell_start(const uint32_t *skey, uint32_t N, uint32_t ncells,
+                                    uint32_t *start, uint32_t *end) {
+    std::fill(start, start + ncells, 0xFFFFFFFFu);
+    std::fill(end, end + ncells, 0xFFFFFFFFu);
+    for (uint32_t t = 0; t < N; t++) {
+        uint32_t h = skey[t];
+        if (t == 0 || h != skey[t - 1]) {
+            if (h < ncells) start[h] = t;
+            if (t > 0 && skey[t - 1] < ncells) end[skey[t - 1]] = t;
+        }
+        if (t == N - 1 && h < ncells) end[h] = t + 1;
+    }
+}
+
+/* HFS/GPU_kernel.cu:218-294 (ParticleToMesh_kernel) with the NGP box weight
+ * shape_function_mass (HFS/GPU_kernel.cu:31-50).  The reference gathers, per
+ * grid cell, over the 5^3 hash cells around it in (kk, jj, ii) lexicographic
+ * order and then in sorted particle order; that is the global sorted order
+ * restricted to the window, so scattering each sorted particle to the cells
+ * where its weight is 1 accumulates in exactly the reference's order. */
+extern "C" void orc_p2m(const uint32_t *start, const uint32_t *end, const float *spos4,
+                        const double *smass, double cell_h, uint32_t n, uint32_t N,
+                        const double *origin3, double *grid) {
+    const F4 *pos = as_f4(spos4);
+    const double invh = 1.0 / cell_h;
+    const int d = (int)n;
+    std::vector<double> sum((size_t)d * d * d, 0.0);
+    /* Walk hash cells in key order (the reference's window order). */
+    for (int kk = 0; kk < d; kk++)
+        for (int jj = 0; jj < d; jj++)
+            for (int ii = 0; ii < d; ii++) {
+                size_t c = gidx(ii, jj, kk, d);
+                if (start[c] == 0xFFFFFFFFu) continue;
+                for (uint32_t p = start[c]; p < end[c]; p++) {
+                    if (p >= N) continue;
+                    float px = (float)((double)pos[p].x - origin3[0]);
+                    float py = (float)((double)pos[p].y - origin3[1]);
+                    float pz = (float)((double)pos[p].z - origin3[2]);
+                    /* grid cells whose window holds hash cell (ii,jj,kk) */
+                    for (int k = std::max(0, kk - 2); k <= std::min(d - 1, kk + 2); k++) {
+                        double r3 = (double)pz * invh - (double)(float)((double)k + 0.5);
+                        if (!(r3 < 0.5 && r3 >= -0.5)) continue;
+                        for (int j = std::max(0, jj - 2); j <= std::min(d - 1, jj + 2); j++) {
+                            double r2 = (double)py * invh - (double)(float)((double)j + 0.5);
+                            if (!(r2 < 0.5 && r2 >= -0.5)) continue;
+                            for (int i = std::max(0, ii - 2); i <= std::min(d - 1, ii + 2); i++) {
+                                double r1 = (double)px * invh - (double)(float)((double)i + 0.5);
+                                if (!(r1 < 0.5 && r1 >= -0.5)) continue;
+                                sum[gidx(i, j, k, d)] += 1.0 * smass[p];
+                            }
+                        }
+                    }
+                }
+            }
+    const size_t C = (size_t)d * d * d;
+    for (size_t c = 0; c < C; c++) grid[c] = invh * invh * invh * sum[c];
+}
+
+/* ------------------------------------------------------------------------
+ * Multigrid: MG/MultiGrid.h:114-139 (levels), MG/MultiGrid.cpp:128-250
+ * (V-cycle, FMG), MG/Multigrid.cu:46-55,202-330 and
+ * MG/MultiGrid_kernel.cu:422-934 (kernels).  Operator: sum of the six
+ * neighbours minus 6x, neighbours outside the box read as 0.
+ * ---------------------------------------------------------------------- */
+namespace {
+
+struct Level { int d; std::vector<double> x, b, r; };
+
+inline double nbr_sum(const double *x, int i, int j, int k, int d) {
+    size_t c = gidx(i, j, k, d);
+    double lv = (i > 0) ? x[c - 1] : 0.0;
+    double rv = (i < d - 1) ? x[c + 1] : 0.0;
+    double uv = (j < d - 1) ? x[c + d] : 0.0;
+    double dv = (j > 0) ? x[c - d] : 0.0;
+    double fv = (k > 0) ? x[c - (size_t)d * d] : 0.0;
+    double bv = (k < d - 1) ? x[c + (size_t)d * d] : 0.0;
+    double r = lv + rv;
+    r += uv + dv;
+    r += fv + bv;
+    return r;
+}
+
+/* MG/Multigrid.cu:202-239, MG/MultiGrid_kernel.cu:722-820: per iteration the
+ * "red" launch updates cells with (i+j+k) odd, then the "black" launch the
+ * even cells; x <- (1-w) x + w (sum_nbr - b) / 6. */
+void rbsor(double *x, const double *b, int d, int iters) {
+    const double invdiag = 1.0 / 6.0;
+    for (int it = 0; it < iters; it++) {
+        for (int color = 1; color >= 0; color--) {
+#pragma omp parallel for schedule(static) collapse(2)
+            for (int k = 0; k < d; k++)
+                for (int j = 0; j < d; j++) {
+                    int i0 = ((j + k + color) & 1);
+                    for (int i = i0; i < d; i += 2) {
+                        size_t c = gidx(i, j, k, d);
+                        double r = nbr_sum(x, i, j, k, d);
+                        r -= b[c];
+                        x[c] = kOneMinusOmega * x[c] + kOmega * r * invdiag;
+                    }
+                }
+        }
+    }
+}
+
+/* MG/MultiGrid_kernel.cu:821-871: r = b - (sum_nbr - 6 x). */
+void residual(const double *x, const double *b, double *res, int d) {
+#pragma omp parallel for schedule(static) collapse(2)
+    for (int k = 0; k < d; k++)
+        for (int j = 0; j < d; j++)
+            for (int i = 0; i < d; i++) {
+                size_t c = gidx(i, j, k, d);
+                double r = nbr_sum(x, i, j, k, d);
+                r -= 6 * x[c];
+                res[c] = b[c] - r;
+            }
+}
+
+/* MG/MultiGrid_kernel.cu:873-910: coarse = 0.5 * sum of the 8 children. */
+void restrict_(double *coarse, const double *fine, int dc) {
+    const int df = 2 * dc;
+#pragma omp parallel for schedule(static) collapse(2)
+    for (int k = 0; k < dc; k++)
+        for (int j = 0; j < dc; j++)
+            for (int i = 0; i < dc; i++) {
+                size_t f = gidx(2 * i, 2 * j, 2 * k, df);
+                size_t fy = f + df, fz = f + (size_t)df * df, fyz = fz + df;
+                double r = 0;
+                r += fine[f];
+                r += fine[f + 1];
+                r += fine[fy];
+                r += fine[fy + 1];
+                r += fine[fz];
+                r += fine[fz + 1];
+                r += fine[fyz];
+                r += fine[fyz + 1];
+                r = r * 0.5;
+                coarse[gidx(i, j, k, dc)] = r;
+            }
+}
+
+/* MG/MultiGrid_kernel.cu:912-934: fine += coarse[i/2, j/2, k/2]. */
+void prolong(double *fine, const double *coarse, int df) {
+    const int dc = df / 2;
+#pragma omp parallel for schedule(static) collapse(2)
+    for (int k = 0; k < df; k++)
+        for (int j = 0; j < df; j++)
+            for (int i = 0; i < df; i++)
+                fine[gidx(i, j, k, df)] += coarse[gidx(i / 2, j / 2, k / 2, dc)];
+}
+
+/* MG/MultiGrid_kernel.cu:422-498 (exact_solve_period3D_jacobi_kerneld): 100
+ * iterations of x <- (sum_nbr - b) / 6.  The reference's live phase updates x
+ * in place from 512 concurrent threads, so its order is not defined; mode 0
+ * runs the update in cell order (in-place Gauss-Seidel), mode 1 as Jacobi. */
+void coarse_solve(double *x, const double *b, int d, int coarse_mode) {
+    const size_t C = (size_t)d * d * d;
+    std::vector<double> xn(x, x + C);
+    std::vector<double> tmp(C);
+    for (int t = 0; t < 100; t++) {
+        if (coarse_mode == 1) {
+            for (size_t c = 0; c < C; c++) {
+                int i = (int)(c % d), j = (int)((c / d) % d), k = (int)(c / ((size_t)d * d));
+                double r = nbr_sum(xn.data(), i, j, k, d);
+                r -= b[c];
+                tmp[c] = r / 6;
+            }
+            xn.swap(tmp);
+        } else {
+            for (size_t c = 0; c < C; c++) {
+                int i = (int)(c % d), j = (int)((c / d) % d), k = (int)(c / ((size_t)d * d));
+                double r = nbr_sum(xn.data(), i, j, k, d);
+                r -= b[c];
+                xn[c] = r / 6;
+            }
+        }
+    }
+    std::memcpy(x, xn.data(), sizeof(double) * C);
+}
+
+struct MG {
+    std::vector<Level> lv;
+    int coarse_mode = 0;
+    explicit MG(int n, int cm) : coarse_mode(cm) {
+        int x = n, L = 0;
+        while ((long long)x * x * x > 512) { L++; x = x / 2; if (x == 0) x = 1; }
+        int levels = L + 1;
+        lv.resize(levels);
+        int d = n;
+        for (int l = 0; l < levels; l++) {
+            lv[l].d = d;
+            size_t C = (size_t)d * d * d;
+            lv[l].x.assign(C, 0.0); lv[l].b.assign(C, 0.0); lv[l].r.assign(C, 0.0);
+            d = (d / 2 == 0) ? 1 : d / 2;
+        }
+    }
+    int levels() const { return (int)lv.size(); }
+    void zero_from(int l0) {
+        for (int l = l0; l < levels(); l++) {
+            std::fill(lv[l].x.begin(), lv[l].x.end(), 0.0);
+            std::fill(lv[l].b.begin(), lv[l].b.end(), 0.0);
+            std::fill(lv[l].r.begin(), lv[l].r.end(), 0.0);
+        }
+    }
+    /* MG/MultiGrid.cpp:128-201, with level `level` holding x and b. */
+    void vcycle(int level) {
+        const int Lm = levels();
+        zero_from(level + 1);
+        std::fill(lv[level].r.begin(), lv[level].r.end(), 0.0);
+        for (int i = level; i < Lm - 1; ++i) {
+            rbsor(lv[i].x.data(), lv[i].b.data(), lv[i].d, 4);
+            residual(lv[i].x.data(), lv[i].b.data(), lv[i].r.data(), lv[i].d);
+            restrict_(lv[i + 1].b.data(), lv[i].r.data(), lv[i + 1].d);
+        }
+        coarse_solve(lv[Lm - 1].x.data(), lv[Lm - 1].b.data(), lv[Lm - 1].d, coarse_mode);
+        for (int i = Lm - 2; i >= level; --i) {
+            prolong(lv[i].x.data(), lv[i + 1].x.data(), lv[i].d);
+            rbsor(lv[i].x.data(), lv[i].b.data(), lv[i].d, 4);
+        }
+        zero_from(level + 1);
+    }
+    /* MG/MultiGrid.cpp:202-250. */
+    void fmg() {
+        const int Lm = levels();
+        zero_from(1);
+        std::fill(lv[0].r.begin(), lv[0].r.end(), 0.0);
+        for (int i = 0; i < Lm - 1; ++i) {
+            residual(lv[i].x.data(), lv[i].b.data(), lv[i].r.data(), lv[i].d);
+            restrict_(lv[i + 1].b.data(), lv[i].r.data(), lv[i + 1].d);
+        }
+        coarse_solve(lv[Lm - 1].x.data(), lv[Lm - 1].b.data(), lv[Lm - 1].d, coarse_mode);
+        for (int i = Lm - 2; i >= 0; --i) {
+            prolong(lv[i].x.data(), lv[i + 1].x.data(), lv[i].d);
+            vcycle(i);
+        }
+        vcycle(0);
+    }
+};
+
+double norm2(const double *v, size_t C) {
+    double s = 0;
+    for (size_t c = 0; c < C; c++) s += v[c] * v[c];
+    return std::sqrt(s);
+}
+
+}  // namespace
+
+extern "C" int orc_mg_levels(uint32_t n) { return MG((int)n, 0).levels(); }
+
+extern "C" void orc_apply_laplacian(const double *x, double *y, uint32_t n) {
+    const int d = (int)n;
+#pragma omp parallel for schedule(static) collapse(2)
+    for (int k = 0; k < d; k++)
+        for (int j = 0; j < d; j++)
+            for (int i = 0; i < d; i++) {
+                size_t c = gidx(i, j, k, d);
+                y[c] = nbr_sum(x, i, j, k, d) - 6 * x[c];
+            }
+}
+
+extern "C" double orc_residual_norm(const double *x, const double *b, uint32_t n) {
+    const size_t C = (size_t)n * n * n;
+    std::vector<double> r(C);
+    residual(x, b, r.data(), (int)n);
+    return norm2(r.data(), C);
+}
+
+/* One V-cycle at the finest level starting from x (MG/MultiGrid.cpp:128-201). */
+extern "C" void orc_mg_vcycle(double *x, const double *b, uint32_t n, int coarse_mode) {
+    MG mg((int)n, coarse_mode);
+    const size_t C = (size_t)n * n * n;
+    std::memcpy(mg.lv[0].x.data(), x, sizeof(double) * C);
+    std::memcpy(mg.lv[0].b.data(), b, sizeof(double) * C);
+    mg.vcycle(0);
+    std::memcpy(x, mg.lv[0].x.data(), sizeof(double) * C);
+}
+
+/* HFS/BiotSavartSolverImp.cpp:603-620: psi = 0, then m_FullMultiGrid.  In
+ * mode 1 further V-cycles run until the relative residual meets tol. */
+extern "C" void orc_mg_solve(double *x, const double *b, uint32_t n, int mg_mode,
+                             int coarse_mode, double tol, int max_cycles,
+                             int32_t *cycles_out, double *relres_out) {
+    MG mg((int)n, coarse_mode);
+    const size_t C = (size_t)n * n * n;
+    std::fill(mg.lv[0].x.begin(), mg.lv[0].x.end(), 0.0);
+    std::memcpy(mg.lv[0].b.data(), b, sizeof(double) * C);
+    mg.fmg();
+    int cycles = 1;
+    double bn = norm2(b, C);
+    std::vector<double> r(C);
+    residual(mg.lv[0].x.data(), b, r.data(), (int)n);
+    double rel = bn > 0 ? norm2(r.data(), C) / bn : 0.0;
+    if (mg_mode == 1) {
+        while (rel > tol && cycles < max_cycles) {
+            mg.vcycle(0);
+            cycles++;
+            residual(mg.lv[0].x.data(), b, r.data(), (int)n);
+            rel = bn > 0 ? norm2(r.data(), C) / bn : 0.0;
+        }
+    }
+    std::memcpy(x, mg.lv[0].x.data(), sizeof(double) * C);
+    if (cycles_out) *cycles_out = cycles;
+    if (relres_out) *relres_out = rel;
+}
+
+/* HFS/GPU_kernel.cu:1750-1805 (compute_curl_kernel) with the clamped
+ * sampling of sample3D (HFS/GPU_kernel.cu:23-30). */
+extern "C" void orc_curl(const double *psi3, double *u3, uint32_t n, double h) {
+    const int d = (int)n;
+    const size_t C = (size_t)d * d * d;
+    const double *Fx = psi3, *Fy = psi3 + C, *Fz = psi3 + 2 * C;
+    double *u = u3, *v = u3 + C, *w = u3 + 2 * C;
+    const double inv_h = 1.0 / h;
+    auto S = [&](const double *f, int x, int y, int z) {
+        int i = std::min(std::max(0, x), d - 1);
+        int j = std::min(std::max(0, y), d - 1);
+        int k = std::min(std::max(0, z), d - 1);
+        return f[gidx(i, j, k, d)];
+    };
+#pragma omp parallel for schedule(static) collapse(2)
+    for (int k = 0; k < d; k++)
+        for (int j = 0; j < d; j++)
+            for (int i = 0; i < d; i++) {
+                size_t c = gidx(i, j, k, d);
+                double Fz_up = S(Fz, i, j + 1, k), Fz_down = S(Fz, i, j - 1, k);
+                double Fz_left = S(Fz, i - 1, j, k), Fz_right = S(Fz, i + 1, j, k);
+                double Fy_front = S(Fy, i, j, k - 1), Fy_back = S(Fy, i, j, k + 1);
+                double Fy_left = S(Fy, i - 1, j, k), Fy_right = S(Fy, i + 1, j, k);
+                double Fx_front = S(Fx, i, j, k - 1), Fx_back = S(Fx, i, j, k + 1);
+                double Fx_up = S(Fx, i, j + 1, k), Fx_down = S(Fx, i, j - 1, k);
+                u[c] = 0.5 * inv_h * (Fz_up - Fz_down + Fy_front - Fy_back);
+                v[c] = 0.5 * inv_h * (Fx_back - Fx_front + Fz_left - Fz_right);
+                w[c] = 0.5 * inv_h * (Fy_right - Fy_left + Fx_down - Fx_up);
+            }
+}
+
+/* HFS/GPU_kernel.cu:11-17 (cpu_compute_r) and 2646-2677: central-difference
+ * gradient (step h) of 1/(4 pi |X - X'|) with X at the centre slot (the only
+ * slot Step1 reads, :2546-2549) and X' the cell-centre offset.  A coincident
+ * pair reads 1/1e24.  table[(off_z+K)(2K+1)^2 + (off_y+K)(2K+1) + off_x+K][3];
+ * the centre entry is left 0 (the reference never reads it). */
+extern "C" void orc_farfield_table(int K, double h, double *table) {
+    auto inv_r = [](double ax, double ay, double az, double bx, double by, double bz) {
+        double r_sqr = (ax - bx) * (ax - bx) + (ay - by) * (ay - by) + (az - bz) * (az - bz);
+        double r = (r_sqr > 1e-12) ? kFourPi * std::sqrt(r_sqr) : 1e+24;
+        return 1.0 / r;
+    };
+    const int W = 2 * K + 1;
+    for (int kk = -K; kk <= K; kk++)
+        for (int jj = -K; jj <= K; jj++)
+            for (int ii = -K; ii <= K; ii++) {
+                double *t = table + 3 * ((size_t)((kk + K) * W + (jj + K)) * W + (ii + K));
+                if (ii == 0 && jj == 0 && kk == 0) { t[0] = t[1] = t[2] = 0; continue; }
+                double Xpx = ((double)ii + 0.5) * h, Xpy = ((double)jj + 0.5) * h, Xpz = ((double)kk + 0.5) * h;
+                double Xx = 0.5 * h, Xy = 0.5 * h, Xz = 0.5 * h;
+                t[0] = 0.5 * (inv_r(Xx + h, Xy, Xz, Xpx, Xpy, Xpz) - inv_r(Xx - h, Xy, Xz, Xpx, Xpy, Xpz)) / h;
+                t[1] = 0.5 * (inv_r(Xx, Xy + h, Xz, Xpx, Xpy, Xpz) - inv_r(Xx, Xy - h, Xz, Xpx, Xpy, Xpz)) / h;
+                t[2] = 0.5 * (inv_r(Xx, Xy, Xz + h, Xpx, Xpy, Xpz) - inv_r(Xx, Xy, Xz - h, Xpx, Xpy, Xpz)) / h;
+            }
+}
+
+/* HFS/GPU_kernel.cu:2634-2734 (BiotSavartComputeFarField):
+ *   Step1 (:2487-2564): far = U - sum_{c' != c, |c'-c|<=K, in box}
+ *                              D[c'-c] x (omega(c') h^3)
+ *   then psi_d = 0.250580605913965 * omega * h^2 (:1976-2001), its clamped
+ *   curl, and far -= curl(psi_d) (:2566-2630; the jjj*dimy index equals
+ *   jjj*dimx on the cubic grids used here). */
+extern "C" void orc_farfield(const double *vort3, const double *u3, double *far3,
+                             uint32_t n, int K, double h) {
+    const int d = (int)n;
+    const size_t C = (size_t)d * d * d;
+    const int W = 2 * K + 1;
+    std::vector<double> table((size_t)W * W * W * 3);
+    orc_farfield_table(K, h, table.data());
+    const double vh3 = h * h * h;
+#pragma omp parallel for schedule(static) collapse(2)
+    for (int k = 0; k < d; k++)
+        for (int j = 0; j < d; j++)
+            for (int i = 0; i < d; i++) {
+                size_t c = gidx(i, j, k, d);
+                double mx = 0, my = 0, mz = 0;
+                for (int kk = k - K; kk <= k + K; kk++)
+                    for (int jj = j - K; jj <= j + K; jj++)
+                        for (int ii = i - K; ii <= i + K; ii++) {
+                            double ox = 0, oy = 0, oz = 0, dx = 0, dy = 0, dz = 0;
+                            if (kk >= 0 && kk < d && jj >= 0 && jj < d && ii >= 0 && ii < d) {
+                                size_t s = gidx(ii, jj, kk, d);
+                                ox = vort3[s] * vh3; oy = vort3[C + s] * vh3; oz = vort3[2 * C + s] * vh3;
+                                if (!(kk == k && jj == j && ii == i)) {
+                                    const double *t = table.data() + 3 * ((size_t)((kk - k + K) * W + (jj - j + K)) * W + (ii - i + K));
+                                    dx = t[0]; dy = t[1]; dz = t[2];
+                                }
+                            }
+                            mx += dy * oz - dz * oy;
+                            my += dz * ox - dx * oz;
+                            mz += dx * oy - dy * ox;
+                        }
+                far3[c] = u3[c] - mx;
+                far3[C + c] = u3[C + c] - my;
+                far3[2 * C + c] = u3[2 * C + c] - mz;
+            }
+    std::vector<double> psid(3 * C), ud(3 * C);
+    const double h2 = h * h;
+    for (size_t c = 0; c < 3 * C; c++) psid[c] = kDiagPsi * vort3[c] * h2;
+    orc_curl(psid.data(), ud.data(), n, h);
+    for (size_t c = 0; c < 3 * C; c++) far3[c] -= ud[c];
+}
+
+/* HFS/GPU_kernel.cu:2886-2976 (BiotSavartInterpolate_far_field_kernel2) with
+ * the hat weight poly_shape (HFS/GPU_kernel.cu:51-84).  Points whose own cell
+ * lies outside the grid are left untouched (the caller has zeroed out3). */
+extern "C" void orc_interp(const float *eval4, uint32_t M, const double *far3, uint32_t n,
+                           double cell_h, const double *origin3, double *out3) {
+    const F4 *pos = as_f4(eval4);
+    const int d = (int)n;
+    const size_t C = (size_t)d * d * d;
+    const double invh = 1.0 / cell_h;
+    auto poly = [](double r) { double rr = std::fabs(r); return rr < 1 ? 1 - rr : 0.0; };
+#pragma omp parallel for schedule(static)
+    for (int64_t t = 0; t < (int64_t)M; t++) {
+        float px = (float)((double)pos[t].x - origin3[0]);
+        float py = (float)((double)pos[t].y - origin3[1]);
+        float pz = (float)((double)pos[t].z - origin3[2]);
+        int i = (int)std::floor((double)px * invh);
+        int j = (int)std::floor((double)py * invh);
+        int k = (int)std::floor((double)pz * invh);
+        if (!(i >= 0 && i < d && j >= 0 && j < d && k >= 0 && k < d)) continue;
+        double sx = 0, sy = 0, sz = 0;
+        double qx = (double)px * invh, qy = (double)py * invh, qz = (double)pz * invh;
+        for (int kk = k - 2; kk <= k + 2; kk++)
+            for (int jj = j - 2; jj <= j + 2; jj++)
+                for (int ii = i - 2; ii <= i + 2; ii++) {
+                    if (!(kk >= 0 && kk < d && jj >= 0 && jj < d && ii >= 0 && ii < d)) continue;
+                    size_t g = gidx(ii, jj, kk, d);
+                    double gx = (double)(float)((double)ii + 0.5);
+                    double gy = (double)(float)((double)jj + 0.5);
+                    double gz = (double)(float)((double)kk + 0.5);
+                    double wgt = poly(gx - qx) * poly(gy - qy) * poly(gz - qz);
+                    sx += far3[g] * wgt;
+                    sy += far3[C + g] * wgt;
+                    sz += far3[2 * C + g] * wgt;
+                }
+        out3[t] = sx;
+        out3[M + t] = sy;
+        out3[2 * (size_t)M + t] = sz;
+    }
+}
+
+/* HFS/GPU_kernel.cu:2262-2485 (BiotSavartPPCorrScaleMN_kernel).  For every
+ * evaluation point, over hash cells [i-K-1, i+K+1]^3 and vortices inside the
+ * axis box |dx|,|dy|,|dz| < (K+0.5) h (float differences of float relative
+ * positions):  u += (alpha x (x_a - y_p)) * c(r) with
+ *   c = (1 - exp(-(r/a)^3)) / (4 pi r^3)        for r/a >= 0.01,
+ *   c = (1 - (r/a)^3 / 2) / (4 pi a^3)           otherwise (the 1/6 and 1/24
+ *                                                 terms are integer 0, :2401),
+ * c = 0 if r < 1e-12 or, for segments, if |x_b - y_p| < 1e-12.  Adds into u3
+ * (which holds the interpolated far field).  Returns the number of vortex
+ * candidates that passed the axis box. */
+extern "C" uint64_t orc_pp(const uint32_t *start, const uint32_t *end,
+                           const float *eval_a4, const float *eval_b4, int is_segment,
+                           const float *svort4, const double *salpha3, double *u3,
+                           uint32_t n, double cell_h, int K, uint32_t M, uint32_t N,
+                           const double *origin3, double a) {
+    const F4 *ea = as_f4(eval_a4), *eb = as_f4(eval_b4), *vp = as_f4(svort4);
+    const double *vx = salpha3, *vy = salpha3 + N, *vz = salpha3 + 2 * (size_t)N;
+    const int d = (int)n;
+    const double invh = 1.0 / cell_h;
+    const double correct_radius = ((double)K + 0.5) / invh;
+    uint64_t pairs = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : pairs)
+    for (int64_t t = 0; t < (int64_t)M; t++) {
+        float pax = (float)((double)ea[t].x - origin3[0]);
+        float pay = (float)((double)ea[t].y - origin3[1]);
+        float paz = (float)((double)ea[t].z - origin3[2]);
+        float pbx = 0, pby = 0, pbz = 0;
+        if (is_segment == 1) {
+            pbx = (float)((double)eb[t].x - origin3[0]);
+            pby = (float)((double)eb[t].y - origin3[1]);
+            pbz = (float)((double)eb[t].z - origin3[2]);
+        }
+        int i = (int)std::floor((double)pax * invh);
+        int j = (int)std::floor((double)pay * invh);
+        int k = (int)std::floor((double)paz * invh);
+        double ux = 0, uy = 0, uz = 0;
+        for (int kk = k - K - 1; kk <= k + K + 1; kk++)
+            for (int jj = j - K - 1; jj <= j + K + 1; jj++)
+                for (int ii = i - K - 1; ii <= i + K + 1; ii++) {
+                    if (!(kk >= 0 && kk < d && jj >= 0 && jj < d && ii >= 0 && ii < d)) continue;
+                    size_t c = gidx(ii, jj, kk, d);
+                    if (start[c] == 0xFFFFFFFFu) continue;
+                    for (uint32_t p = start[c]; p < end[c]; p++) {
+                        if (p >= N) continue;
+                        float qx = (float)((double)vp[p].x - origin3[0]);
+                        float qy = (float)((double)vp[p].y - origin3[1]);
+                        float qz = (float)((double)vp[p].z - origin3[2]);
+                        if (!((double)std::fabs(qx - pax) < correct_radius &&
+                              (double)std::fabs(qy - pay) < correct_radius &&
+                              (double)std::fabs(qz - paz) < correct_radius))
+                            continue;
+                        pairs++;
+                        double ox = vx[p], oy = vy[p], oz = vz[p];
+                        double dax = (double)(float)(pax - qx), day = (double)(float)(pay - qy),
+                               daz = (double)(float)(paz - qz);
+                        double r1 = std::sqrt(dax * dax + day * day + daz * daz);
+                        double coeff;
+                        double r_inva = r1 / a;
+                        if (r_inva >= 0.01) {
+                            coeff = (1 - std::exp(-r_inva * r_inva * r_inva)) / (kFourPi * r1 * r1 * r1);
+                        } else {
+                            double r3a3 = r_inva * r_inva * r_inva;
+                            coeff = 1 / (kFourPi * a * a * a) * (1 - 0.5 * r3a3);
+                        }
+                        if (r1 < 1e-12) coeff = 0;
+                        if (is_segment == 1) {
+                            double dbx = (double)(float)(pbx - qx), dby = (double)(float)(pby - qy),
+                                   dbz = (double)(float)(pbz - qz);
+                            double r2 = std::sqrt(dbx * dbx + dby * dby + dbz * dbz);
+                            if (r2 < 1e-12) coeff = 0;
+                        }
+                        double cx = oy * daz - oz * day;
+                        double cy = oz * dax - ox * daz;
+                        double cz = ox * day - oy * dax;
+                        ux += cx * coeff;
+                        uy += cy * coeff;
+                        uz += cz * coeff;
+                    }
+                }
+        u3[t] += ux;
+        u3[M + t] += uy;
+        u3[2 * (size_t)M + t] += uz;
+    }
+    return pairs;
+}
+
+/* HFS/BiotSavartSolverImp.cpp:756-816 (computeFarFieldBuffer) followed by
+ * :410-516 (evaluateVelocity), non-VIC branch.  Evaluation points are not
+ * reordered: each point's result is independent of the evaluation order. */
+extern "C" int orc_pppm(const orc_params *prm, uint32_t N, const float *vort_pos4,
+                        const double *ax, const double *ay, const double *az,
+                        uint32_t M, const float *eval_a4, const float *eval_b4,
+                        int is_segment, double *u, double *v, double *w, orc_dump *dump) {
+    if (!prm || N == 0 || prm->n < 2) return 1;
+    const uint32_t n = prm->n;
+    const size_t C = (size_t)n * n * n;
+    const F4 *vp = as_f4(vort_pos4);
+
+    double origin[3], L;
+    if (prm->domain_mode == 1) {
+        origin[0] = prm->fixed_origin[0]; origin[1] = prm->fixed_origin[1];
+        origin[2] = prm->fixed_origin[2]; L = prm->fixed_length;
+    } else {
+        orc_set_domain(vort_pos4, N, origin, &L);
+    }
+    /* setSpatialHashGrid(n, L/n as float, origin as float3), PH/SpaceHashClass.h:46-54 */
+    const float h_f = (float)(L / (double)n);
+    const float of[3] = {(float)origin[0], (float)origin[1], (float)origin[2]};
+    const double cell_h = (double)h_f;
+
+    std::vector<uint32_t> key(N), idx(N), start(C), end(C);
+    orc_calc_hash(vort_pos4, N, n, h_f, of, key.data(), idx.data());
+    orc_sort_by_key(key.data(), idx.data(), N);
+    orc_find_cell_start(key.data(), N, (uint32_t)C, start.data(), end.data());
+
+    std::vector<F4> spos(N);
+    std::vector<double> salpha(3 * (size_t)N);
+    for (uint32_t t = 0; t < N; t++) {
+        spos[t] = vp[idx[t]];
+        salpha[t] = ax[idx[t]];
+        salpha[N + t] = ay[idx[t]];
+        salpha[2 * (size_t)N + t] = az[idx[t]];
+    }
+
+    std::vector<double> gvort(3 * C), rhs(3 * C), psi(3 * C), gu(3 * C), far(3 * C);
+    const double h2f = (double)(h_f * h_f); /* getCellSize().x squared in float, :557 */
+    for (int c = 0; c < 3; c++) {
+        orc_p2m(start.data(), end.data(), reinterpret_cast<const float *>(spos.data()),
+                salpha.data() + c * (size_t)N, cell_h, n, N, origin, gvort.data() + c * C);
+        for (size_t q = 0; q < C; q++) rhs[c * C + q] = gvort[c * C + q] * h2f * -1.0;
+    }
+    for (int c = 0; c < 3; c++) {
+        int32_t cyc = 0; double rr = 0;
+        orc_mg_solve(psi.data() + c * C, rhs.data() + c * C, n, prm->mg_mode, prm->coarse_mode,
+                     prm->mg_tol, prm->mg_max_cycles, &cyc, &rr);
+        if (dump && dump->mg_cycles) dump->mg_cycles[c] = cyc;
+        if (dump && dump->mg_relres) dump->mg_relres[c] = rr;
+    }
+    orc_curl(psi.data(), gu.data(), n, cell_h);
+    if (prm->K >= 0)
+        orc_farfield(gvort.data(), gu.data(), far.data(), n, prm->K, cell_h);
+    else
+        far = gu; /* BiotSavartComputeFarField is a no-op for K < 0 (:2640) */
+
+    std::vector<double> U(3 * (size_t)M, 0.0);
+    orc_interp(eval_a4, M, far.data(), n, cell_h, origin, U.data());
+    if (dump && dump->u_far_only) std::memcpy(dump->u_far_only, U.data(), sizeof(double) * 3 * M);
+    uint64_t pairs = 0;
+    if (prm->K >= 0)
+        pairs = orc_pp(start.data(), end.data(), eval_a4, eval_b4, is_segment,
+                       reinterpret_cast<const float *>(spos.data()), salpha.data(), U.data(), n,
+                       cell_h, prm->K, M, N, origin, prm->a);
+    for (uint32_t t = 0; t < M; t++) {
+        u[t] = U[t];
+        v[t] = U[M + t];
+        w[t] = U[2 * (size_t)M + t];
+    }
+    if (dump) {
+        if (dump->origin) std::memcpy(dump->origin, origin, sizeof(origin));
+        if (dump->length) *dump->length = L;
+        if (dump->h_f) *dump->h_f = h_f;
+        if (dump->vort_key) std::memcpy(dump->vort_key, key.data(), sizeof(uint32_t) * N);
+        if (dump->vort_idx) std::memcpy(dump->vort_idx, idx.data(), sizeof(uint32_t) * N);
+        if (dump->cell_start) std::memcpy(dump->cell_start, start.data(), sizeof(uint32_t) * C);
+        if (dump->cell_end) std::memcpy(dump->cell_end, end.data(), sizeof(uint32_t) * C);
+        if (dump->grid_vort) std::memcpy(dump->grid_vort, gvort.data(), sizeof(double) * 3 * C);
+        if (dump->psi) std::memcpy(dump->psi, psi.data(), sizeof(double) * 3 * C);
+        if (dump->grid_u) std::memcpy(dump->grid_u, gu.data(), sizeof(double) * 3 * C);
+        if (dump->far_u) std::memcpy(dump->far_u, far.data(), sizeof(double) * 3 * C);
+        if (dump->pairs) *dump->pairs = pairs;
+    }
+    return 0;
+}
+
+/* FP64 O(N*M) sum with the same smoothing kernel as the near field,
+ * c(r) = (1 - exp(-(r/a)^3)) / (4 pi r^3), on the float input positions
+ * promoted to double; r = 0 and (for segments) |x_b - y_p| = 0 excluded. */
+extern "C" void orc_direct_sum(uint32_t N, const float *vort_pos4, const double *ax,
+                               const double *ay, const double *az, uint32_t M,
+                               const float *eval_a4, const float *eval_b4, int is_segment,
+                               double a, double *u, double *v, double *w) {
+    const F4 *vp = as_f4(vort_pos4), *ea = as_f4(eval_a4), *eb = as_f4(eval_b4);
+    const double inva = 1.0 / a;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t t = 0; t < (int64_t)M; t++) {
+        const double xa = ea[t].x, ya = ea[t].y, za = ea[t].z;
+        double xb = 0, yb = 0, zb = 0;
+        if (is_segment == 1) { xb = eb[t].x; yb = eb[t].y; zb = eb[t].z; }
+        double sx = 0, sy = 0, sz = 0;
+        for (uint32_t p = 0; p < N; p++) {
+            double dx = xa - (double)vp[p].x, dy = ya - (double)vp[p].y, dz = za - (double)vp[p].z;
+            double r2 = dx * dx + dy * dy + dz * dz;
+            if (r2 == 0.0) continue;
+            if (is_segment == 1) {
+                double ex = xb - (double)vp[p].x, ey = yb - (double)vp[p].y, ez = zb - (double)vp[p].z;
+                if (ex == 0.0 && ey == 0.0 && ez == 0.0) continue;
+            }
+            double r = std::sqrt(r2);
+            double s = r * inva;
+            double s3 = s * s * s;
+            double c = (s3 > 1e-8) ? -std::expm1(-s3) / (kFourPi * r2 * r)
+                                   : (1.0 - 0.5 * s3) * inva * inva * inva / kFourPi;
+            double ox = ax[p], oy = ay[p], oz = az[p];
+            sx += (oy * dz - oz * dy) * c;
+            sy += (oz * dx - ox * dz) * c;
+            sz += (ox * dy - oy * dx) * c;
+        }
+        u[t] = sx; v[t] = sy; w[t] = sz;
+    }
+}

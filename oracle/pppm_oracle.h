@@ -1,0 +1,119 @@
+/*
+ * CPU oracle for the PPPM vortex-particle velocity evaluation.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is a plain C++17 / OpenMP / FP64 restatement
+ * of the reference's BiotSavartSolver::computeFarFieldBuffer +
+ * evaluateVelocity path (hybridFastSummation, multigrid, particle_hash).  It is
+ * the checker the CUDA path is compared against and the timed CPU baseline.
+ * Nothing in the product links it: only tests/, __graft_entry__.smoke() and the
+ * cpu_baseline / reference legs of bench.py load it.
+ *
+ * Parity status: UNPINNED against reference outputs.  The reference ships no
+ * golden vectors and cannot be built or run here (it needs GL headers, the CUDA
+ * samples' helper_cuda.h / helper_math.h, and the texture-reference API that
+ * CUDA 12 removed).  The restatement is anchored instead by known-answer tests
+ * (tests/golden/, tests/test_oracle_*.py): FP32 cell assignment on crafted
+ * face / +-1 ulp particles, the discrete zero-ghost Laplacian's sine
+ * eigenmodes, the closed-form smoothed Biot-Savart kernel for one and two
+ * blobs, the finite-difference Green's-gradient table, and an independent
+ * numpy restatement of every stage at small sizes.
+ *
+ * Every function cites the reference file:line it restates.  Paths are
+ * relative to the reference project root; HFS = hybridFastSummation/
+ * hybridFastSummation, MG = multigrid/multigrid, PH = particle_hash/
+ * particle_hash.
+ */
+#ifndef PPPM_ORACLE_H
+#define PPPM_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Solver options.  mg_mode 0 = the reference schedule (full multigrid followed
+ * by one V(4,4) cycle, MG/MultiGrid.cpp:202-250); 1 = converged (further
+ * V-cycles until ||b-Ax||_2 <= mg_tol * ||b||_2).  coarse_mode selects the
+ * deterministic stand-in for the reference's racy in-place coarsest solve
+ * (MG/MultiGrid_kernel.cu:422-498): 0 = in-place sweeps in cell order
+ * (Gauss-Seidel), 1 = Jacobi (every read before any write). */
+typedef struct {
+    uint32_t n;            /* cubic grid edge (gridx == gridy == gridz)        */
+    int32_t  K;            /* near-field range in cells                        */
+    double   a;            /* smoothing radius (absolute length)               */
+    int32_t  domain_mode;  /* 0 = 3x vortex bbox (reference), 1 = fixed        */
+    double   fixed_origin[3];
+    double   fixed_length;
+    int32_t  mg_mode;
+    int32_t  coarse_mode;
+    double   mg_tol;
+    int32_t  mg_max_cycles;
+} orc_params;
+
+/* Optional intermediate outputs of orc_pppm (any pointer may be NULL). */
+typedef struct {
+    double   *origin;      /* [3]                                              */
+    double   *length;      /* [1]                                              */
+    float    *h_f;         /* [1] cell size as the hash stores it (float)      */
+    uint32_t *vort_key;    /* [N] sorted cell keys                             */
+    uint32_t *vort_idx;    /* [N] sorted original indices                      */
+    uint32_t *cell_start;  /* [n^3]                                            */
+    uint32_t *cell_end;    /* [n^3]                                            */
+    double   *grid_vort;   /* [3][n^3] P2M result (sum alpha / h^3)            */
+    double   *psi;         /* [3][n^3] vector potential                        */
+    double   *grid_u;      /* [3][n^3] curl(psi)                               */
+    double   *far_u;       /* [3][n^3] far-field velocity                      */
+    double   *u_far_only;  /* [3][M] interpolated far field (caller order)     */
+    uint64_t *pairs;       /* [1] near-field pairs inside the axis box         */
+    int32_t  *mg_cycles;   /* [3] V-cycles run after FMG per component         */
+    double   *mg_relres;   /* [3] final ||b-Ax||/||b|| per component           */
+} orc_dump;
+
+/* --- individual stages ------------------------------------------------- */
+void orc_set_domain(const float *pos4, uint32_t N, double *origin3, double *length);
+void orc_calc_hash(const float *pos4, uint32_t N, uint32_t n, float h_f,
+                   const float *origin_f3, uint32_t *key, uint32_t *idx);
+void orc_sort_by_key(uint32_t *key, uint32_t *idx, uint32_t N);
+void orc_find_cell_start(const uint32_t *skey, uint32_t N, uint32_t ncells,
+                         uint32_t *start, uint32_t *end);
+void orc_p2m(const uint32_t *start, const uint32_t *end, const float *spos4,
+             const double *smass, double cell_h, uint32_t n, uint32_t N,
+             const double *origin3, double *grid);
+int  orc_mg_levels(uint32_t n);
+void orc_mg_solve(double *x, const double *b, uint32_t n, int mg_mode,
+                  int coarse_mode, double tol, int max_cycles,
+                  int32_t *cycles_out, double *relres_out);
+void orc_mg_vcycle(double *x, const double *b, uint32_t n, int coarse_mode);
+double orc_residual_norm(const double *x, const double *b, uint32_t n);
+void orc_apply_laplacian(const double *x, double *y, uint32_t n);
+void orc_curl(const double *psi3, double *u3, uint32_t n, double h);
+void orc_farfield_table(int K, double h, double *table);
+void orc_farfield(const double *vort3, const double *u3, double *far3,
+                  uint32_t n, int K, double h);
+void orc_interp(const float *eval4, uint32_t M, const double *far3, uint32_t n,
+                double cell_h, const double *origin3, double *out3);
+uint64_t orc_pp(const uint32_t *start, const uint32_t *end,
+                const float *eval_a4, const float *eval_b4, int is_segment,
+                const float *svort4, const double *salpha3, double *u3,
+                uint32_t n, double cell_h, int K, uint32_t M, uint32_t N,
+                const double *origin3, double a);
+
+/* --- whole path: computeFarFieldBuffer + evaluateVelocity --------------- */
+int orc_pppm(const orc_params *p, uint32_t N, const float *vort_pos4,
+             const double *ax, const double *ay, const double *az,
+             uint32_t M, const float *eval_a4, const float *eval_b4,
+             int is_segment, double *u, double *v, double *w, orc_dump *dump);
+
+/* --- FP64 O(N*M) smoothed Biot-Savart sum (accuracy ground truth) ------- */
+void orc_direct_sum(uint32_t N, const float *vort_pos4, const double *ax,
+                    const double *ay, const double *az, uint32_t M,
+                    const float *eval_a4, const float *eval_b4, int is_segment,
+                    double a, double *u, double *v, double *w);
+
+int orc_num_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

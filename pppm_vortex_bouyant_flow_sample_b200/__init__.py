@@ -1,0 +1,441 @@
+"""B200-native PPPM vortex-particle velocity evaluation (host-side mirror).
+
+The compute path is libpppm_b200.so (hand-written sm_100a CUDA behind the C
+ABI of include/pppm.h).  This module binds it with ctypes and mirrors the
+reference's C++ interface for the path, using torch CUDA tensors only as
+device buffers:
+
+* ``BiotSavartSolver`` — hybridFastSummation/BiotSavartSolver.h:16-38
+  (initializeSolver, setVortParameter, setEvalParameter, computeFarFieldBuffer,
+  evaluateVelocity, getU, getVort, getSortVort, getSortPos, getVortStartTable,
+  getVortEndTable, sortVort, getCellh, getOrigin, shutdown);
+* ``ParticleManager`` — particle_hash/SpaceHashClass.h:10-84;
+* ``MultiGridSolver3DPeriod_double`` — multigrid/MultiGrid.h:188-209;
+* ``Scene`` — a direct wrapper of one pppm_scene.
+
+There is no CPU fallback: without the library or a CUDA device every call
+raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import torch
+
+from ._lib import (DOMAIN_BBOX3X, DOMAIN_FIXED, GRID_FAR, GRID_PSI, GRID_VORT, MG_CONVERGED,
+                   MG_REFERENCE, PppmError, PppmParams, check, default_params, load)
+
+__all__ = [
+    "Scene", "BiotSavartSolver", "ParticleManager", "MultiGridSolver3DPeriod_double", "PppmError",
+    "PppmParams", "default_params", "load", "direct_sum_fp64", "MG_REFERENCE", "MG_CONVERGED",
+    "DOMAIN_BBOX3X", "DOMAIN_FIXED",
+]
+
+
+def _require_cuda():
+    if not torch.cuda.is_available():
+        raise RuntimeError("pppm_b200 needs a CUDA device (B200, sm_100a); no CPU path exists")
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _stream_handle(stream):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def _pos4(t: torch.Tensor) -> torch.Tensor:
+    if t.dtype != torch.float32 or t.dim() != 2 or t.shape[1] != 4 or not t.is_cuda:
+        raise ValueError("positions must be a CUDA float32 tensor of shape (N, 4)")
+    return t.contiguous()
+
+
+def _alpha3(t: torch.Tensor, N: int):
+    """Accepts (N, 3) or (3, N) float64; returns three contiguous (N,) tensors."""
+    if t.dtype != torch.float64 or not t.is_cuda:
+        raise ValueError("strengths must be a CUDA float64 tensor")
+    if t.shape == (N, 3):
+        t = t.t()
+    if t.shape != (3, N):
+        raise ValueError(f"strengths must have shape (N, 3) or (3, N) with N={N}")
+    return [t[c].contiguous() for c in range(3)]
+
+
+class Scene:
+    """One resident PPPM scene (pppm_scene)."""
+
+    def __init__(self, n: int, K: int = 1, a: float = 0.08, domain: str = "bbox3x",
+                 fixed_origin=(0.0, 0.0, 0.0), fixed_length: float = 1.0, mg: str = "reference",
+                 mg_tol: float = 1e-10, mg_max_cycles: int = 50, cap_vort: int = 1, cap_eval: int = 1,
+                 stream: torch.cuda.Stream | None = None):
+        _require_cuda()
+        self._lib = load()
+        self.params = default_params(
+            n, K=K, a=a, domain_mode=DOMAIN_FIXED if domain == "fixed" else DOMAIN_BBOX3X,
+            fixed_origin=fixed_origin, fixed_length=fixed_length,
+            mg_mode=MG_CONVERGED if mg == "converged" else MG_REFERENCE, mg_tol=mg_tol,
+            mg_max_cycles=mg_max_cycles)
+        self.stream = stream if stream is not None else torch.cuda.current_stream()
+        h = C.c_void_p()
+        check(self._lib.pppm_scene_create(C.byref(self.params), cap_vort, cap_eval,
+                                          _stream_handle(self.stream), C.byref(h)), "pppm_scene_create")
+        self._h = h
+        self._keep = []
+        self.N = 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.pppm_scene_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_vortices(self, pos4: torch.Tensor, alpha: torch.Tensor):
+        pos4 = _pos4(pos4)
+        N = pos4.shape[0]
+        ax, ay, az = _alpha3(alpha, N)
+        check(self._lib.pppm_set_vortices(self._h, N, _ptr(pos4), _ptr(ax), _ptr(ay), _ptr(az)),
+              "pppm_set_vortices")
+        self._keep = [pos4, ax, ay, az]  # copies are enqueued; keep sources alive until they land
+        self.N = N
+
+    def build_far_field(self):
+        check(self._lib.pppm_build_far_field(self._h), "pppm_build_far_field")
+
+    def eval(self, eval_a: torch.Tensor, eval_b: torch.Tensor | None = None, is_segment: int = 0,
+             out: torch.Tensor | None = None) -> torch.Tensor:
+        """Velocities (M, 3) float64... returned as a (3, M) tensor view transposed to (M, 3)."""
+        ea = _pos4(eval_a)
+        M = ea.shape[0]
+        eb = _pos4(eval_b) if eval_b is not None else None
+        if is_segment == 1 and eb is None:
+            raise ValueError("is_segment=1 needs eval_b")
+        if out is None:
+            out = torch.empty((3, M), dtype=torch.float64, device=ea.device)
+        check(self._lib.pppm_eval(self._h, M, _ptr(ea), _ptr(eb), int(is_segment), _ptr(out[0]),
+                                  _ptr(out[1]), _ptr(out[2])), "pppm_eval")
+        return out.t()
+
+    def eval_f32(self, eval_a, eval_b=None, is_segment=0, out=None) -> torch.Tensor:
+        ea = _pos4(eval_a)
+        M = ea.shape[0]
+        eb = _pos4(eval_b) if eval_b is not None else None
+        if out is None:
+            out = torch.empty((M, 3), dtype=torch.float32, device=ea.device)
+        check(self._lib.pppm_eval_f32(self._h, M, _ptr(ea), _ptr(eb), int(is_segment), _ptr(out)),
+              "pppm_eval_f32")
+        return out
+
+    def solve_host(self, pos4_host, alpha_host, eval_a_host=None, eval_b_host=None, is_segment=0,
+                   out_host=None):
+        """End to end on (pinned) host tensors; returns (3, M) float64 host tensor."""
+        N = pos4_host.shape[0]
+        ax, ay, az = [alpha_host[c] for c in range(3)] if alpha_host.shape[0] == 3 else \
+            [alpha_host[:, c].contiguous() for c in range(3)]
+        M = N if eval_a_host is None else eval_a_host.shape[0]
+        if out_host is None:
+            out_host = torch.empty((3, M), dtype=torch.float64, pin_memory=True)
+        check(self._lib.pppm_solve_host(self._h, N, _ptr(pos4_host), _ptr(ax), _ptr(ay), _ptr(az), M,
+                                        _ptr(eval_a_host), _ptr(eval_b_host), int(is_segment),
+                                        _ptr(out_host[0]), _ptr(out_host[1]), _ptr(out_host[2])),
+              "pppm_solve_host")
+        return out_host
+
+    def domain(self):
+        o = (C.c_double * 3)()
+        L = C.c_double()
+        h = C.c_double()
+        check(self._lib.pppm_get_domain(self._h, o, C.byref(L), C.byref(h)), "pppm_get_domain")
+        return (o[0], o[1], o[2]), L.value, h.value
+
+    def cell_tables(self):
+        """(start, end) as int64 CPU tensors of the uint32 tables (n^3 each)."""
+        s = C.c_void_p()
+        e = C.c_void_p()
+        check(self._lib.pppm_get_cell_tables(self._h, C.byref(s), C.byref(e)), "pppm_get_cell_tables")
+        return _copy_u32(s.value, self.params.n ** 3, self.stream), _copy_u32(e.value, self.params.n ** 3, self.stream)
+
+    def sorted_index(self):
+        k = C.c_void_p()
+        i = C.c_void_p()
+        check(self._lib.pppm_get_sorted_index(self._h, C.byref(k), C.byref(i)), "pppm_get_sorted_index")
+        return _copy_u32(k.value, self.N, self.stream), _copy_u32(i.value, self.N, self.stream)
+
+    def sorted_vortices(self):
+        pos = torch.empty((self.N, 4), dtype=torch.float32, device="cuda")
+        al = torch.empty((3, self.N), dtype=torch.float64, device="cuda")
+        check(self._lib.pppm_get_sorted_vortices(self._h, _ptr(pos), _ptr(al[0]), _ptr(al[1]), _ptr(al[2])),
+              "pppm_get_sorted_vortices")
+        return pos, al
+
+    def grid(self, which: int) -> torch.Tensor:
+        p = C.c_void_p()
+        check(self._lib.pppm_get_grid(self._h, which, C.byref(p)), "pppm_get_grid")
+        n3 = self.params.n ** 3
+        dt = torch.float64 if which == GRID_PSI else torch.float32
+        return _copy_dev(p.value, 3 * n3, dt, self.stream).reshape(3, n3)
+
+    def stats(self):
+        pairs = C.c_uint64()
+        cyc = C.c_int32()
+        rr = C.c_double()
+        check(self._lib.pppm_get_stats(self._h, C.byref(pairs), C.byref(cyc), C.byref(rr)), "pppm_get_stats")
+        return {"mg_cycles": cyc.value, "mg_relres": rr.value}
+
+    def count_pairs(self, eval_a: torch.Tensor) -> int:
+        ea = _pos4(eval_a)
+        pairs = C.c_uint64()
+        check(self._lib.pppm_count_pairs(self._h, ea.shape[0], _ptr(ea), C.byref(pairs)), "pppm_count_pairs")
+        return int(pairs.value)
+
+
+class _DevView:
+    """Zero-copy view of device memory owned by the library."""
+
+    def __init__(self, ptr: int, count: int, typestr: str):
+        self.__cuda_array_interface__ = {"shape": (count,), "typestr": typestr, "data": (ptr, False),
+                                         "version": 2, "strides": None}
+
+
+def _copy_dev(ptr: int, count: int, dtype, stream) -> torch.Tensor:
+    """Copy `count` elements at a device address into a new CPU tensor."""
+    typestr = {torch.float32: "<f4", torch.float64: "<f8", torch.int32: "<i4"}[dtype]
+    torch.cuda.synchronize()
+    view = torch.as_tensor(_DevView(ptr, count, typestr), device="cuda")
+    return view.cpu()
+
+
+def _copy_u32(ptr: int, count: int, stream) -> torch.Tensor:
+    t = _copy_dev(ptr, count, torch.int32, stream)
+    return t.to(torch.int64) & 0xFFFFFFFF
+
+
+def direct_sum_fp64(vort_pos4, alpha, eval_a, a: float, eval_b=None, is_segment: int = 0, stream=None):
+    """FP64 O(N*M) smoothed Biot-Savart sum on the GPU; returns (M, 3) float64."""
+    _require_cuda()
+    L = load()
+    vp = _pos4(vort_pos4)
+    N = vp.shape[0]
+    ax, ay, az = _alpha3(alpha, N)
+    ea = _pos4(eval_a)
+    eb = _pos4(eval_b) if eval_b is not None else None
+    M = ea.shape[0]
+    out = torch.empty((3, M), dtype=torch.float64, device=ea.device)
+    check(L.pppm_direct_sum_fp64(N, _ptr(vp), _ptr(ax), _ptr(ay), _ptr(az), M, _ptr(ea), _ptr(eb),
+                                 int(is_segment), float(a), _ptr(out[0]), _ptr(out[1]), _ptr(out[2]),
+                                 _stream_handle(stream)), "pppm_direct_sum_fp64")
+    return out.t()
+
+
+class BiotSavartSolver:
+    """Mirror of hybridFastSummation/BiotSavartSolver.h:16-38 over one Scene.
+
+    Inputs are torch CUDA tensors standing in for the reference's GpuArrayf4
+    (float4 positions) and GpuArrayd (double per-component arrays).
+    """
+
+    def __init__(self):
+        self._scene = None
+        self._dims = None
+        self._K = 1
+        self._M = 0
+        self._N = 0
+        self._eval_pos = None
+        self._U = None
+        self._vort = None
+        self._sorted = None
+
+    def initializeSolver(self, gdx, gdy, gdz, isVIC, K, M, N, a=0.08, mg="reference"):
+        """HFS/BiotSavartSolverImp.cpp:44-229.  Cubic grids only; isVIC=True
+        (mesh-only velocities) is not part of the path and is rejected."""
+        if not (gdx == gdy == gdz):
+            raise ValueError("the hash and multigrid are cubic: gdx == gdy == gdz required")
+        if isVIC:
+            raise ValueError("isVIC is not supported (the reference ships with it off)")
+        if self._scene is None or self._dims != (gdx, K):
+            if self._scene is not None:
+                self._scene.close()
+            self._scene = Scene(gdx, K=K, a=a, mg=mg, cap_vort=max(N, 1), cap_eval=max(M, 1))
+            self._dims = (gdx, K)
+        self._K, self._M, self._N = K, M, N
+        return True
+
+    def setVortParameter(self, n, pos, omega):
+        """HFS/BiotSavartSolverImp.cpp:318-360: omega is a list of 3 double arrays."""
+        self._N = n
+        self._vort = [o[:n] for o in omega]
+        self._scene.set_vortices(pos[:n], torch.stack(self._vort))
+        self._sorted = None
+        return True
+
+    def setEvalParameter(self, m, pos):
+        """HFS/BiotSavartSolverImp.cpp:266-316."""
+        self._M = m
+        self._eval_pos = pos[:m]
+        return True
+
+    def computeFarFieldBuffer(self):
+        """HFS/BiotSavartSolverImp.cpp:756-816."""
+        self._scene.build_far_field()
+
+    def evaluateVelocity(self, another_end, is_segment):
+        """HFS/BiotSavartSolverImp.cpp:410-516."""
+        eb = another_end[:self._M] if (is_segment == 1 and another_end is not None) else None
+        self._U = self._scene.eval(self._eval_pos, eb, int(is_segment)).t()
+        return True
+
+    def getU(self, i):
+        return self._U[i]
+
+    def getVort(self, i):
+        return self._vort[i]
+
+    def sortVort(self):
+        """HFS/BiotSavartSolverImp.cpp:733-753 (bounding box + hash + reorder);
+        the far-field build performs the same steps, so this only refreshes the
+        sorted copies."""
+        self._scene.build_far_field()
+        self._sorted = self._scene.sorted_vortices()
+
+    def _sorted_copy(self):
+        if self._sorted is None:
+            self._sorted = self._scene.sorted_vortices()
+        return self._sorted
+
+    def getSortPos(self):
+        return self._sorted_copy()[0]
+
+    def getSortVort(self, i):
+        return self._sorted_copy()[1][i]
+
+    def getVortStartTable(self):
+        return self._scene.cell_tables()[0]
+
+    def getVortEndTable(self):
+        return self._scene.cell_tables()[1]
+
+    def getCellh(self):
+        return self._scene.domain()[2]
+
+    def getOrigin(self):
+        o, _, _ = self._scene.domain()
+        return (o[0], o[1], o[2], 0.0)
+
+    def shutdown(self):
+        if self._scene is not None:
+            self._scene.close()
+            self._scene = None
+        return True
+
+
+class ParticleManager:
+    """Mirror of particle_hash/SpaceHashClass.h:10-84 (pppm_hasher)."""
+
+    def __init__(self):
+        self._h = None
+        self._n = 0
+        self._N = 0
+        self._h_cell = 0.0
+        self._origin = (0.0, 0.0, 0.0)
+
+    def initSpatialHash(self, numParticles, dimx, dimy, dimz):
+        _require_cuda()
+        if not (dimx == dimy == dimz):
+            raise ValueError("cubic hash grids only")
+        self.endSpatialHash()
+        L = load()
+        h = C.c_void_p()
+        check(L.pppm_hasher_create(numParticles, dimx, _stream_handle(None), C.byref(h)), "pppm_hasher_create")
+        self._h = h
+        self._n = dimx
+        self._N = numParticles
+        self._h_cell = 1.0 / dimx
+
+    def endSpatialHash(self):
+        if self._h is not None:
+            load().pppm_hasher_destroy(self._h)
+            self._h = None
+
+    def setSpatialHashGrid(self, size0, h, bbmin, numParticles):
+        self._h_cell = float(torch.tensor(h, dtype=torch.float32))
+        self._origin = tuple(float(torch.tensor(v, dtype=torch.float32)) for v in bbmin)
+        self._N = numParticles
+
+    def setHashParam(self):
+        pass  # parameters travel with each call; no global constant memory
+
+    def doSpatialHash(self, pos, numParticles):
+        pos = _pos4(pos)
+        o = (C.c_float * 3)(*self._origin)
+        check(load().pppm_hasher_run(self._h, numParticles, _ptr(pos), C.c_float(self._h_cell), o),
+              "pppm_hasher_run")
+
+    def _tables(self):
+        k, i, s, e = C.c_void_p(), C.c_void_p(), C.c_void_p(), C.c_void_p()
+        check(load().pppm_hasher_tables(self._h, C.byref(k), C.byref(i), C.byref(s), C.byref(e)),
+              "pppm_hasher_tables")
+        return k.value, i.value, s.value, e.value
+
+    def getHashTable(self):
+        return _copy_u32(self._tables()[0], self._N, None)
+
+    def getIndexTable(self):
+        return _copy_u32(self._tables()[1], self._N, None)
+
+    def getStartTable(self):
+        return _copy_u32(self._tables()[2], self._n ** 3, None)
+
+    def getEndTable(self):
+        return _copy_u32(self._tables()[3], self._n ** 3, None)
+
+    def reorderData(self, numParticles, data, dataReorder, stride, precision):
+        check(load().pppm_hasher_reorder(self._h, numParticles, _ptr(data), _ptr(dataReorder), stride, precision),
+              "pppm_hasher_reorder")
+
+    def deorderData(self, numParticles, data, dataReorder, stride, precision):
+        check(load().pppm_hasher_deorder(self._h, numParticles, _ptr(data), _ptr(dataReorder), stride, precision),
+              "pppm_hasher_deorder")
+
+
+class MultiGridSolver3DPeriod_double:
+    """Mirror of multigrid/MultiGrid.h:188-209 (pppm_mg)."""
+
+    def __init__(self):
+        self._h = None
+        self.n = 0
+
+    def m_InitialSystem(self, gridx, gridy, gridz):
+        _require_cuda()
+        if not (gridx == gridy == gridz):
+            raise ValueError("cubic grids only")
+        self.m_FinalMemoryEachLevel()
+        h = C.c_void_p()
+        check(load().pppm_mg_create(gridx, _stream_handle(None), C.byref(h)), "pppm_mg_create")
+        self._h = h
+        self.n = gridx
+
+    def m_FinalMemoryEachLevel(self):
+        if self._h is not None:
+            load().pppm_mg_destroy(self._h)
+            self._h = None
+
+    def m_FullMultiGrid(self, x: torch.Tensor, b: torch.Tensor, tol: float = 1e-10,
+                        mode: int = MG_REFERENCE, max_cycles: int = 50) -> float:
+        """Solves sum_nbr(x) - 6x = b (zero ghosts) into x; returns the
+        relative residual (-1 in reference mode, which does not measure it)."""
+        if x.dtype != torch.float64 or b.dtype != torch.float64 or not x.is_cuda:
+            raise ValueError("x and b must be CUDA float64 tensors")
+        rr = C.c_double()
+        check(load().pppm_mg_full_multigrid(self._h, _ptr(x), _ptr(b.contiguous()), mode, tol, max_cycles,
+                                            C.byref(rr)), "pppm_mg_full_multigrid")
+        return rr.value

@@ -1,0 +1,127 @@
+"""ctypes binding of libpppm_b200.so (the C ABI declared in include/pppm.h).
+
+Loading fails loudly: there is no CPU fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from . import _build
+
+PPPM_OK = 0
+STATUS_NAMES = {0: "PPPM_OK", 1: "PPPM_ERR_INVALID", 2: "PPPM_ERR_CUDA", 3: "PPPM_ERR_OOM",
+                4: "PPPM_ERR_STATE", 5: "PPPM_ERR_DOMAIN"}
+DOMAIN_BBOX3X, DOMAIN_FIXED = 0, 1
+MG_REFERENCE, MG_CONVERGED = 0, 1
+GRID_VORT, GRID_PSI, GRID_FAR = 0, 1, 2
+
+# Every symbol include/pppm.h declares; tests check the library exports them.
+EXPORTED = (
+    "pppm_last_error", "pppm_version", "pppm_params_default", "pppm_scene_create",
+    "pppm_scene_destroy", "pppm_scene_set_stream", "pppm_scene_get_params", "pppm_set_vortices",
+    "pppm_build_far_field", "pppm_eval", "pppm_eval_f32", "pppm_solve_host", "pppm_get_domain",
+    "pppm_get_cell_tables", "pppm_get_sorted_index", "pppm_get_sorted_vortices", "pppm_get_grid",
+    "pppm_get_stats", "pppm_count_pairs", "pppm_mg_create", "pppm_mg_destroy",
+    "pppm_mg_full_multigrid", "pppm_hasher_create", "pppm_hasher_destroy", "pppm_hasher_run",
+    "pppm_hasher_tables", "pppm_hasher_reorder", "pppm_hasher_deorder", "pppm_direct_sum_fp64",
+)
+
+
+class PppmParams(C.Structure):
+    _fields_ = [
+        ("n", C.c_uint32),
+        ("K", C.c_int32),
+        ("a", C.c_double),
+        ("domain_mode", C.c_int32),
+        ("fixed_origin", C.c_double * 3),
+        ("fixed_length", C.c_double),
+        ("mg_mode", C.c_int32),
+        ("mg_tol", C.c_double),
+        ("mg_max_cycles", C.c_int32),
+    ]
+
+
+class PppmError(RuntimeError):
+    def __init__(self, status: int, where: str, msg: str):
+        super().__init__(f"{where}: {STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+_lib = None
+vp = C.c_void_p
+u32 = C.c_uint32
+i32 = C.c_int32
+
+
+def library_path() -> str:
+    return _build.LIB
+
+
+def load(build_if_missing: bool = True):
+    """Load the library (building it in-tree first if it is missing or stale)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if build_if_missing and not _build.up_to_date():
+        _build.build()
+    path = library_path()
+    if not os.path.exists(path):
+        raise ImportError(f"libpppm_b200.so not found at {path}; run __graft_entry__.build()")
+    L = C.CDLL(path)
+    st = C.c_int
+    sig = {
+        "pppm_last_error": (C.c_char_p, []),
+        "pppm_version": (C.c_char_p, []),
+        "pppm_params_default": (st, [C.POINTER(PppmParams)]),
+        "pppm_scene_create": (st, [C.POINTER(PppmParams), u32, u32, vp, C.POINTER(vp)]),
+        "pppm_scene_destroy": (st, [vp]),
+        "pppm_scene_set_stream": (st, [vp, vp]),
+        "pppm_scene_get_params": (st, [vp, C.POINTER(PppmParams)]),
+        "pppm_set_vortices": (st, [vp, u32, vp, vp, vp, vp]),
+        "pppm_build_far_field": (st, [vp]),
+        "pppm_eval": (st, [vp, u32, vp, vp, C.c_int, vp, vp, vp]),
+        "pppm_eval_f32": (st, [vp, u32, vp, vp, C.c_int, vp]),
+        "pppm_solve_host": (st, [vp, u32, vp, vp, vp, vp, u32, vp, vp, C.c_int, vp, vp, vp]),
+        "pppm_get_domain": (st, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+        "pppm_get_cell_tables": (st, [vp, C.POINTER(vp), C.POINTER(vp)]),
+        "pppm_get_sorted_index": (st, [vp, C.POINTER(vp), C.POINTER(vp)]),
+        "pppm_get_sorted_vortices": (st, [vp, vp, vp, vp, vp]),
+        "pppm_get_grid": (st, [vp, C.c_int, C.POINTER(vp)]),
+        "pppm_get_stats": (st, [vp, C.POINTER(C.c_uint64), C.POINTER(i32), C.POINTER(C.c_double)]),
+        "pppm_count_pairs": (st, [vp, u32, vp, C.POINTER(C.c_uint64)]),
+        "pppm_mg_create": (st, [u32, vp, C.POINTER(vp)]),
+        "pppm_mg_destroy": (st, [vp]),
+        "pppm_mg_full_multigrid": (st, [vp, vp, vp, C.c_int, C.c_double, C.c_int, C.POINTER(C.c_double)]),
+        "pppm_hasher_create": (st, [u32, u32, vp, C.POINTER(vp)]),
+        "pppm_hasher_destroy": (st, [vp]),
+        "pppm_hasher_run": (st, [vp, u32, vp, C.c_float, C.POINTER(C.c_float)]),
+        "pppm_hasher_tables": (st, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
+        "pppm_hasher_reorder": (st, [vp, u32, vp, vp, u32, u32]),
+        "pppm_hasher_deorder": (st, [vp, u32, vp, vp, u32, u32]),
+        "pppm_direct_sum_fp64": (st, [u32, vp, vp, vp, vp, u32, vp, vp, C.c_int, C.c_double, vp, vp, vp, vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return _lib
+
+
+def check(status: int, where: str):
+    if status != PPPM_OK:
+        msg = load().pppm_last_error().decode(errors="replace")
+        raise PppmError(status, where, msg)
+
+
+def default_params(n: int, **kw) -> PppmParams:
+    p = PppmParams()
+    check(load().pppm_params_default(C.byref(p)), "pppm_params_default")
+    p.n = n
+    for k, v in kw.items():
+        if k == "fixed_origin":
+            p.fixed_origin[:] = list(v)
+        else:
+            setattr(p, k, v)
+    return p

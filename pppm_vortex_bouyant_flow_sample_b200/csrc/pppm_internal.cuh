@@ -1,0 +1,155 @@
+// Internal declarations shared by the sm_100a kernels and the C ABI.
+//
+// Data layout in HBM (one scene, grid edge n, C = n^3 cells, N vortices,
+// M evaluation points):
+//   * grids are x-fastest, index (k*n + j)*n + i, components stored as three
+//     consecutive planes [3][C] (structure of arrays);
+//   * sorted vortex records are two float4 streams: {rel.x, rel.y, rel.z,
+//     ngp cell id as bits} and {alpha.x, alpha.y, alpha.z, 0}, where rel is the
+//     position relative to the domain origin rounded to float exactly as the
+//     reference rounds it, and the ngp cell is floor(rel * (1/h)) in FP64;
+//   * multigrid levels are FP32 [3][C_l] planes; the corrected potential psi is
+//     FP64 [3][C].
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/pppm.h"
+
+namespace pppm {
+
+constexpr uint32_t kEmpty = 0xFFFFFFFFu;
+constexpr int kMaxLevels = 12;
+constexpr int kMaxK = 4;  // near-field range limit (table (2K+1)^3 in shared memory)
+
+// Literal constants of the reference kernels.
+constexpr double kFourPi = 12.5663706144;          // HFS/GPU_kernel.cu:12,2397,2403
+constexpr double kDiagPsi = 0.250580605913965;     // HFS/GPU_kernel.cu:1990-1992
+
+// Per-scene parameters derived on the device from the vortex bounding box
+// (HFS/BiotSavartSolverImp.cpp:379-409, PH/SpaceHashClass.h:46-54), so that no
+// host round trip is needed between the bounding box and the hash.
+struct DevParams {
+    double origin[3];   // domain origin (double, as the solver keeps it)
+    double length;      // domain edge L
+    double cell_h;      // (double)h_f: the solver reads the float cell size back
+    double invh;        // 1.0 / cell_h
+    float origin_f[3];  // float origin the hash uses
+    float h_f;          // float cell size the hash uses
+    float h2f;          // h_f*h_f rounded to float (ComputeRHS argument, :557)
+    float invh3_f;      // (float)(invh^3)
+    float cr_f;         // largest float strictly below (K+0.5)/invh
+    float vh3_f;        // (float)(h^3) for the mesh correction
+    float kdiag_f;      // (float)(0.5 * invh * 0.250580605913965 * h^2)
+    float inv_a3_f;     // 1/a^3
+    float inv4pia3_f;   // 1/(4 pi a^3)
+    uint32_t n;
+    int32_t K;
+    int32_t status;     // 0 ok, else PPPM_ERR_* raised on the device
+};
+
+struct Level {
+    uint32_t d;       // edge
+    uint32_t cells;   // d^3
+    float *x;         // [comps][cells]
+    float *b;         // [comps][cells]
+};
+
+// Everything one multigrid solve touches; comps independent right-hand sides.
+struct MGPlan {
+    int levels = 0;
+    Level lv[kMaxLevels];
+    int comps = 3;
+    cudaStream_t st = nullptr;
+    double *psi = nullptr;          // [comps][C0] FP64 solution
+    const double *b64 = nullptr;    // FP64 right-hand side, or
+    const float *vort = nullptr;    // b = -(vort * h2f) from the P2M grid
+    const DevParams *P = nullptr;
+    double *norms = nullptr;        // [2] device scratch
+};
+
+}  // namespace pppm
+
+// Scene: every buffer is sized at creation (or on growth in
+// pppm_set_vortices / pppm_eval), so the per-call path allocates nothing.
+struct pppm_scene {
+    pppm_params prm;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    uint32_t n = 0, C = 0;
+    int levels = 0;
+    pppm::Level lv[pppm::kMaxLevels];
+
+    uint32_t capN = 0, capM = 0;
+    uint32_t N = 0, M = 0;
+    bool vort_set = false, far_ready = false;
+
+    pppm::DevParams *dparams = nullptr;   // device
+    float *bbox_partial = nullptr;        // [6][bbox_blocks]
+    int bbox_blocks = 0;
+
+    // vortex side
+    float4 *vpos = nullptr;               // caller order copy [capN]
+    double *valpha = nullptr;             // caller order copy [3][capN]
+    uint32_t *vkey[2] = {nullptr, nullptr};
+    uint32_t *vidx[2] = {nullptr, nullptr};
+    uint32_t *vsorted_key = nullptr, *vsorted_idx = nullptr;  // point into vkey/vidx
+    float4 *vrec = nullptr;               // sorted {rel, ngp}
+    float4 *valf = nullptr;               // sorted {alpha, 0}
+    uint32_t *cell_start = nullptr, *cell_end = nullptr, *mflag = nullptr;
+    uint32_t epoch = 0;
+
+    // radix-sort histogram scratch
+    uint32_t *hist = nullptr;
+    size_t hist_cap = 0;
+
+    // grid side
+    float *vort = nullptr;                // [3][C]
+    float *mg_pool = nullptr;             // all levels' x and b
+    double *psi = nullptr;                // [3][C]
+    float *far = nullptr;                 // [3][C]
+    double *norms = nullptr;              // [2] residual / rhs squared norms
+
+    // evaluation side
+    uint32_t *ekey[2] = {nullptr, nullptr};
+    uint32_t *eidx[2] = {nullptr, nullptr};
+    uint32_t *esorted_idx = nullptr;
+    float4 *stage_ea = nullptr, *stage_eb = nullptr;  // pppm_solve_host staging [capM]
+    double *stage_out = nullptr;                       // [3][capM]
+
+    // statistics
+    unsigned long long *pair_count = nullptr;
+    int mg_cycles_last = 0;
+    double mg_relres_last = 0.0;
+};
+
+namespace pppm {
+
+// Kernel launchers (each enqueues on s->stream and returns the launch status).
+cudaError_t launch_bbox_and_params(pppm_scene *s);
+cudaError_t launch_hash_sort(pppm_scene *s, const float4 *pos, uint32_t N, uint32_t *key[2],
+                             uint32_t *idx[2], uint32_t **sorted_key, uint32_t **sorted_idx);
+cudaError_t launch_cells_reorder(pppm_scene *s);
+cudaError_t launch_p2m(pppm_scene *s);
+cudaError_t run_multigrid(pppm_scene *s);
+cudaError_t launch_farfield(pppm_scene *s);
+cudaError_t launch_eval(pppm_scene *s, const float4 *eval_a, const float4 *eval_b, int is_segment,
+                        uint32_t M, double *u, double *v, double *w, float *uf, int count_pairs);
+cudaError_t launch_gather_sorted(pppm_scene *s, float4 *pos_out, double *alpha_out);
+
+cudaError_t mg_solve(const MGPlan &m, int mode, double tol, int max_cycles, int *cycles_out,
+                     double *relres_out);
+
+int mg_level_count(uint32_t n);
+bool mg_shape_ok(uint32_t n);
+uint32_t key_bits(uint32_t n);
+size_t radix_hist_entries(uint32_t N);
+
+}  // namespace pppm
+
+#define PPPM_CUDA_TRY(expr)                            \
+    do {                                               \
+        cudaError_t _e = (expr);                       \
+        if (_e != cudaSuccess) return _e;              \
+    } while (0)
