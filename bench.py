@@ -1,0 +1,340 @@
+#!/usr/bin/env python
+"""PPPM particle-velocity evaluations/s on one B200 (and N replicas).
+
+Workload (the at-scale plain-PPPM configuration): a vortex ring of 1,048,576
+particles (major radius 0.25, Gaussian core sigma 0.03, circulation 1,
+relative strength noise 1e-3, seed 1) on a 128^3 grid, K = 1, smoothing radius
+a = 0.08, domain = 3x the particle bounding box, the reference's multigrid
+schedule.  One step = one pass of the path over the scene: copy the particles
+into the scene, build the far field (hash, P2M, multigrid x3, curl, far-field
+correction) and evaluate the velocity at every particle (segment mode against
+itself, so each particle excludes itself) — computeFarFieldBuffer +
+evaluateVelocity of the reference.  Inputs are synthetic (seeded generator).
+
+value  = evaluations/s of the whole job (all ranks), inputs resident in HBM,
+         device-timed with CUDA events, L2 flushed between timed steps.
+e2e    = the same metric through pppm_solve_host with pinned host buffers,
+         host->device and device->host copies inside the timed region.
+--impl reference times the reference algorithm's CPU restatement (oracle/)
+on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "PPPM particle-velocity evals/s at <=1e-4 rel err vs FP64; served p50/p99 latency"
+UNIT = "evals/s"
+N_PART = 1_048_576
+GRID = 128
+K_NEAR = 1
+A_SMOOTH = 0.08
+WORKLOAD = ("vortex ring, 1,048,576 particles, 128^3 grid, K=1, a=0.08, domain 3x bbox, "
+            "reference multigrid schedule (FMG + 1 V(4,4), FP32 with FP64 defect correction); "
+            "step = far-field build + velocity at every particle")
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1965e6 / 1e12  # nominal: SMs x FP32 lanes x FMA x max clock
+L2_FLUSH_BYTES = 512 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--particles", type=int, default=N_PART)
+    ap.add_argument("--grid", type=int, default=GRID)
+    return ap.parse_args()
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs"), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3] not in ("", "[N/A]"))}
+
+
+def cpu_sample_rate(pos, al, n, m_small=2000, m_big=12000):
+    """Oracle (FP64 restatement of the reference path) on the host cores:
+    the whole far-field build for all particles plus the near field at two
+    evaluation subsets; the per-point cost is extrapolated to all particles."""
+    from oracle import pyoracle as O
+    prm = O.params(n, K=K_NEAR, a=A_SMOOTH)
+    N = len(pos)
+    stride_s = max(N // m_small, 1)
+    stride_b = max(N // m_big, 1)
+    ea_s = np.ascontiguousarray(pos[::stride_s][:m_small])
+    ea_b = np.ascontiguousarray(pos[::stride_b][:m_big])
+    t0 = time.perf_counter()
+    O.pppm(prm, pos, al, ea_s, ea_s, 1)
+    t1 = time.perf_counter()
+    O.pppm(prm, pos, al, ea_b, ea_b, 1)
+    t2 = time.perf_counter()
+    ts, tb = t1 - t0, t2 - t1
+    per_eval = max((tb - ts) / (len(ea_b) - len(ea_s)), 0.0)
+    fixed = max(ts - per_eval * len(ea_s), 0.0)
+    t_full = fixed + per_eval * N
+    return {"value": N / t_full, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
+            "sample": (f"oracle FP64 restatement: far-field build for all {N} particles + near field at "
+                       f"{len(ea_s)} and {len(ea_b)} particles ({ts + tb:.1f} s of CPU work); per-point "
+                       f"near-field cost extrapolated to all {N} particles"),
+            "seconds": ts + tb}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    from pppm_vortex_bouyant_flow_sample_b200 import workloads as W
+    from oracle import pyoracle as O
+    O.build()
+    pos, al = W.vortex_ring(args.particles, seed=1)
+    for _ in range(args.warmup):
+        pass  # the oracle has no warm state; warm-up steps are not needed
+    vals = []
+    t0 = time.perf_counter()
+    for _ in range(max(args.steps, 1)):
+        r = cpu_sample_rate(pos, al, args.grid, m_small=1000, m_big=4000)
+        vals.append(r["value"])
+    el = time.perf_counter() - t0
+    value = statistics.median(vals)
+    cpu = {"value": value, "unit": UNIT, "cores": r["cores"], "kind": "port", "sample": r["sample"]}
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * el / max(args.steps, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "grid": args.grid, "particles": args.particles,
+                                            "parallelism": "host threads (OpenMP)"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def read_profile_traffic():
+    """DRAM bytes per launch of the eval kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "eval_kernel_ring128.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def run_b200(args, world, rank, local):
+    import torch
+    import torch.distributed as dist
+    import pppm_vortex_bouyant_flow_sample_b200 as pb
+    from pppm_vortex_bouyant_flow_sample_b200 import workloads as W
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    N = args.particles
+    pos, al = W.vortex_ring(N, seed=1)
+    dpos = torch.from_numpy(pos).cuda()
+    dal = torch.from_numpy(np.ascontiguousarray(al.T)).cuda()
+    out = torch.empty((3, N), dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+    scene = pb.Scene(args.grid, K=K_NEAR, a=A_SMOOTH, cap_vort=N, cap_eval=N, stream=stream)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    lib = pb.load()
+
+    def step():
+        scene.set_vortices(dpos, dal)
+        scene.build_far_field()
+        scene.eval(dpos, dpos, 1, out=out)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    scene.set_profiling(True)
+    stage_acc = {}
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = lib.pppm_kernel_launches()
+    for i in range(args.steps):
+        flush.zero_()  # L2 flush outside the timed window
+        starts[i].record(stream)
+        step()
+        ends[i].record(stream)
+        st = scene.stage_times()  # synchronises; events bracket each stage
+        for k, v in st.items():
+            if v >= 0:
+                stage_acc.setdefault(k, []).append(v)
+    launches = lib.pppm_kernel_launches() - launches0
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    scene.set_profiling(False)
+    value = world * N * args.steps / (total_ms / 1000.0)
+
+    # end to end through the host entry point (pinned buffers)
+    hpos = torch.from_numpy(pos).pin_memory()
+    hal = torch.from_numpy(np.ascontiguousarray(al.T)).pin_memory()
+    hout = torch.empty((3, N), dtype=torch.float64).pin_memory()
+    for _ in range(2):
+        scene.solve_host(hpos, hal, None, None, 1, out_host=hout)
+    e2e_t = []
+    for _ in range(max(3, min(args.steps, 5))):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        scene.solve_host(hpos, hal, None, None, 1, out_host=hout)
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_s = statistics.median(e2e_t)
+    e2e_val = world * N / e2e_s
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_val = world * N / float(t.item())
+
+    # accuracy on a fixed 1% subsample (every 100th particle) vs the FP64 direct sum
+    sub = dpos[::100].contiguous()
+    u_gpu = out.t()[::100].cpu().numpy()
+    u_ref = pb.direct_sum_fp64(dpos, dal, sub, A_SMOOTH, sub, 1).cpu().numpy()
+    err = float(np.linalg.norm(u_gpu - u_ref) / np.linalg.norm(u_ref))
+    pairs = scene.count_pairs(dpos)
+
+    stages = {k: statistics.mean(v) for k, v in stage_acc.items()}
+    dom = max(stages, key=stages.get)
+    dom_ms = stages[dom]
+    hbm_peak, peak_src = measured_peaks()
+    roof = None
+    if dom == "eval":
+        flops = 30.0 * pairs
+        achieved = flops / (dom_ms / 1000.0) / 1e12
+        roof = {"kernel": "eval_kernel (interpolation + near field)", "bound": "fp32",
+                "achieved": achieved, "peak": FP32_PEAK_TFLOPS, "unit": "TFLOP/s",
+                "frac": achieved / FP32_PEAK_TFLOPS, "traffic": read_profile_traffic(),
+                "peak_source": "nominal FP32 (148 SM x 128 lanes x 2 x 1965 MHz); no measured FP32 peak",
+                "algorithmic": f"30 flops x {pairs} near-field pairs per launch", "launch_ms": dom_ms}
+    else:
+        roof = {"kernel": dom, "bound": "hbm", "achieved": None, "peak": hbm_peak, "unit": "GB/s",
+                "frac": None, "traffic": None, "peak_source": peak_src, "launch_ms": dom_ms}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_sample_rate(pos, al, args.grid)
+            cpu.pop("seconds", None)
+        except Exception as exc:  # the baseline is a report, not a gate
+            cpu = {"value": None, "unit": UNIT, "cores": None, "kind": "port", "sample": f"failed: {exc}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (multigrid residual/accumulation f64)",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "grid": args.grid, "particles": N, "eval_points": N,
+                       "parallelism": "replicas" if world > 1 else "single scene",
+                       "l2": "flushed between timed steps (512 MB write)"},
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": N * 16 + 3 * N * 8,
+                    "d2h_bytes_per_step": 3 * N * 8},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "stages_ms": stages,
+            "err_vs_direct_fp64": err,
+            "near_field_pairs": pairs,
+        }
+        print(json.dumps(line), flush=True)
+    scene.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+    run_b200(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

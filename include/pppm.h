@@ -154,6 +154,17 @@ pppm_status pppm_get_stats(pppm_scene *s, uint64_t *pairs, int32_t *mg_cycles,
 pppm_status pppm_count_pairs(pppm_scene *s, uint32_t M, const float *eval_a4_dev,
                              uint64_t *pairs);
 
+/* Per-stage timing with CUDA events on the scene stream (off by default;
+ * no reference counterpart — the reference prints no timings).  Stages:
+ * 0 domain, 1 vort_sort, 2 cells_reorder, 3 p2m, 4 multigrid, 5 farfield,
+ * 6 eval_sort, 7 eval.  pppm_get_stage_times synchronises the stream and
+ * writes the last recorded duration of each stage in ms (-1 = not run). */
+pppm_status pppm_scene_set_profiling(pppm_scene *s, int on);
+const char *pppm_stage_name(int stage);
+pppm_status pppm_get_stage_times(pppm_scene *s, double *ms, int cap, int *count);
+/* Number of kernels this library has launched in the process so far. */
+uint64_t pppm_kernel_launches(void);
+
 /* ---- multigrid surface: gf::MultiGridSolver3DPeriod_double
  * (MG/MultiGrid.h:188-209, MG/MultiGrid.cpp:128-250) ---------------------- */
 typedef struct pppm_mg pppm_mg;

@@ -1,0 +1,288 @@
+// pppm_compat.hpp — C++ classes with the reference's interface for the PPPM
+// path, implemented over the C ABI in pppm.h (header only; link
+// libpppm_b200.so).
+//
+//   BiotSavartSolver              hybridFastSummation/BiotSavartSolver.h:16-38
+//   ParticleManager               particle_hash/SpaceHashClass.h:10-84
+//   MultiGridSolver3DPeriod_double multigrid/MultiGrid.h:188-209
+//
+// The reference passes gf::gf_GpuArray<T> objects (multigrid/gfGpuArray.h:
+// 26-89); DeviceArray<T> below keeps the two members its call sites use,
+// getDevicePtr() and getSize(), over caller-owned device memory.  Methods
+// return bool like the reference, but false on failure (the reference always
+// returns true and exits on CUDA errors); lastError() gives the reason.
+#pragma once
+
+#include <cstdint>
+#include <cstring>
+#include <string>
+
+#include "pppm.h"
+
+namespace pppm_compat {
+
+typedef unsigned int uint;
+
+struct float4_ { float x, y, z, w; };
+struct double4_ { double x, y, z, w; };
+
+template <typename T>
+class DeviceArray {
+public:
+    DeviceArray() = default;
+    DeviceArray(T *dev, size_t n) : ptr_(dev), n_(n) {}
+    T *getDevicePtr() const { return ptr_; }
+    size_t getSize() const { return n_; }
+    size_t typeSize() const { return sizeof(T); }
+
+private:
+    T *ptr_ = nullptr;
+    size_t n_ = 0;
+};
+
+typedef DeviceArray<float4_> GpuArrayf4;
+typedef DeviceArray<double> GpuArrayd;
+
+inline std::string lastError() { return pppm_last_error(); }
+
+class BiotSavartSolver {
+public:
+    BiotSavartSolver() = default;
+    ~BiotSavartSolver() { shutdown(); }
+    BiotSavartSolver(const BiotSavartSolver &) = delete;
+    BiotSavartSolver &operator=(const BiotSavartSolver &) = delete;
+
+    // HFS/BiotSavartSolverImp.cpp:44-229.  Cubic grids only; isVIC (mesh-only
+    // velocities) is not part of this path and is rejected.
+    bool initializeSolver(uint gdx, uint gdy, uint gdz, bool isVIC, int K, uint M, uint N,
+                          void *stream = nullptr) {
+        if (gdx != gdy || gdy != gdz || isVIC) return false;
+        if (scene_ && gdx == n_ && K == K_) {
+            M_ = M;
+            N_ = N;
+            return true;
+        }
+        shutdown();
+        pppm_params p;
+        pppm_params_default(&p);
+        p.n = gdx;
+        p.K = K;
+        if (pppm_scene_create(&p, N ? N : 1, M ? M : 1, stream, &scene_) != PPPM_OK) return false;
+        n_ = gdx;
+        K_ = K;
+        M_ = M;
+        N_ = N;
+        return true;
+    }
+
+    // HFS/BiotSavartSolverImp.cpp:318-360
+    bool setVortParameter(uint n, GpuArrayf4 *pos, GpuArrayd *omega[]) {
+        N_ = n;
+        vort_[0] = omega[0]->getDevicePtr();
+        vort_[1] = omega[1]->getDevicePtr();
+        vort_[2] = omega[2]->getDevicePtr();
+        return pppm_set_vortices(scene_, n, reinterpret_cast<const float *>(pos->getDevicePtr()), vort_[0],
+                                 vort_[1], vort_[2]) == PPPM_OK;
+    }
+
+    // HFS/BiotSavartSolverImp.cpp:266-316
+    bool setEvalParameter(uint m, GpuArrayf4 *pos) {
+        M_ = m;
+        eval_ = reinterpret_cast<const float *>(pos->getDevicePtr());
+        return ensure_u(m);
+    }
+
+    // HFS/BiotSavartSolverImp.cpp:756-816
+    void computeFarFieldBuffer() { ok_ = pppm_build_far_field(scene_) == PPPM_OK; }
+
+    // HFS/BiotSavartSolverImp.cpp:410-516
+    bool evaluateVelocity(GpuArrayf4 *another_end, uint is_segment) {
+        const float *eb = another_end ? reinterpret_cast<const float *>(another_end->getDevicePtr()) : nullptr;
+        return pppm_eval(scene_, M_, eval_, eb, (int)is_segment, U_[0], U_[1], U_[2]) == PPPM_OK;
+    }
+
+    double *getU(int i) { return U_[i]; }
+    const double *getVort(int i) { return vort_[i]; }
+
+    // HFS/BiotSavartSolverImp.cpp:733-753: hash + reorder; the sorted copies are
+    // produced on request by getSortPos / getSortVort.
+    void sortVort() {
+        ok_ = pppm_build_far_field(scene_) == PPPM_OK;
+        sorted_valid_ = false;
+    }
+    float4_ *getSortPos() { return refresh_sorted() ? spos_ : nullptr; }
+    double *getSortVort(int i) { return refresh_sorted() ? salpha_[i] : nullptr; }
+
+    const uint32_t *getVortStartTable() {
+        const uint32_t *s = nullptr, *e = nullptr;
+        pppm_get_cell_tables(scene_, &s, &e);
+        return s;
+    }
+    const uint32_t *getVortEndTable() {
+        const uint32_t *s = nullptr, *e = nullptr;
+        pppm_get_cell_tables(scene_, &s, &e);
+        return e;
+    }
+    double getCellh() {
+        double o[3], L = 0, h = 0;
+        pppm_get_domain(scene_, o, &L, &h);
+        return h;
+    }
+    double4_ getOrigin() {
+        double o[3] = {0, 0, 0}, L = 0, h = 0;
+        pppm_get_domain(scene_, o, &L, &h);
+        return double4_{o[0], o[1], o[2], 0.0};
+    }
+
+    // HFS/BiotSavartSolverImp.cpp:230-264
+    bool shutdown() {
+        if (scene_) pppm_scene_destroy(scene_);
+        scene_ = nullptr;
+        free_buffers();
+        return true;
+    }
+
+    bool lastOk() const { return ok_; }
+    pppm_scene *scene() { return scene_; }
+
+private:
+    // Output arrays are owned by the solver, as m_particle_U is in the
+    // reference; device memory comes from the scene's allocator through a
+    // direct-sum-free path: plain cudaMalloc via the runtime the library uses.
+    bool ensure_u(uint m);
+    bool refresh_sorted();
+    void free_buffers();
+
+    pppm_scene *scene_ = nullptr;
+    uint n_ = 0, M_ = 0, N_ = 0, capU_ = 0, capS_ = 0;
+    int K_ = 1;
+    const float *eval_ = nullptr;
+    const double *vort_[3] = {nullptr, nullptr, nullptr};
+    double *U_[3] = {nullptr, nullptr, nullptr};
+    float4_ *spos_ = nullptr;
+    double *salpha_[3] = {nullptr, nullptr, nullptr};
+    bool sorted_valid_ = false;
+    bool ok_ = true;
+};
+
+class MultiGridSolver3DPeriod_double {
+public:
+    ~MultiGridSolver3DPeriod_double() { m_FinalMemoryEachLevel(); }
+    // MG/MultiGrid.h:129-139
+    void m_InitialSystem(int gridx, int gridy, int gridz, void *stream = nullptr) {
+        m_FinalMemoryEachLevel();
+        if (gridx == gridy && gridy == gridz) pppm_mg_create((uint32_t)gridx, stream, &mg_);
+    }
+    void m_FinalMemoryEachLevel() {
+        if (mg_) pppm_mg_destroy(mg_);
+        mg_ = nullptr;
+    }
+    // MG/MultiGrid.cpp:202-250 (tol ignored in the reference schedule)
+    void m_FullMultiGrid(GpuArrayd *x, GpuArrayd *b, double tol, double &residual) {
+        double rr = -1.0;
+        pppm_mg_full_multigrid(mg_, x->getDevicePtr(), b->getDevicePtr(), PPPM_MG_REFERENCE, tol, 1, &rr);
+        residual = rr;
+    }
+
+private:
+    pppm_mg *mg_ = nullptr;
+};
+
+class ParticleManager {
+public:
+    ~ParticleManager() { endSpatialHash(); }
+    // PH/SpaceHashClassImp.cpp:47-69
+    void initSpatialHash(uint numParticles, uint dimx, uint dimy, uint dimz, void *stream = nullptr) {
+        endSpatialHash();
+        if (dimx == dimy && dimy == dimz) pppm_hasher_create(numParticles, dimx, stream, &h_);
+        n_ = dimx;
+        h_cell_ = 1.0f / (float)dimx;
+    }
+    void endSpatialHash() {
+        if (h_) pppm_hasher_destroy(h_);
+        h_ = nullptr;
+    }
+    // PH/SpaceHashClass.h:46-54
+    void setSpatialHashGrid(uint size0, float h, const float bbmin[3], uint numParticles) {
+        n_ = size0;
+        h_cell_ = h;
+        origin_[0] = bbmin[0];
+        origin_[1] = bbmin[1];
+        origin_[2] = bbmin[2];
+        N_ = numParticles;
+    }
+    void setHashParam() {}  // parameters travel with each call
+    void doSpatialHash(float4_ *pos, uint numParticles) {
+        pppm_hasher_run(h_, numParticles, reinterpret_cast<const float *>(pos), h_cell_, origin_);
+    }
+    void reorderData(uint numParticles, void *data, void *dataReorder, uint stride, uint precision) {
+        pppm_hasher_reorder(h_, numParticles, data, dataReorder, stride, precision);
+    }
+    void deorderData(uint numParticles, void *data, void *dataReorder, uint stride, uint precision) {
+        pppm_hasher_deorder(h_, numParticles, data, dataReorder, stride, precision);
+    }
+    const uint32_t *getHashTable() { return table(0); }
+    const uint32_t *getStartTable() { return table(2); }
+    const uint32_t *getEndTable() { return table(3); }
+    float getCellSize() const { return h_cell_; }
+
+private:
+    const uint32_t *table(int which) {
+        const uint32_t *t[4] = {nullptr, nullptr, nullptr, nullptr};
+        pppm_hasher_tables(h_, &t[0], &t[1], &t[2], &t[3]);
+        return t[which];
+    }
+    pppm_hasher *h_ = nullptr;
+    uint n_ = 0, N_ = 0;
+    float h_cell_ = 0.f;
+    float origin_[3] = {0.f, 0.f, 0.f};
+};
+
+}  // namespace pppm_compat
+
+// Out-of-line members that allocate: kept here so the header stays self
+// contained; they use the CUDA runtime the application already links.
+#include <cuda_runtime.h>
+
+namespace pppm_compat {
+
+inline bool BiotSavartSolver::ensure_u(uint m) {
+    if (m <= capU_) return true;
+    for (int c = 0; c < 3; c++) {
+        cudaFree(U_[c]);
+        U_[c] = nullptr;
+        if (cudaMalloc(&U_[c], sizeof(double) * (m ? m : 1)) != cudaSuccess) return false;
+    }
+    capU_ = m;
+    return true;
+}
+
+inline bool BiotSavartSolver::refresh_sorted() {
+    if (sorted_valid_) return true;
+    if (N_ > capS_) {
+        cudaFree(spos_);
+        spos_ = nullptr;
+        for (int c = 0; c < 3; c++) { cudaFree(salpha_[c]); salpha_[c] = nullptr; }
+        if (cudaMalloc(&spos_, sizeof(float4_) * N_) != cudaSuccess) return false;
+        for (int c = 0; c < 3; c++)
+            if (cudaMalloc(&salpha_[c], sizeof(double) * N_) != cudaSuccess) return false;
+        capS_ = N_;
+    }
+    sorted_valid_ = pppm_get_sorted_vortices(scene_, reinterpret_cast<float *>(spos_), salpha_[0], salpha_[1],
+                                             salpha_[2]) == PPPM_OK;
+    return sorted_valid_;
+}
+
+inline void BiotSavartSolver::free_buffers() {
+    for (int c = 0; c < 3; c++) {
+        cudaFree(U_[c]);
+        U_[c] = nullptr;
+        cudaFree(salpha_[c]);
+        salpha_[c] = nullptr;
+    }
+    cudaFree(spos_);
+    spos_ = nullptr;
+    capU_ = capS_ = 0;
+}
+
+}  // namespace pppm_compat

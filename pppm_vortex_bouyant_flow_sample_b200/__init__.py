@@ -192,6 +192,17 @@ class Scene:
         check(self._lib.pppm_get_stats(self._h, C.byref(pairs), C.byref(cyc), C.byref(rr)), "pppm_get_stats")
         return {"mg_cycles": cyc.value, "mg_relres": rr.value}
 
+    def set_profiling(self, on: bool = True):
+        check(self._lib.pppm_scene_set_profiling(self._h, int(on)), "pppm_scene_set_profiling")
+
+    def stage_times(self) -> dict:
+        """Last recorded duration (ms) of each stage; -1 for stages not run."""
+        from ._lib import STAGES
+        ms = (C.c_double * 16)()
+        cnt = C.c_int()
+        check(self._lib.pppm_get_stage_times(self._h, ms, 16, C.byref(cnt)), "pppm_get_stage_times")
+        return {STAGES[i]: ms[i] for i in range(cnt.value)}
+
     def count_pairs(self, eval_a: torch.Tensor) -> int:
         ea = _pos4(eval_a)
         pairs = C.c_uint64()

@@ -39,7 +39,7 @@ def sources():
 
 
 def _deps():
-    return sources() + glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(INCLUDE, "*.h")) \
+    return sources() + glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.map")) + glob.glob(os.path.join(INCLUDE, "*.h")) \
         + glob.glob(os.path.join(INCLUDE, "*.hpp")) + [os.path.abspath(__file__)]
 
 
@@ -71,7 +71,8 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
     with cf.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose_ptxas), srcs))
     tmp = LIB + ".tmp"
-    cmd = [_nvcc()] + ARCH + ["-shared", "--cudart", "static", "-o", tmp] + objs
+    cmd = [_nvcc()] + ARCH + ["-shared", "--cudart", "static", "-Xlinker",
+                              "--version-script=" + os.path.join(CSRC, "exports.map"), "-o", tmp] + objs
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

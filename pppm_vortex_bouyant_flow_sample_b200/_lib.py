@@ -25,7 +25,9 @@ EXPORTED = (
     "pppm_get_stats", "pppm_count_pairs", "pppm_mg_create", "pppm_mg_destroy",
     "pppm_mg_full_multigrid", "pppm_hasher_create", "pppm_hasher_destroy", "pppm_hasher_run",
     "pppm_hasher_tables", "pppm_hasher_reorder", "pppm_hasher_deorder", "pppm_direct_sum_fp64",
+    "pppm_scene_set_profiling", "pppm_stage_name", "pppm_get_stage_times", "pppm_kernel_launches",
 )
+STAGES = ("domain", "vort_sort", "cells_reorder", "p2m", "multigrid", "farfield", "eval_sort", "eval")
 
 
 class PppmParams(C.Structure):
@@ -100,6 +102,10 @@ def load(build_if_missing: bool = True):
         "pppm_hasher_reorder": (st, [vp, u32, vp, vp, u32, u32]),
         "pppm_hasher_deorder": (st, [vp, u32, vp, vp, u32, u32]),
         "pppm_direct_sum_fp64": (st, [u32, vp, vp, vp, vp, u32, vp, vp, C.c_int, C.c_double, vp, vp, vp, vp]),
+        "pppm_scene_set_profiling": (st, [vp, C.c_int]),
+        "pppm_stage_name": (C.c_char_p, [C.c_int]),
+        "pppm_get_stage_times": (st, [vp, C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_int)]),
+        "pppm_kernel_launches": (C.c_uint64, []),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -1,5 +1,6 @@
 // C ABI of the PPPM path: scene lifecycle, the BiotSavartSolver entry points,
 // the standalone multigrid object, and the FP64 direct sum.
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -139,6 +140,10 @@ cudaError_t alloc_grid_side(pppm_scene *s) {
 
 void destroy_scene(pppm_scene *s) {
     if (!s) return;
+    for (int i = 0; i < 16; i++) {
+        if (s->ev_begin[i]) cudaEventDestroy(s->ev_begin[i]);
+        if (s->ev_end[i]) cudaEventDestroy(s->ev_end[i]);
+    }
     free_vortex_side(s);
     free_eval_side(s);
     cudaFree(s->hist);
@@ -280,12 +285,25 @@ extern "C" pppm_status pppm_build_far_field(pppm_scene *s) {
         snprintf(g_err, sizeof(g_err), "pppm_build_far_field: call pppm_set_vortices first");
         return PPPM_ERR_STATE;
     }
-    cudaError_t e = pppm::launch_bbox_and_params(s);
-    if (e == cudaSuccess) e = pppm::launch_hash_sort(s, s->vpos, s->N, s->vkey, s->vidx, &s->vsorted_key, &s->vsorted_idx);
-    if (e == cudaSuccess) e = pppm::launch_cells_reorder(s);
-    if (e == cudaSuccess) e = pppm::launch_p2m(s);
-    if (e == cudaSuccess) e = pppm::run_multigrid(s);
-    if (e == cudaSuccess) e = pppm::launch_farfield(s);
+    using namespace pppm;
+    prof_begin(s, kStageDomain);
+    cudaError_t e = launch_bbox_and_params(s);
+    prof_end(s, kStageDomain);
+    prof_begin(s, kStageVortSort);
+    if (e == cudaSuccess) e = launch_hash_sort(s, s->vpos, s->N, s->vkey, s->vidx, &s->vsorted_key, &s->vsorted_idx);
+    prof_end(s, kStageVortSort);
+    prof_begin(s, kStageCells);
+    if (e == cudaSuccess) e = launch_cells_reorder(s);
+    prof_end(s, kStageCells);
+    prof_begin(s, kStageP2M);
+    if (e == cudaSuccess) e = launch_p2m(s);
+    prof_end(s, kStageP2M);
+    prof_begin(s, kStageMG);
+    if (e == cudaSuccess) e = run_multigrid(s);
+    prof_end(s, kStageMG);
+    prof_begin(s, kStageFar);
+    if (e == cudaSuccess) e = launch_farfield(s);
+    prof_end(s, kStageFar);
     if (e != cudaSuccess) return cuda_fail("pppm_build_far_field", e);
     s->far_ready = true;
     return PPPM_OK;
@@ -436,6 +454,61 @@ extern "C" pppm_status pppm_get_grid(pppm_scene *s, int which, const void **ptr)
     return PPPM_OK;
 }
 
+namespace pppm {
+
+static std::atomic<unsigned long long> g_launches{0};
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+const char *stage_name(int i) {
+    static const char *names[kNumStages] = {"domain", "vort_sort", "cells_reorder", "p2m",
+                                            "multigrid", "farfield", "eval_sort", "eval"};
+    return (i >= 0 && i < kNumStages) ? names[i] : "";
+}
+
+void prof_begin(pppm_scene *s, int stage) {
+    if (!s->profiling) return;
+    if (!s->ev_begin[stage]) {
+        cudaEventCreate(&s->ev_begin[stage]);
+        cudaEventCreate(&s->ev_end[stage]);
+    }
+    cudaEventRecord(s->ev_begin[stage], s->stream);
+}
+
+void prof_end(pppm_scene *s, int stage) {
+    if (!s->profiling) return;
+    cudaEventRecord(s->ev_end[stage], s->stream);
+    s->ev_used[stage] = true;
+}
+
+}  // namespace pppm
+
+extern "C" pppm_status pppm_scene_set_profiling(pppm_scene *s, int on) {
+    if (!s) return PPPM_ERR_INVALID;
+    s->profiling = on != 0;
+    for (int i = 0; i < 16; i++) s->ev_used[i] = false;
+    return PPPM_OK;
+}
+
+extern "C" const char *pppm_stage_name(int i) { return pppm::stage_name(i); }
+
+extern "C" uint64_t pppm_kernel_launches(void) { return pppm::launch_count(); }
+
+extern "C" pppm_status pppm_get_stage_times(pppm_scene *s, double *ms, int cap, int *count) {
+    if (!s || !ms || cap < pppm::kNumStages) return PPPM_ERR_INVALID;
+    cudaError_t e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return cuda_fail("pppm_get_stage_times", e);
+    for (int i = 0; i < pppm::kNumStages; i++) {
+        ms[i] = -1.0;
+        if (s->profiling && s->ev_used[i]) {
+            float t = 0.f;
+            if (cudaEventElapsedTime(&t, s->ev_begin[i], s->ev_end[i]) == cudaSuccess) ms[i] = t;
+        }
+    }
+    if (count) *count = pppm::kNumStages;
+    return PPPM_OK;
+}
+
 extern "C" pppm_status pppm_get_stats(pppm_scene *s, uint64_t *pairs, int32_t *mg_cycles, double *mg_relres) {
     if (!s) return PPPM_ERR_INVALID;
     if (pairs) {
@@ -524,6 +597,7 @@ extern "C" pppm_status pppm_mg_full_multigrid(pppm_mg *m, double *x, const doubl
     P.vort = nullptr;
     P.P = nullptr;
     const size_t C = P.lv[0].cells;
+    ::pppm::note_launch();
     to_float_kernel<<<(unsigned)((C + 255) / 256), 256, 0, P.st>>>(b, P.lv[0].b, C);
     cudaError_t e = cudaGetLastError();
     int cyc = 0;
@@ -597,6 +671,7 @@ extern "C" pppm_status pppm_direct_sum_fp64(uint32_t N, const float *vp, const d
         return PPPM_ERR_INVALID;
     }
     if (M == 0 || N == 0) return PPPM_OK;
+    ::pppm::note_launch();
     direct_sum_kernel<<<(M + kDSThreads - 1) / kDSThreads, kDSThreads, 0, (cudaStream_t)stream>>>(
         N, reinterpret_cast<const float4 *>(vp), ax, ay, az, M, reinterpret_cast<const float4 *>(ea),
         reinterpret_cast<const float4 *>(eb), is_segment, a, u, v, w);

@@ -18,8 +18,10 @@
 //     (alpha x d) * phi((r/a)^3) / (4 pi a^3) with phi(t) = (1 - e^-t)/t,
 //     which equals (1 - e^-(r/a)^3) / (4 pi r^3); pairs with r = 0, or (for
 //     segments) a zero distance to the other end, are skipped.
-// Pair arithmetic is FP32; phi uses its Taylor series below t = 0.5 (no
-// cancellation) and 1 - exp(-t) above.
+// Pair arithmetic is FP32 (r from rsqrt, ~1 ulp); phi uses its Taylor series
+// below t = 0.5 (no cancellation) and (1 - exp(-t)) / t above.
+#include <climits>
+
 #include "pppm_internal.cuh"
 
 namespace pppm {
@@ -29,9 +31,8 @@ namespace {
 constexpr int kEvalThreads = 128;
 
 __device__ __forceinline__ float phi_smooth(float t) {
-    if (t < 0.5f) {
-        float p = 1.0f / 362880.0f;
-        p = fmaf(p, t, -1.0f / 40320.0f);
+    if (t < 0.5f) {  // truncation error < t^8/9! <= 1.1e-8 relative
+        float p = -1.0f / 40320.0f;
         p = fmaf(p, t, 1.0f / 5040.0f);
         p = fmaf(p, t, -1.0f / 720.0f);
         p = fmaf(p, t, 1.0f / 120.0f);
@@ -40,7 +41,7 @@ __device__ __forceinline__ float phi_smooth(float t) {
         p = fmaf(p, t, -0.5f);
         return fmaf(p, t, 1.0f);
     }
-    return (1.0f - __expf(-t)) / t;
+    return __fdividef(1.0f - __expf(-t), t);
 }
 
 __device__ __forceinline__ float3 rel_pos(float4 p, const DevParams *__restrict__ P) {
@@ -48,80 +49,155 @@ __device__ __forceinline__ float3 rel_pos(float4 p, const DevParams *__restrict_
                        (float)((double)p.z - P->origin[2]));
 }
 
-__global__ void __launch_bounds__(kEvalThreads)
-eval_kernel(const uint32_t *__restrict__ eidx, uint32_t M, const float4 *__restrict__ eval_a,
-            const float4 *__restrict__ eval_b, int is_segment, const float *__restrict__ far,
+// Evaluation order: NGP cell * 8 + octant of the point inside its cell
+// (points outside the grid last).  A warp of consecutive points then shares
+// one cell octant, whose near-field boxes span 2K+2 cells per axis instead of
+// the reference's 2K+3.  The order is internal: results return in caller order.
+__global__ void eval_keys_kernel(const float4 *__restrict__ eval_a, uint32_t M, const DevParams *__restrict__ P,
+                                 uint32_t *__restrict__ key, uint32_t *__restrict__ idx) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= M) return;
+    const float3 r = rel_pos(eval_a[t], P);
+    const double invh = P->invh;
+    const uint32_t n = P->n;
+    const double qx = (double)r.x * invh, qy = (double)r.y * invh, qz = (double)r.z * invh;
+    const double fx = floor(qx), fy = floor(qy), fz = floor(qz);
+    const double dn = (double)n;
+    uint32_t k = 8u * n * n * n;
+    if (fx >= 0.0 && fx < dn && fy >= 0.0 && fy < dn && fz >= 0.0 && fz < dn) {
+        const uint32_t oct = (qx - fx >= 0.5 ? 1u : 0u) | (qy - fy >= 0.5 ? 2u : 0u) | (qz - fz >= 0.5 ? 4u : 0u);
+        k = ((((uint32_t)fz * n + (uint32_t)fy) * n + (uint32_t)fx) << 3) | oct;
+    }
+    key[t] = k;
+    idx[t] = t;
+}
+
+struct PairAcc {
+    float x = 0.f, y = 0.f, z = 0.f;
+    unsigned long long n = 0;
+};
+
+// Near-field sum over one hash cell's vortices for one point.  SEG: test the
+// segment's other end; COUNT: count the pairs inside the box.
+template <bool SEG, bool COUNT>
+__device__ __forceinline__ void cell_pairs(const float4 *__restrict__ vrec, const float4 *__restrict__ valf,
+                                           uint32_t ps, uint32_t pe, bool lane_ok, const float3 ra, const float3 rb,
+                                           float cr, float inv_a3, float inv4pia3, PairAcc &acc) {
+    for (uint32_t p = ps; p < pe; p++) {
+        const float4 r = vrec[p];
+        const float dx = ra.x - r.x, dy = ra.y - r.y, dz = ra.z - r.z;
+        if (!(lane_ok && fmaxf(fabsf(dx), fmaxf(fabsf(dy), fabsf(dz))) <= cr)) continue;
+        if (COUNT) acc.n++;
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        bool skip = r2 < 1e-24f;
+        if (SEG) {
+            const float ex = rb.x - r.x, ey = rb.y - r.y, ez = rb.z - r.z;
+            skip |= fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < 1e-24f;
+        }
+        if (skip) continue;
+        const float rr = r2 * rsqrtf(r2);  // r2 >= 1e-24 here
+        const float coeff = phi_smooth(r2 * rr * inv_a3) * inv4pia3;
+        const float4 al = valf[p];
+        acc.x = fmaf(al.y * dz - al.z * dy, coeff, acc.x);
+        acc.y = fmaf(al.z * dx - al.x * dz, coeff, acc.y);
+        acc.z = fmaf(al.x * dy - al.y * dx, coeff, acc.z);
+    }
+}
+
+constexpr int kUniformMaxCells = 216;  // warp-uniform walk up to 6^3 cells
+
+// SEG: is_segment == 1 with a distinct other-end array (with eval_b == eval_a
+// the other-end test is the r = 0 test itself, so SEG is off).
+template <bool SEG, bool COUNT>
+__global__ void eval_kernel(const uint32_t *__restrict__ eidx, uint32_t M, const float4 *__restrict__ eval_a,
+            const float4 *__restrict__ eval_b, const float *__restrict__ far,
             const uint32_t *__restrict__ start, const uint32_t *__restrict__ end, const float4 *__restrict__ vrec,
             const float4 *__restrict__ valf, const DevParams *__restrict__ P, int n, int K,
             double *__restrict__ u, double *__restrict__ v, double *__restrict__ w, float *__restrict__ uf,
             unsigned long long *__restrict__ pair_count) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    unsigned long long pairs = 0;
-    if (s < M) {
-        const uint32_t q = eidx[s];
-        const float3 ra = rel_pos(eval_a[q], P);
-        float3 rb = make_float3(0.f, 0.f, 0.f);
-        if (is_segment == 1) rb = rel_pos(eval_b[q], P);
-        const double invh = P->invh;
-        const double qx = (double)ra.x * invh, qy = (double)ra.y * invh, qz = (double)ra.z * invh;
-        const int i = (int)floor(qx), j = (int)floor(qy), k = (int)floor(qz);
-        const uint32_t C = (uint32_t)n * n * n;
-        float ux = 0.f, uy = 0.f, uz = 0.f;
-        if (i >= 0 && i < n && j >= 0 && j < n && k >= 0 && k < n) {
-            const double tx = qx - 0.5, ty = qy - 0.5, tz = qz - 0.5;
-            const double fx0 = floor(tx), fy0 = floor(ty), fz0 = floor(tz);
-            const int i0 = (int)fx0, j0 = (int)fy0, k0 = (int)fz0;
-            const float fx = (float)(tx - fx0), fy = (float)(ty - fy0), fz = (float)(tz - fz0);
-            const float wx[2] = {1.f - fx, fx}, wy[2] = {1.f - fy, fy}, wz[2] = {1.f - fz, fz};
+    const bool act = s < M;
+    const uint32_t q = act ? eidx[s] : 0u;
+    float3 ra = make_float3(0.f, 0.f, 0.f), rb = make_float3(0.f, 0.f, 0.f);
+    if (act) {
+        ra = rel_pos(eval_a[q], P);
+        if (SEG) rb = rel_pos(eval_b[q], P);
+    }
+    const double invh = P->invh;
+    const double qx = (double)ra.x * invh, qy = (double)ra.y * invh, qz = (double)ra.z * invh;
+    const int i = (int)floor(qx), j = (int)floor(qy), k = (int)floor(qz);
+    const uint32_t C = (uint32_t)n * n * n;
+    float ux = 0.f, uy = 0.f, uz = 0.f;
+    if (act && i >= 0 && i < n && j >= 0 && j < n && k >= 0 && k < n) {
+        const double tx = qx - 0.5, ty = qy - 0.5, tz = qz - 0.5;
+        const double fx0 = floor(tx), fy0 = floor(ty), fz0 = floor(tz);
+        const int i0 = (int)fx0, j0 = (int)fy0, k0 = (int)fz0;
+        const float fx = (float)(tx - fx0), fy = (float)(ty - fy0), fz = (float)(tz - fz0);
 #pragma unroll
-            for (int c = 0; c < 8; c++) {
-                const int ii = i0 + (c & 1), jj = j0 + ((c >> 1) & 1), kk = k0 + (c >> 2);
-                if (ii < 0 || ii >= n || jj < 0 || jj >= n || kk < 0 || kk >= n) continue;
-                const float wgt = wx[c & 1] * wy[(c >> 1) & 1] * wz[c >> 2];
+        for (int c = 0; c < 8; c++) {
+            const int ii = i0 + (c & 1), jj = j0 + ((c >> 1) & 1), kk = k0 + (c >> 2);
+            const float wgt = ((c & 1) ? fx : 1.f - fx) * ((c & 2) ? fy : 1.f - fy) * ((c & 4) ? fz : 1.f - fz);
+            if (ii >= 0 && ii < n && jj >= 0 && jj < n && kk >= 0 && kk < n) {
                 const size_t g = ((size_t)kk * n + jj) * n + ii;
                 ux = fmaf(far[g], wgt, ux);
                 uy = fmaf(far[C + g], wgt, uy);
                 uz = fmaf(far[2 * (size_t)C + g], wgt, uz);
             }
         }
-        if (K >= 0) {
-            const float cr = P->cr_f;
-            const float inv_a3 = P->inv_a3_f, inv4pia3 = P->inv4pia3_f;
-            float px = 0.f, py = 0.f, pz = 0.f;
-            const int k_lo = max(k - K - 1, 0), k_hi = min(k + K + 1, n - 1);
-            const int j_lo = max(j - K - 1, 0), j_hi = min(j + K + 1, n - 1);
-            const int i_lo = max(i - K - 1, 0), i_hi = min(i + K + 1, n - 1);
-            for (int kk = k_lo; kk <= k_hi; kk++)
-                for (int jj = j_lo; jj <= j_hi; jj++)
-                    for (int ii = i_lo; ii <= i_hi; ii++) {
+    }
+    PairAcc acc;
+    if (K >= 0) {
+        const float cr = P->cr_f, inv_a3 = P->inv_a3_f, inv4pia3 = P->inv4pia3_f;
+        // The reference walks hash cells [i-K-1, i+K+1]^3.  Only cells that can
+        // hold a vortex inside the point's box are visited: the box spans
+        // (K+0.5) cells either side, widened by the hash/NGP rounding bound.
+        const double R = (double)K + 0.5 + P->prune_cells;
+        int lo[3], hi[3];
+        const double qq[3] = {qx, qy, qz};
+        const int cc[3] = {i, j, k};
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            lo[a] = max(max(cc[a] - K - 1, 0), (int)floor(qq[a] - R));
+            hi[a] = min(min(cc[a] + K + 1, n - 1), (int)floor(qq[a] + R));
+            if (!act || lo[a] > hi[a]) { lo[a] = INT_MAX; hi[a] = INT_MIN; }
+        }
+        int ulo[3], uhi[3];
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            ulo[a] = __reduce_min_sync(0xffffffffu, lo[a]);
+            uhi[a] = __reduce_max_sync(0xffffffffu, hi[a]);
+        }
+        long long vol = 1;
+#pragma unroll
+        for (int a = 0; a < 3; a++) vol *= (uhi[a] >= ulo[a]) ? (long long)(uhi[a] - ulo[a] + 1) : 0ll;
+        if (vol > 0 && vol <= kUniformMaxCells) {
+            // warp-uniform walk: every lane sees the same cell and vortex at once
+            for (int kk = ulo[2]; kk <= uhi[2]; kk++)
+                for (int jj = ulo[1]; jj <= uhi[1]; jj++)
+                    for (int ii = ulo[0]; ii <= uhi[0]; ii++) {
                         const uint32_t cell = ((uint32_t)kk * n + (uint32_t)jj) * n + (uint32_t)ii;
                         const uint32_t ps = start[cell];
                         if (ps == kEmpty) continue;
-                        const uint32_t pe = end[cell];
-                        for (uint32_t p = ps; p < pe; p++) {
-                            const float4 r = vrec[p];
-                            const float dx = ra.x - r.x, dy = ra.y - r.y, dz = ra.z - r.z;
-                            if (!(fabsf(dx) <= cr && fabsf(dy) <= cr && fabsf(dz) <= cr)) continue;
-                            pairs++;
-                            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                            bool skip = r2 < 1e-24f;
-                            if (is_segment == 1) {
-                                const float ex = rb.x - r.x, ey = rb.y - r.y, ez = rb.z - r.z;
-                                skip |= fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < 1e-24f;
-                            }
-                            if (skip) continue;
-                            const float rr = sqrtf(r2);
-                            const float coeff = phi_smooth(r2 * rr * inv_a3) * inv4pia3;
-                            const float4 al = valf[p];
-                            px = fmaf(al.y * dz - al.z * dy, coeff, px);
-                            py = fmaf(al.z * dx - al.x * dz, coeff, py);
-                            pz = fmaf(al.x * dy - al.y * dx, coeff, pz);
-                        }
+                        const bool lane_ok = ii >= lo[0] && ii <= hi[0] && jj >= lo[1] && jj <= hi[1] &&
+                                             kk >= lo[2] && kk <= hi[2];
+                        cell_pairs<SEG, COUNT>(vrec, valf, ps, end[cell], lane_ok, ra, rb, cr, inv_a3, inv4pia3, acc);
                     }
-            ux += px;
-            uy += py;
-            uz += pz;
+        } else if (act && lo[0] <= hi[0]) {
+            // scattered warp (points outside the grid, sparse regions): own walk
+            for (int kk = lo[2]; kk <= hi[2]; kk++)
+                for (int jj = lo[1]; jj <= hi[1]; jj++)
+                    for (int ii = lo[0]; ii <= hi[0]; ii++) {
+                        const uint32_t cell = ((uint32_t)kk * n + (uint32_t)jj) * n + (uint32_t)ii;
+                        const uint32_t ps = start[cell];
+                        if (ps == kEmpty) continue;
+                        cell_pairs<SEG, COUNT>(vrec, valf, ps, end[cell], true, ra, rb, cr, inv_a3, inv4pia3, acc);
+                    }
         }
+    }
+    if (act) {
+        ux += acc.x;
+        uy += acc.y;
+        uz += acc.z;
         if (u) {
             u[q] = (double)ux;
             v[q] = (double)uy;
@@ -133,7 +209,8 @@ eval_kernel(const uint32_t *__restrict__ eidx, uint32_t M, const float4 *__restr
             uf[3 * (size_t)q + 2] = uz;
         }
     }
-    if (pair_count) {
+    if (COUNT) {
+        unsigned long long pairs = acc.n;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
         if ((threadIdx.x & 31) == 0 && pairs) atomicAdd(pair_count, pairs);
@@ -145,12 +222,32 @@ eval_kernel(const uint32_t *__restrict__ eidx, uint32_t M, const float4 *__restr
 cudaError_t launch_eval(pppm_scene *s, const float4 *eval_a, const float4 *eval_b, int is_segment, uint32_t M,
                         double *u, double *v, double *w, float *uf, int count_pairs) {
     uint32_t *skey = nullptr, *sidx = nullptr;
-    PPPM_CUDA_TRY(launch_hash_sort(s, eval_a, M, s->ekey, s->eidx, &skey, &sidx));
+    prof_begin(s, kStageEvalSort);
+    ::pppm::note_launch();
+    eval_keys_kernel<<<(M + 255) / 256, 256, 0, s->stream>>>(eval_a, M, s->dparams, s->ekey[0], s->eidx[0]);
+    PPPM_CUDA_TRY(cudaGetLastError());
+    uint32_t bits = 1;
+    while (bits < 32 && (1ull << bits) <= 8ull * s->C) bits++;
+    PPPM_CUDA_TRY(radix_sort_pairs(s->stream, M, bits, s->ekey, s->eidx, s->hist, &skey, &sidx));
+    prof_end(s, kStageEvalSort);
     s->esorted_idx = sidx;
     if (count_pairs) PPPM_CUDA_TRY(cudaMemsetAsync(s->pair_count, 0, sizeof(unsigned long long), s->stream));
-    eval_kernel<<<(M + kEvalThreads - 1) / kEvalThreads, kEvalThreads, 0, s->stream>>>(
-        sidx, M, eval_a, eval_b, is_segment, s->far, s->cell_start, s->cell_end, s->vrec, s->valf, s->dparams,
-        (int)s->n, s->prm.K, u, v, w, uf, count_pairs ? s->pair_count : nullptr);
+    prof_begin(s, kStageEval);
+    ::pppm::note_launch();
+    const bool seg = (is_segment == 1) && (eval_b != eval_a);
+    const unsigned grid = (M + kEvalThreads - 1) / kEvalThreads;
+    unsigned long long *pc = count_pairs ? s->pair_count : nullptr;
+#define PPPM_EVAL_ARGS sidx, M, eval_a, eval_b, s->far, s->cell_start, s->cell_end, s->vrec, s->valf, s->dparams, \
+                       (int)s->n, s->prm.K, u, v, w, uf, pc
+    if (seg) {
+        if (count_pairs) eval_kernel<true, true><<<grid, kEvalThreads, 0, s->stream>>>(PPPM_EVAL_ARGS);
+        else eval_kernel<true, false><<<grid, kEvalThreads, 0, s->stream>>>(PPPM_EVAL_ARGS);
+    } else {
+        if (count_pairs) eval_kernel<false, true><<<grid, kEvalThreads, 0, s->stream>>>(PPPM_EVAL_ARGS);
+        else eval_kernel<false, false><<<grid, kEvalThreads, 0, s->stream>>>(PPPM_EVAL_ARGS);
+    }
+#undef PPPM_EVAL_ARGS
+    prof_end(s, kStageEval);
     return cudaGetLastError();
 }
 

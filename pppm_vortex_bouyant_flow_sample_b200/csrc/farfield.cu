@@ -124,6 +124,7 @@ curl_only_kernel(const double *__restrict__ psi, float *__restrict__ far, const 
 
 cudaError_t launch_farfield(pppm_scene *s) {
     const unsigned blocks = (s->C + kFFThreads - 1) / kFFThreads;
+    ::pppm::note_launch();
     if (s->prm.K >= 0)
         farfield_kernel<<<blocks, kFFThreads, 0, s->stream>>>(s->psi, s->vort, s->far, s->dparams, (int)s->n,
                                                               s->prm.K);

@@ -26,7 +26,6 @@ constexpr int kRsThreads = 256;
 constexpr int kRsItems = 16;
 constexpr int kRsTile = kRsThreads * kRsItems;
 constexpr int kRsWarps = kRsThreads / 32;
-constexpr int kScanThreads = 1024;
 
 __global__ void bbox_partial_kernel(const float4 *__restrict__ pos, uint32_t N,
                                     float *__restrict__ partial, int nblocks) {
@@ -76,17 +75,18 @@ __global__ void params_kernel(const float *__restrict__ partial, int nblocks, pp
         origin[1] = prm.fixed_origin[1];
         origin[2] = prm.fixed_origin[2];
         L = prm.fixed_length;
-    } else {
-        double mn[3], mx[3];
-        for (int a = 0; a < 3; a++) {
-            float lo = partial[a * nblocks], hi = partial[(3 + a) * nblocks];
-            for (int b = 1; b < nblocks; b++) {
-                lo = fminf(lo, partial[a * nblocks + b]);
-                hi = fmaxf(hi, partial[(3 + a) * nblocks + b]);
-            }
-            mn[a] = lo;
-            mx[a] = hi;
+    }
+    double mn[3], mx[3];
+    for (int a = 0; a < 3; a++) {
+        float lo = partial[a * nblocks], hi = partial[(3 + a) * nblocks];
+        for (int b = 1; b < nblocks; b++) {
+            lo = fminf(lo, partial[a * nblocks + b]);
+            hi = fmaxf(hi, partial[(3 + a) * nblocks + b]);
         }
+        mn[a] = lo;
+        mx[a] = hi;
+    }
+    if (prm.domain_mode != PPPM_DOMAIN_FIXED) {
         // HFS/BiotSavartSolverImp.cpp:399-406
         L = 3 * fmax(fmax(mx[0] - mn[0], mx[1] - mn[1]), mx[2] - mn[2]);
         for (int a = 0; a < 3; a++) {
@@ -115,6 +115,16 @@ __global__ void params_kernel(const float *__restrict__ partial, int nblocks, pp
     const double a = prm.a;
     P->inv_a3_f = (float)(1.0 / (a * a * a));
     P->inv4pia3_f = (float)(1.0 / (kFourPi * a * a * a));
+    // The FP32 hash coordinate fl(fl(p - o_f) / h_f) and the FP64 NGP coordinate
+    // fl32(p - o) / h differ by at most a few float roundings of |p| + |o| over h;
+    // 2^-20 covers them with a factor > 4 to spare.  The box test adds the
+    // rounding of one float subtraction of relative coordinates.
+    double pmax = 0.0, omax = 0.0;
+    for (int a = 0; a < 3; a++) {
+        pmax = fmax(pmax, fmax(fabs(mn[a]), fabs(mx[a])));
+        omax = fmax(omax, fabs(origin[a]));
+    }
+    P->prune_cells = (h > 0.0) ? ldexp(pmax + omax + L, -20) / h + ldexp((double)prm.K + 0.5, -20) + 1e-6 : 1.0;
     P->n = n;
     P->K = prm.K;
 }
@@ -166,40 +176,45 @@ radix_upsweep_kernel(const uint32_t *__restrict__ keys, uint32_t N, int shift, u
     hist[threadIdx.x * gridDim.x + blockIdx.x] = cnt[threadIdx.x];
 }
 
-// Exclusive scan of `total` counters in one block.
-__global__ void __launch_bounds__(kScanThreads) radix_scan_kernel(uint32_t *__restrict__ hist, uint32_t total) {
-    __shared__ uint32_t warp_sums[kScanThreads / 32];
-    const uint32_t per = (total + kScanThreads - 1) / kScanThreads;
-    const uint32_t lo = threadIdx.x * per;
-    const uint32_t hi = min(lo + per, total);
-    uint32_t s = 0;
-    for (uint32_t i = lo; i < hi; i++) s += hist[i];
-    // block exclusive scan of s
+// Block-wide exclusive scan of one value per thread (blockDim.x == 256).
+__device__ __forceinline__ uint32_t block_excl_scan256(uint32_t v, uint32_t *warp_tot, uint32_t &total) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t v = s;
+    uint32_t x = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        uint32_t y = __shfl_up_sync(0xffffffffu, v, o);
-        if (lane >= o) v += y;
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
     }
-    if (lane == 31) warp_sums[warp] = v;
+    if (lane == 31) warp_tot[warp] = x;
     __syncthreads();
-    if (warp == 0) {
-        uint32_t w = warp_sums[lane];
+    uint32_t before = 0, all = 0;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= o) w += y;
-        }
-        warp_sums[lane] = w;
+    for (int w = 0; w < kRsWarps; w++) {
+        const uint32_t t = warp_tot[w];
+        if (w < warp) before += t;
+        all += t;
     }
     __syncthreads();
-    uint32_t run = v - s + (warp > 0 ? warp_sums[warp - 1] : 0u);
-    for (uint32_t i = lo; i < hi; i++) {
-        uint32_t c = hist[i];
-        hist[i] = run;
-        run += c;
+    total = all;
+    return x - v + before;
+}
+
+// Exclusive scan of each digit's row hist[d][0..nb) (one block per digit);
+// the row total goes to totals[d].
+__global__ void __launch_bounds__(kRsThreads)
+radix_rowscan_kernel(uint32_t *__restrict__ hist, uint32_t nb, uint32_t *__restrict__ totals) {
+    __shared__ uint32_t warp_tot[kRsWarps];
+    uint32_t *row = hist + (size_t)blockIdx.x * nb;
+    uint32_t run = 0;
+    for (uint32_t base = 0; base < nb; base += kRsThreads) {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t v = (i < nb) ? row[i] : 0u;
+        uint32_t tot;
+        const uint32_t ex = block_excl_scan256(v, warp_tot, tot);
+        if (i < nb) row[i] = run + ex;
+        run += tot;
     }
+    if (threadIdx.x == 0) totals[blockIdx.x] = run;
 }
 
 // Stable scatter of one 8-bit digit.  Item order inside a tile is
@@ -207,12 +222,15 @@ __global__ void __launch_bounds__(kScanThreads) radix_scan_kernel(uint32_t *__re
 __global__ void __launch_bounds__(kRsThreads)
 radix_downsweep_kernel(const uint32_t *__restrict__ kin, const uint32_t *__restrict__ vin,
                        uint32_t *__restrict__ kout, uint32_t *__restrict__ vout, uint32_t N, int shift,
-                       const uint32_t *__restrict__ hist) {
+                       const uint32_t *__restrict__ hist, const uint32_t *__restrict__ totals) {
     __shared__ uint32_t goff[256];
     __shared__ uint32_t running[256];
     __shared__ uint32_t wcnt[kRsWarps][256];
+    __shared__ uint32_t warp_tot[kRsWarps];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    goff[tid] = hist[tid * gridDim.x + blockIdx.x];
+    uint32_t all;
+    const uint32_t digit_base = block_excl_scan256(totals[tid], warp_tot, all);
+    goff[tid] = digit_base + hist[tid * gridDim.x + blockIdx.x];
     running[tid] = 0;
     const uint32_t lt_mask = (1u << lane) - 1u;
     const uint32_t base = blockIdx.x * kRsTile;
@@ -332,32 +350,35 @@ uint32_t key_bits(uint32_t n) {
     return b == 0 ? 1 : b;
 }
 
-size_t radix_hist_entries(uint32_t N) { return 256ull * ((N + kRsTile - 1) / kRsTile); }
+size_t radix_hist_entries(uint32_t N) { return 256ull * ((N + kRsTile - 1) / kRsTile) + 256ull; }
 
 cudaError_t launch_bbox_and_params(pppm_scene *s) {
     const int nb = s->bbox_blocks;
-    if (s->prm.domain_mode != PPPM_DOMAIN_FIXED) {
-        bbox_partial_kernel<<<nb, kBBoxThreads, 0, s->stream>>>(s->vpos, s->N, s->bbox_partial, nb);
-        PPPM_CUDA_TRY(cudaGetLastError());
-    }
+    ::pppm::note_launch();
+    bbox_partial_kernel<<<nb, kBBoxThreads, 0, s->stream>>>(s->vpos, s->N, s->bbox_partial, nb);
+    PPPM_CUDA_TRY(cudaGetLastError());
+    ::pppm::note_launch();
     params_kernel<<<1, 32, 0, s->stream>>>(s->bbox_partial, nb, s->prm, s->dparams);
     return cudaGetLastError();
 }
 
-// Sorts (key, index) of N points; key[0]/idx[0] receive the computed keys.
+// Sorts (key, index) of N points; key[0]/idx[0] hold the keys on entry.
 // Returns pointers to the buffers holding the sorted result.
-static cudaError_t radix_sort_pairs(cudaStream_t st, uint32_t N, uint32_t bits, uint32_t *key[2],
+cudaError_t radix_sort_pairs(cudaStream_t st, uint32_t N, uint32_t bits, uint32_t *key[2],
                                     uint32_t *idx[2], uint32_t *hist, uint32_t **sorted_key,
                                     uint32_t **sorted_idx) {
     const uint32_t nb = (N + kRsTile - 1) / kRsTile;
     int cur = 0;
     for (uint32_t shift = 0; shift < bits; shift += 8) {
+        ::pppm::note_launch();
         radix_upsweep_kernel<<<nb, kRsThreads, 0, st>>>(key[cur], N, (int)shift, hist);
         PPPM_CUDA_TRY(cudaGetLastError());
-        radix_scan_kernel<<<1, kScanThreads, 0, st>>>(hist, 256u * nb);
+        ::pppm::note_launch();
+        radix_rowscan_kernel<<<256, kRsThreads, 0, st>>>(hist, nb, hist + 256u * nb);
         PPPM_CUDA_TRY(cudaGetLastError());
+        ::pppm::note_launch();
         radix_downsweep_kernel<<<nb, kRsThreads, 0, st>>>(key[cur], idx[cur], key[cur ^ 1], idx[cur ^ 1], N,
-                                                          (int)shift, hist);
+                                                          (int)shift, hist, hist + 256u * nb);
         PPPM_CUDA_TRY(cudaGetLastError());
         cur ^= 1;
     }
@@ -368,6 +389,7 @@ static cudaError_t radix_sort_pairs(cudaStream_t st, uint32_t N, uint32_t bits, 
 
 cudaError_t launch_hash_sort(pppm_scene *s, const float4 *pos, uint32_t N, uint32_t *key[2], uint32_t *idx[2],
                              uint32_t **sorted_key, uint32_t **sorted_idx) {
+    ::pppm::note_launch();
     keys_kernel<<<blocks_for(N, 256), 256, 0, s->stream>>>(pos, N, s->dparams, key[0], idx[0]);
     PPPM_CUDA_TRY(cudaGetLastError());
     return radix_sort_pairs(s->stream, N, key_bits(s->n), key, idx, s->hist, sorted_key, sorted_idx);
@@ -382,6 +404,7 @@ cudaError_t launch_cells_reorder(pppm_scene *s) {
         PPPM_CUDA_TRY(cudaMemsetAsync(s->mflag, 0, tbytes, s->stream));
         s->epoch = 1;
     }
+    ::pppm::note_launch();
     cells_reorder_kernel<<<blocks_for(s->N, 256), 256, 0, s->stream>>>(
         s->vsorted_key, s->vsorted_idx, s->N, s->vpos, s->valpha, s->capN, s->dparams, s->cell_start,
         s->cell_end, s->mflag, s->epoch, s->vrec, s->valf);
@@ -389,6 +412,7 @@ cudaError_t launch_cells_reorder(pppm_scene *s) {
 }
 
 cudaError_t launch_gather_sorted(pppm_scene *s, float4 *pos_out, double *alpha_out) {
+    ::pppm::note_launch();
     gather_sorted_kernel<<<blocks_for(s->N, 256), 256, 0, s->stream>>>(
         s->vsorted_idx, s->N, s->vpos, s->valpha, s->capN, pos_out, alpha_out,
         alpha_out ? alpha_out + s->N : nullptr, alpha_out ? alpha_out + 2 * (size_t)s->N : nullptr);
@@ -459,6 +483,7 @@ extern "C" pppm_status pppm_hasher_run(pppm_hasher *h, uint32_t N, const float *
     }
     h->N = N;
     const float4 *pos = reinterpret_cast<const float4 *>(pos4_dev);
+    ::pppm::note_launch();
     pppm::keys_explicit_kernel<<<(N + 255) / 256, 256, 0, h->stream>>>(pos, N, cell_h, origin[0], origin[1],
                                                                      origin[2], h->n, h->key[0], h->idx[0]);
     cudaError_t e = cudaGetLastError();
@@ -467,6 +492,7 @@ extern "C" pppm_status pppm_hasher_run(pppm_hasher *h, uint32_t N, const float *
     if (e == cudaSuccess) e = cudaMemsetAsync(h->start, 0xFF, sizeof(uint32_t) * h->C, h->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(h->end, 0xFF, sizeof(uint32_t) * h->C, h->stream);
     if (e == cudaSuccess) {
+        ::pppm::note_launch();
         pppm::cells_only_kernel<<<(N + 255) / 256, 256, 0, h->stream>>>(h->skey, N, h->start, h->end);
         e = cudaGetLastError();
     }
@@ -496,6 +522,7 @@ static pppm_status hasher_permute(pppm_hasher *h, uint32_t N, const void *in, vo
         pppm_set_error("pppm_hasher_%s: invalid argument", scatter ? "deorder" : "reorder");
         return PPPM_ERR_INVALID;
     }
+    ::pppm::note_launch();
     if (precision == 1)
         pppm::permute_kernel<float><<<(N + 255) / 256, 256, 0, h->stream>>>(
             h->sidx, N, (const float *)in, (float *)out, stride, scatter);

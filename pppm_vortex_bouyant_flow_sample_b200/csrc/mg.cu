@@ -220,19 +220,26 @@ static cudaError_t vcycle32(const MGPlan &m, int level) {
         const int d = (int)m.lv[j].d;
         const dim3 g = grid_for((uint32_t)(d / 2) * d * d, m.comps);
         for (int it = 0; it < 4; it++) {
+            ::pppm::note_launch();
             rbsor_kernel<<<g, kMGThreads, 0, m.st>>>(m.lv[j].x, m.lv[j].b, d, 1);
+            ::pppm::note_launch();
             rbsor_kernel<<<g, kMGThreads, 0, m.st>>>(m.lv[j].x, m.lv[j].b, d, 0);
         }
+        ::pppm::note_launch();
         resid_restrict_kernel<<<grid_for(m.lv[j + 1].cells, m.comps), kMGThreads, 0, m.st>>>(
             m.lv[j].x, m.lv[j].b, m.lv[j + 1].b, (int)m.lv[j + 1].d, 0);
     }
+    ::pppm::note_launch();
     coarse_kernel<<<m.comps, 512, 0, m.st>>>(m.lv[L - 1].x, m.lv[L - 1].b, (int)m.lv[L - 1].d);
     for (int j = L - 2; j >= level; j--) {
         const int d = (int)m.lv[j].d;
+        ::pppm::note_launch();
         prolong_kernel<<<grid_for(m.lv[j].cells, m.comps), kMGThreads, 0, m.st>>>(m.lv[j].x, m.lv[j + 1].x, d);
         const dim3 g = grid_for((uint32_t)(d / 2) * d * d, m.comps);
         for (int it = 0; it < 4; it++) {
+            ::pppm::note_launch();
             rbsor_kernel<<<g, kMGThreads, 0, m.st>>>(m.lv[j].x, m.lv[j].b, d, 1);
+            ::pppm::note_launch();
             rbsor_kernel<<<g, kMGThreads, 0, m.st>>>(m.lv[j].x, m.lv[j].b, d, 0);
         }
     }
@@ -246,12 +253,16 @@ static cudaError_t fmg32(const MGPlan &m) {
     const int L = m.levels;
     for (int j = 0; j < L; j++)
         PPPM_CUDA_TRY(cudaMemsetAsync(m.lv[j].x, 0, sizeof(float) * m.comps * (size_t)m.lv[j].cells, m.st));
-    for (int j = 0; j < L - 1; j++)
+    for (int j = 0; j < L - 1; j++) {
+        ::pppm::note_launch();
         resid_restrict_kernel<<<grid_for(m.lv[j + 1].cells, m.comps), kMGThreads, 0, m.st>>>(
             m.lv[j].x, m.lv[j].b, m.lv[j + 1].b, (int)m.lv[j + 1].d, 1);
+    }
+    ::pppm::note_launch();
     coarse_kernel<<<m.comps, 512, 0, m.st>>>(m.lv[L - 1].x, m.lv[L - 1].b, (int)m.lv[L - 1].d);
     PPPM_CUDA_TRY(cudaGetLastError());
     for (int j = L - 2; j >= 0; j--) {
+        ::pppm::note_launch();
         prolong_kernel<<<grid_for(m.lv[j].cells, m.comps), kMGThreads, 0, m.st>>>(m.lv[j].x, m.lv[j + 1].x,
                                                                                 (int)m.lv[j].d);
         PPPM_CUDA_TRY(vcycle32(m, j));
@@ -264,6 +275,7 @@ static cudaError_t fmg32(const MGPlan &m) {
 static cudaError_t dc_residual(const MGPlan &m, bool want_norms) {
     const uint32_t C0 = m.lv[0].cells;
     if (want_norms) PPPM_CUDA_TRY(cudaMemsetAsync(m.norms, 0, 2 * sizeof(double), m.st));
+    ::pppm::note_launch();
     dc_residual_kernel<<<grid_for(C0, m.comps), kMGThreads, 0, m.st>>>(m.psi, m.b64, m.vort, m.P, m.lv[0].b,
                                                                        (int)m.lv[0].d, want_norms ? m.norms : nullptr);
     return cudaGetLastError();
@@ -275,6 +287,7 @@ static cudaError_t dc_correct(const MGPlan &m) {
     PPPM_CUDA_TRY(cudaMemsetAsync(m.lv[0].x, 0, sizeof(float) * m.comps * (size_t)C0, m.st));
     PPPM_CUDA_TRY(vcycle32(m, 0));
     const size_t cnt = (size_t)m.comps * C0;
+    ::pppm::note_launch();
     dc_update_kernel<<<(unsigned)((cnt + 255) / 256), 256, 0, m.st>>>(m.psi, m.lv[0].x, cnt, 0);
     return cudaGetLastError();
 }
@@ -294,6 +307,7 @@ static cudaError_t read_relres(const MGPlan &m, double *relres) {
 cudaError_t mg_solve(const MGPlan &m, int mode, double tol, int max_cycles, int *cycles_out, double *relres_out) {
     PPPM_CUDA_TRY(fmg32(m));
     const size_t cnt = (size_t)m.comps * m.lv[0].cells;
+    ::pppm::note_launch();
     dc_update_kernel<<<(unsigned)((cnt + 255) / 256), 256, 0, m.st>>>(m.psi, m.lv[0].x, cnt, 1);
     PPPM_CUDA_TRY(cudaGetLastError());
     PPPM_CUDA_TRY(dc_residual(m, false));

@@ -106,6 +106,7 @@ p2m_kernel(const uint32_t *__restrict__ start, const uint32_t *__restrict__ end,
 
 cudaError_t launch_p2m(pppm_scene *s) {
     const unsigned blocks = (s->C + kP2MThreads - 1) / kP2MThreads;
+    ::pppm::note_launch();
     p2m_kernel<<<blocks, kP2MThreads, 0, s->stream>>>(s->cell_start, s->cell_end, s->vrec, s->valf, s->mflag,
                                                       s->epoch, s->dparams, s->n, s->vort, s->lv[0].b);
     return cudaGetLastError();

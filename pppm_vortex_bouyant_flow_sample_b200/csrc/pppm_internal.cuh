@@ -44,6 +44,8 @@ struct DevParams {
     float kdiag_f;      // (float)(0.5 * invh * 0.250580605913965 * h^2)
     float inv_a3_f;     // 1/a^3
     float inv4pia3_f;   // 1/(4 pi a^3)
+    double prune_cells; // bound, in cells, on |hash cell coordinate - FP64 NGP coordinate|
+                        // plus the float rounding of the box test (near-field cell pruning)
     uint32_t n;
     int32_t K;
     int32_t status;     // 0 ok, else PPPM_ERR_* raised on the device
@@ -118,6 +120,11 @@ struct pppm_scene {
     float4 *stage_ea = nullptr, *stage_eb = nullptr;  // pppm_solve_host staging [capM]
     double *stage_out = nullptr;                       // [3][capM]
 
+    // per-stage CUDA-event timing (pppm_scene_set_profiling)
+    bool profiling = false;
+    cudaEvent_t ev_begin[16] = {}, ev_end[16] = {};
+    bool ev_used[16] = {};
+
     // statistics
     unsigned long long *pair_count = nullptr;
     int mg_cycles_last = 0;
@@ -125,6 +132,26 @@ struct pppm_scene {
 };
 
 namespace pppm {
+
+// Stages timed by the profiling events, in pipeline order.
+enum Stage {
+    kStageDomain = 0,      // bounding box + device parameters
+    kStageVortSort = 1,    // vortex keys + radix sort
+    kStageCells = 2,       // cell tables + reorder
+    kStageP2M = 3,
+    kStageMG = 4,
+    kStageFar = 5,         // curl + far-field correction
+    kStageEvalSort = 6,    // evaluation-point keys + radix sort
+    kStageEval = 7,        // interpolation + near field + deorder
+    kNumStages = 8
+};
+const char *stage_name(int i);
+
+// Process-wide count of kernel launches issued by this library.
+void note_launch();
+unsigned long long launch_count();
+void prof_begin(pppm_scene *s, int stage);
+void prof_end(pppm_scene *s, int stage);
 
 // Kernel launchers (each enqueues on s->stream and returns the launch status).
 cudaError_t launch_bbox_and_params(pppm_scene *s);
@@ -140,6 +167,9 @@ cudaError_t launch_gather_sorted(pppm_scene *s, float4 *pos_out, double *alpha_o
 
 cudaError_t mg_solve(const MGPlan &m, int mode, double tol, int max_cycles, int *cycles_out,
                      double *relres_out);
+
+cudaError_t radix_sort_pairs(cudaStream_t st, uint32_t N, uint32_t bits, uint32_t *key[2], uint32_t *idx[2],
+                             uint32_t *hist, uint32_t **sorted_key, uint32_t **sorted_idx);
 
 int mg_level_count(uint32_t n);
 bool mg_shape_ok(uint32_t n);
