@@ -77,30 +77,58 @@ struct PairAcc {
     unsigned long long n = 0;
 };
 
-// Near-field sum over one hash cell's vortices for one point.  SEG: test the
-// segment's other end; COUNT: count the pairs inside the box.
+// One candidate pair: box test, then the smoothed Biot-Savart term.
+// SEG: test the segment's other end; COUNT: count the pairs inside the box.
+template <bool SEG, bool COUNT>
+__device__ __forceinline__ void pair_term(const float4 r, const float4 *__restrict__ al_src, bool lane_ok,
+                                          const float3 ra, const float3 rb, float cr, float inv_a3, float inv4pia3,
+                                          PairAcc &acc) {
+    const float dx = ra.x - r.x, dy = ra.y - r.y, dz = ra.z - r.z;
+    if (!(lane_ok && fmaxf(fabsf(dx), fmaxf(fabsf(dy), fabsf(dz))) <= cr)) return;
+    if (COUNT) acc.n++;
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    bool skip = r2 < 1e-24f;
+    if (SEG) {
+        const float ex = rb.x - r.x, ey = rb.y - r.y, ez = rb.z - r.z;
+        skip |= fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < 1e-24f;
+    }
+    if (skip) return;
+    const float rr = r2 * rsqrtf(r2);  // r2 >= 1e-24 here
+    const float coeff = phi_smooth(r2 * rr * inv_a3) * inv4pia3;
+    const float4 al = *al_src;
+    acc.x = fmaf(al.y * dz - al.z * dy, coeff, acc.x);
+    acc.y = fmaf(al.z * dx - al.x * dz, coeff, acc.y);
+    acc.z = fmaf(al.x * dy - al.y * dx, coeff, acc.z);
+}
+
+// Near-field sum over one hash cell's vortices for one point (own walk).
 template <bool SEG, bool COUNT>
 __device__ __forceinline__ void cell_pairs(const float4 *__restrict__ vrec, const float4 *__restrict__ valf,
                                            uint32_t ps, uint32_t pe, bool lane_ok, const float3 ra, const float3 rb,
                                            float cr, float inv_a3, float inv4pia3, PairAcc &acc) {
-    for (uint32_t p = ps; p < pe; p++) {
-        const float4 r = vrec[p];
-        const float dx = ra.x - r.x, dy = ra.y - r.y, dz = ra.z - r.z;
-        if (!(lane_ok && fmaxf(fabsf(dx), fmaxf(fabsf(dy), fabsf(dz))) <= cr)) continue;
-        if (COUNT) acc.n++;
-        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        bool skip = r2 < 1e-24f;
-        if (SEG) {
-            const float ex = rb.x - r.x, ey = rb.y - r.y, ez = rb.z - r.z;
-            skip |= fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < 1e-24f;
+    for (uint32_t p = ps; p < pe; p++)
+        pair_term<SEG, COUNT>(vrec[p], valf + p, lane_ok, ra, rb, cr, inv_a3, inv4pia3, acc);
+}
+
+// Warp-uniform version: the warp copies the cell's records into its shared
+// staging area 32 at a time with one coalesced load per stream, then every
+// lane reads them back as shared-memory broadcasts.
+template <bool SEG, bool COUNT>
+__device__ __forceinline__ void cell_pairs_staged(const float4 *__restrict__ vrec, const float4 *__restrict__ valf,
+                                                  uint32_t ps, uint32_t pe, bool lane_ok, const float3 ra,
+                                                  const float3 rb, float cr, float inv_a3, float inv4pia3,
+                                                  float4 *__restrict__ sv, float4 *__restrict__ sa, int lane,
+                                                  PairAcc &acc) {
+    for (uint32_t base = ps; base < pe; base += 32) {
+        const uint32_t cnt = min(32u, pe - base);
+        if ((uint32_t)lane < cnt) {
+            sv[lane] = vrec[base + lane];
+            sa[lane] = valf[base + lane];
         }
-        if (skip) continue;
-        const float rr = r2 * rsqrtf(r2);  // r2 >= 1e-24 here
-        const float coeff = phi_smooth(r2 * rr * inv_a3) * inv4pia3;
-        const float4 al = valf[p];
-        acc.x = fmaf(al.y * dz - al.z * dy, coeff, acc.x);
-        acc.y = fmaf(al.z * dx - al.x * dz, coeff, acc.y);
-        acc.z = fmaf(al.x * dy - al.y * dx, coeff, acc.z);
+        __syncwarp();
+        for (uint32_t q = 0; q < cnt; q++)
+            pair_term<SEG, COUNT>(sv[q], sa + q, lane_ok, ra, rb, cr, inv_a3, inv4pia3, acc);
+        __syncwarp();
     }
 }
 
@@ -115,6 +143,9 @@ __global__ void eval_kernel(const uint32_t *__restrict__ eidx, uint32_t M, const
             const float4 *__restrict__ valf, const DevParams *__restrict__ P, int n, int K,
             double *__restrict__ u, double *__restrict__ v, double *__restrict__ w, float *__restrict__ uf,
             unsigned long long *__restrict__ pair_count) {
+    __shared__ float4 stage_v[kEvalThreads], stage_a[kEvalThreads];
+    const int lane = threadIdx.x & 31;
+    float4 *sv = stage_v + (threadIdx.x - lane), *sa = stage_a + (threadIdx.x - lane);
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     const bool act = s < M;
     const uint32_t q = act ? eidx[s] : 0u;
@@ -180,7 +211,8 @@ __global__ void eval_kernel(const uint32_t *__restrict__ eidx, uint32_t M, const
                         if (ps == kEmpty) continue;
                         const bool lane_ok = ii >= lo[0] && ii <= hi[0] && jj >= lo[1] && jj <= hi[1] &&
                                              kk >= lo[2] && kk <= hi[2];
-                        cell_pairs<SEG, COUNT>(vrec, valf, ps, end[cell], lane_ok, ra, rb, cr, inv_a3, inv4pia3, acc);
+                        cell_pairs_staged<SEG, COUNT>(vrec, valf, ps, end[cell], lane_ok, ra, rb, cr, inv_a3, inv4pia3, sv, sa,
+                                                      lane, acc);
                     }
         } else if (act && lo[0] <= hi[0]) {
             // scattered warp (points outside the grid, sparse regions): own walk
