@@ -202,6 +202,27 @@ pppm_status pppm_hasher_reorder(pppm_hasher *h, uint32_t N, const void *in_dev, 
 pppm_status pppm_hasher_deorder(pppm_hasher *h, uint32_t N, const void *in_dev, void *out_dev,
                                 uint32_t stride, uint32_t precision);
 
+/* ---- spatial hash that allocates nothing ---------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory on this path (inside stream capture, under an allocator that must
+ * not grow, or when another framework owns the device heap): the same result
+ * as pppm_hasher_run (sorted keys, sorted original indices, cell start/end
+ * tables of n^3 entries) into caller-provided device arrays, with the sort's
+ * scratch in a fixed device array of PPPM_NOALLOC_SCRATCH_BYTES that every
+ * GPU loading the library keeps until the process exits.
+ *   - N must not exceed PPPM_NOALLOC_MAX_PARTICLES (else PPPM_ERR_INVALID).
+ *   - The first call on a device looks up the array's device address; make
+ *     that first call before any stream capture on that device.
+ *   - All calls share the array: calls whose work overlaps on the GPU (other
+ *     streams, other threads) race and corrupt each other's results.
+ *   - No cudaMalloc, cudaFree or allocating library routine is called. */
+#define PPPM_NOALLOC_MAX_PARTICLES 1048576u
+#define PPPM_NOALLOC_SCRATCH_BYTES 8651776u
+pppm_status pppm_spatial_hash_noalloc(uint32_t N, const float *pos4_dev, uint32_t n, float cell_h,
+                                      const float origin[3], uint32_t *sorted_key_dev,
+                                      uint32_t *sorted_idx_dev, uint32_t *cell_start_dev,
+                                      uint32_t *cell_end_dev, void *stream);
+
 /* ---- FP64 O(N*M) direct sum with the near field's smoothing kernel ------
  * (accuracy ground truth; no reference counterpart) */
 pppm_status pppm_direct_sum_fp64(uint32_t N, const float *vort_pos4_dev, const double *ax_dev,

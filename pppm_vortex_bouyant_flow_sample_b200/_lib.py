@@ -26,7 +26,9 @@ EXPORTED = (
     "pppm_mg_full_multigrid", "pppm_hasher_create", "pppm_hasher_destroy", "pppm_hasher_run",
     "pppm_hasher_tables", "pppm_hasher_reorder", "pppm_hasher_deorder", "pppm_direct_sum_fp64",
     "pppm_scene_set_profiling", "pppm_stage_name", "pppm_get_stage_times", "pppm_kernel_launches",
+    "pppm_spatial_hash_noalloc",
 )
+NOALLOC_MAX_PARTICLES = 1048576  # PPPM_NOALLOC_MAX_PARTICLES in include/pppm.h
 STAGES = ("domain", "vort_sort", "cells_reorder", "p2m", "multigrid", "farfield", "eval_sort", "eval")
 
 
@@ -106,6 +108,7 @@ def load(build_if_missing: bool = True):
         "pppm_stage_name": (C.c_char_p, [C.c_int]),
         "pppm_get_stage_times": (st, [vp, C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_int)]),
         "pppm_kernel_launches": (C.c_uint64, []),
+        "pppm_spatial_hash_noalloc": (st, [u32, vp, u32, C.c_float, C.POINTER(C.c_float), vp, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

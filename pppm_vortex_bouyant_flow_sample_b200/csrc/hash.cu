@@ -25,6 +25,7 @@ constexpr int kBBoxThreads = 256;
 constexpr int kRsThreads = 256;
 constexpr int kRsItems = 16;
 constexpr int kRsTile = kRsThreads * kRsItems;
+static_assert(kRsTile == (int)kRsTileHost, "tile size mismatch");
 constexpr int kRsWarps = kRsThreads / 32;
 
 __global__ void bbox_partial_kernel(const float4 *__restrict__ pos, uint32_t N,
@@ -545,4 +546,107 @@ extern "C" pppm_status pppm_hasher_reorder(pppm_hasher *h, uint32_t N, const voi
 extern "C" pppm_status pppm_hasher_deorder(pppm_hasher *h, uint32_t N, const void *in, void *out,
                                            uint32_t stride, uint32_t precision) {
     return hasher_permute(h, N, in, out, stride, precision, 1);
+}
+
+// ---------------------------------------------------------------------------
+// Spatial hash that allocates nothing.
+//
+// For callers that cannot call cudaMalloc on this path: code running inside a
+// stream-capture region, under a host allocator that must not grow, or in a
+// process whose device memory is handed out by another framework.  The caller
+// passes the positions and the four output arrays; the radix sort's second
+// key/index buffer and its digit histograms live in the fixed device array
+// below, which every GPU that loads this library holds until the process
+// exits (PPPM_NOALLOC_SCRATCH_BYTES, about 8.3 MB).
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace {
+
+constexpr uint32_t kNoAllocMaxN = PPPM_NOALLOC_MAX_PARTICLES;
+constexpr size_t kNoAllocHistWords = 256ull * ((kNoAllocMaxN + pppm::kRsTileHost - 1) / pppm::kRsTileHost) + 256ull;
+constexpr size_t kNoAllocWords = 2ull * kNoAllocMaxN + kNoAllocHistWords;
+static_assert(kNoAllocWords * 4 == PPPM_NOALLOC_SCRATCH_BYTES, "scratch size in pppm.h is stale");
+
+// Shared by every call on a device; its contents are whatever the last call
+// left.  Nothing in it needs to start at zero: each pass overwrites every
+// histogram entry and every key/index slot it later reads.
+static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocWords];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+uint32_t *g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device, looked up once
+// per device.  The host-side symbol is only a stand-in and must never be
+// passed to a kernel.
+cudaError_t noalloc_scratch(uint32_t **out) {
+    int dev = 0;
+    PPPM_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[dev]) {
+        void *p = nullptr;
+        PPPM_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_addr[dev] = static_cast<uint32_t *>(p);
+    }
+    *out = g_noalloc_addr[dev];
+    return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" pppm_status pppm_spatial_hash_noalloc(uint32_t N, const float *pos4_dev, uint32_t n, float cell_h,
+                                                 const float origin[3], uint32_t *sorted_key_dev,
+                                                 uint32_t *sorted_idx_dev, uint32_t *cell_start_dev,
+                                                 uint32_t *cell_end_dev, void *stream) {
+    if (N > kNoAllocMaxN) {
+        pppm_set_error("pppm_spatial_hash_noalloc: N=%u exceeds the fixed scratch limit of %u particles", N,
+                       kNoAllocMaxN);
+        return PPPM_ERR_INVALID;
+    }
+    if (N == 0 || !pos4_dev || !origin || !sorted_key_dev || !sorted_idx_dev || !cell_start_dev || !cell_end_dev ||
+        n < 2 || n > 1024 || !(cell_h > 0.f)) {
+        pppm_set_error("pppm_spatial_hash_noalloc: invalid argument");
+        return PPPM_ERR_INVALID;
+    }
+    uint32_t *scratch = nullptr;
+    cudaError_t e = noalloc_scratch(&scratch);
+    if (e != cudaSuccess) {
+        pppm_set_error("pppm_spatial_hash_noalloc: scratch set-up failed: %s", cudaGetErrorString(e));
+        return PPPM_ERR_CUDA;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const uint32_t bits = pppm::key_bits(n);
+    const uint32_t passes = (bits + 7) / 8;
+    // The result lands in key[passes % 2]; start in the scratch when the pass
+    // count is odd so that it ends in the caller's arrays.
+    uint32_t *bk = scratch, *bi = scratch + kNoAllocMaxN, *hist = scratch + 2ull * kNoAllocMaxN;
+    uint32_t *key[2], *idx[2];
+    if (passes & 1u) {
+        key[0] = bk; idx[0] = bi; key[1] = sorted_key_dev; idx[1] = sorted_idx_dev;
+    } else {
+        key[0] = sorted_key_dev; idx[0] = sorted_idx_dev; key[1] = bk; idx[1] = bi;
+    }
+    const uint64_t C = (uint64_t)n * n * n;
+    ::pppm::note_launch();
+    pppm::keys_explicit_kernel<<<(N + 255) / 256, 256, 0, st>>>(reinterpret_cast<const float4 *>(pos4_dev), N,
+                                                               cell_h, origin[0], origin[1], origin[2], n, key[0],
+                                                               idx[0]);
+    e = cudaGetLastError();
+    uint32_t *sk = nullptr, *si = nullptr;
+    if (e == cudaSuccess) e = pppm::radix_sort_pairs(st, N, bits, key, idx, hist, &sk, &si);
+    if (e == cudaSuccess && sk != sorted_key_dev) e = cudaErrorUnknown;  // parity rule above broken
+    if (e == cudaSuccess) e = cudaMemsetAsync(cell_start_dev, 0xFF, sizeof(uint32_t) * C, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(cell_end_dev, 0xFF, sizeof(uint32_t) * C, st);
+    if (e == cudaSuccess) {
+        ::pppm::note_launch();
+        pppm::cells_only_kernel<<<(N + 255) / 256, 256, 0, st>>>(sorted_key_dev, N, cell_start_dev, cell_end_dev);
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) {
+        pppm_set_error("pppm_spatial_hash_noalloc: %s", cudaGetErrorString(e));
+        return PPPM_ERR_CUDA;
+    }
+    return PPPM_OK;
 }

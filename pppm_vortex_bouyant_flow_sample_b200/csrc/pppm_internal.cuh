@@ -22,6 +22,7 @@ namespace pppm {
 constexpr uint32_t kEmpty = 0xFFFFFFFFu;
 constexpr int kMaxLevels = 12;
 constexpr int kMaxK = 4;  // near-field range limit (table (2K+1)^3 in shared memory)
+constexpr uint32_t kRsTileHost = 4096;  // radix-sort keys per block (kRsThreads * kRsItems)
 
 // Literal constants of the reference kernels.
 constexpr double kFourPi = 12.5663706144;          // HFS/GPU_kernel.cu:12,2397,2403
