@@ -40,7 +40,8 @@ N_PART = 1_048_576
 GRID = 128
 K_NEAR = 1
 A_SMOOTH = 0.08
-WORKLOAD = ("vortex ring, 1,048,576 particles, 128^3 grid, K=1, a=0.08, domain 3x bbox, "
+def workload(N: int, n: int) -> str:
+    return (f"vortex ring, {N:,} particles, {n}^3 grid, K=1, a=0.08, domain 3x bbox, "
             "reference multigrid schedule (FMG + 1 V(4,4), FP32 with FP64 defect correction); "
             "step = far-field build + velocity at every particle")
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1965e6 / 1e12  # nominal: SMs x FP32 lanes x FMA x max clock
@@ -56,6 +57,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--particles", type=int, default=N_PART)
     ap.add_argument("--grid", type=int, default=GRID)
+    ap.add_argument("--workload", default="ring", choices=["ring", "mix"],
+                    help="ring: the at-scale single scene (default); mix: 64 independent scenes, "
+                         "one after another vs in one batch")
+    ap.add_argument("--scenes", type=int, default=64)
     return ap.parse_args()
 
 
@@ -168,7 +173,8 @@ def run_reference(args, world, rank):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * el / max(args.steps, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": WORKLOAD, "grid": args.grid, "particles": args.particles,
+            "data": "synthetic", "config": {"workload": workload(args.particles, args.grid), "grid": args.grid,
+                                            "particles": args.particles,
                                             "parallelism": "host threads (OpenMP)"},
             "cpu_baseline": cpu,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -270,6 +276,25 @@ def run_b200(args, world, rank, local):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_val = world * N / float(t.item())
 
+    # one RK2 (midpoint) advection step of the same scene: two far-field
+    # builds and two evaluations (reported beside the headline, not in it)
+    rk_pos = dpos.clone()
+    scene.advect(rk_pos, dal, 1e-3, method="rk2")
+    torch.cuda.synchronize()
+    rk_ms = []
+    for _ in range(3):
+        rk_pos.copy_(dpos)
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        scene.advect(rk_pos, dal, 1e-3, method="rk2")
+        e1.record(stream)
+        torch.cuda.synchronize()
+        rk_ms.append(e0.elapsed_time(e1))
+    rk2_ms = statistics.median(rk_ms)
+    del rk_pos
+
     # accuracy on a fixed 1% subsample (every 100th particle) vs the FP64 direct sum
     sub = dpos[::100].contiguous()
     u_gpu = out.t()[::100].cpu().numpy()
@@ -308,7 +333,7 @@ def run_b200(args, world, rank, local):
             "warmup": max(args.warmup, 3), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 (multigrid residual/accumulation f64)",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "grid": args.grid, "particles": N, "eval_points": N,
+            "config": {"workload": workload(N, args.grid), "grid": args.grid, "particles": N, "eval_points": N,
                        "parallelism": "replicas" if world > 1 else "single scene",
                        "l2": "flushed between timed steps (512 MB write)"},
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": N * 16 + 3 * N * 8,
@@ -319,6 +344,7 @@ def run_b200(args, world, rank, local):
             "cpu_baseline": cpu,
             "stages_ms": stages,
             "err_vs_direct_fp64": err,
+            "rk2_step_ms": rk2_ms,
             "near_field_pairs": pairs,
         }
         print(json.dumps(line), flush=True)
@@ -327,11 +353,81 @@ def run_b200(args, world, rank, local):
         dist.destroy_process_group()
 
 
+def run_mix(args, world, rank, local):
+    """Batched-scene mix: grid edges from {32,48,64,96,128}, particle counts
+    log-uniform in [1e4, 1e6] (seed 2), even scenes uniform clouds, odd scenes
+    rings; each scene evaluated at its own particles.  Times the scenes one
+    after another on one stream (the single-scene path) and all together
+    through pppm_batch_run, device-timed, L2 flushed before each timing."""
+    import torch
+    import pppm_vortex_bouyant_flow_sample_b200 as pb
+    from pppm_vortex_bouyant_flow_sample_b200 import workloads as W
+    torch.cuda.set_device(local)
+    mix = W.scene_mix(args.scenes, seed=2)
+    scenes, data = [], []
+    for n, N, kind, seed in mix:
+        pos, al = W.make_scene(kind, N, seed)
+        dpos = torch.from_numpy(pos).cuda()
+        dal = torch.from_numpy(np.ascontiguousarray(al.T)).cuda()
+        out = torch.empty((3, N), dtype=torch.float64, device="cuda")
+        scenes.append(pb.Scene(n, cap_vort=N, cap_eval=N))
+        data.append((dpos, dal, out))
+    total = sum(N for _, N, _, _ in mix)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def sequential():
+        for sc, (dpos, dal, out) in zip(scenes, data):
+            sc.set_vortices(dpos, dal)
+            sc.build_far_field()
+            sc.eval(dpos, dpos, 1, out=out)
+
+    jobs = [(sc, dpos, dal, None, None, 1) for sc, (dpos, dal, _) in zip(scenes, data)]
+
+    def batched():
+        pb.batch_run(jobs)
+
+    def timed(fn):
+        for _ in range(max(args.warmup, 3)):
+            fn()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(args.steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return statistics.median(ms)
+
+    seq_ms = timed(sequential)
+    bat_ms = timed(batched)
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": total / (bat_ms / 1000.0), "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": bat_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (multigrid residual/accumulation f64)",
+            "data": "synthetic",
+            "config": {"workload": f"{len(mix)}-scene mix (grid 32..128, 1e4..1e6 particles, clouds + rings), "
+                                   "each scene evaluated at its particles", "scenes": len(mix),
+                       "particles_total": total, "l2": "flushed before each timed step"},
+            "sequential_ms": seq_ms, "batched_ms": bat_ms, "batch_speedup": seq_ms / bat_ms,
+            "sequential_evals_per_s": total / (seq_ms / 1000.0)}), flush=True)
+    for sc in scenes:
+        sc.close()
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
         run_reference(args, world, rank)
+        return
+    if args.workload == "mix":
+        run_mix(args, world, rank, local)
         return
     run_b200(args, world, rank, local)
 

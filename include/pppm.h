@@ -130,6 +130,18 @@ pppm_status pppm_solve_host(pppm_scene *s, uint32_t N, const float *pos4_host,
                             uint32_t M, const float *eval_a4_host, const float *eval_b4_host,
                             int is_segment, double *u_host, double *v_host, double *w_host);
 
+/* One time step of the vortex positions (device, in place) by their own
+ * velocity, strengths fixed.  Euler: the reference's particle move
+ * (HFS/VortexSimulationSystemImp.cpp:277-314, move_particle at
+ * HFS/GPU_kernel.cu:3118-3140): p <- float(double(p) + u dt), w = 0, with u the
+ * full evaluation at the vortices.  RK2 (midpoint): u1 = U(x),
+ * x_mid = x + dt/2 u1, u2 = U(x_mid), x <- x + dt u2 (two far-field builds and
+ * two evaluations).  The scene's far field afterwards is the last one built. */
+pppm_status pppm_advect_euler(pppm_scene *s, uint32_t N, float *pos4_dev, const double *ax_dev,
+                              const double *ay_dev, const double *az_dev, double dt);
+pppm_status pppm_advect_rk2(pppm_scene *s, uint32_t N, float *pos4_dev, const double *ax_dev,
+                            const double *ay_dev, const double *az_dev, double dt);
+
 /* Accessors matching BiotSavartSolver::getOrigin / getCellh
  * (HFS/BiotSavartSolver.h:34-35); synchronises the stream. */
 pppm_status pppm_get_domain(pppm_scene *s, double origin[3], double *length, double *cell_h);
@@ -164,6 +176,26 @@ const char *pppm_stage_name(int stage);
 pppm_status pppm_get_stage_times(pppm_scene *s, double *ms, int cap, int *count);
 /* Number of kernels this library has launched in the process so far. */
 uint64_t pppm_kernel_launches(void);
+
+/* ---- several independent scenes in one call -----------------------------
+ * No reference counterpart (the reference drives one solver from one host
+ * thread).  Each item is one scene's set_vortices + build_far_field + eval
+ * (M = 0 skips the eval).  Every item runs on its own stream from a pool the
+ * library keeps per device, ordered after the caller's earlier work on
+ * `stream`; `stream` then waits for all items.  A scene may appear once per
+ * batch.  Each scene's result is the one it gets alone. */
+typedef struct pppm_batch_item {
+    pppm_scene *scene;
+    uint32_t N;
+    const float *pos4_dev;
+    const double *ax_dev, *ay_dev, *az_dev;
+    uint32_t M;
+    const float *eval_a4_dev;
+    const float *eval_b4_dev;
+    int is_segment;
+    double *u_dev, *v_dev, *w_dev;
+} pppm_batch_item;
+pppm_status pppm_batch_run(pppm_batch_item *items, uint32_t count, void *stream);
 
 /* ---- multigrid surface: gf::MultiGridSolver3DPeriod_double
  * (MG/MultiGrid.h:188-209, MG/MultiGrid.cpp:128-250) ---------------------- */

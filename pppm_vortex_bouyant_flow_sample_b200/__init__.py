@@ -23,12 +23,12 @@ import ctypes as C
 import torch
 
 from ._lib import (DOMAIN_BBOX3X, DOMAIN_FIXED, GRID_FAR, GRID_PSI, GRID_VORT, MG_CONVERGED,
-                   MG_REFERENCE, PppmError, PppmParams, check, default_params, load)
+                   MG_REFERENCE, PppmBatchItem, PppmError, PppmParams, check, default_params, load)
 
 __all__ = [
     "Scene", "BiotSavartSolver", "ParticleManager", "MultiGridSolver3DPeriod_double", "PppmError",
     "PppmParams", "default_params", "load", "direct_sum_fp64", "MG_REFERENCE", "MG_CONVERGED",
-    "DOMAIN_BBOX3X", "DOMAIN_FIXED",
+    "DOMAIN_BBOX3X", "DOMAIN_FIXED", "batch_run",
 ]
 
 
@@ -192,6 +192,18 @@ class Scene:
         check(self._lib.pppm_get_stats(self._h, C.byref(pairs), C.byref(cyc), C.byref(rr)), "pppm_get_stats")
         return {"mg_cycles": cyc.value, "mg_relres": rr.value}
 
+    def advect(self, pos4: torch.Tensor, alpha: torch.Tensor, dt: float, method: str = "rk2"):
+        """Moves pos4 (CUDA float32 (N, 4), in place) by one Euler or RK2 step."""
+        if pos4.dtype != torch.float32 or not pos4.is_cuda or not pos4.is_contiguous() or pos4.shape[1] != 4:
+            raise ValueError("pos4 must be a contiguous CUDA float32 (N, 4) tensor (updated in place)")
+        N = pos4.shape[0]
+        ax, ay, az = _alpha3(alpha, N)
+        fn = self._lib.pppm_advect_rk2 if method == "rk2" else self._lib.pppm_advect_euler
+        check(fn(self._h, N, _ptr(pos4), _ptr(ax), _ptr(ay), _ptr(az), float(dt)), f"pppm_advect_{method}")
+        self._keep = [ax, ay, az]
+        self.N = N
+        return pos4
+
     def set_profiling(self, on: bool = True):
         check(self._lib.pppm_scene_set_profiling(self._h, int(on)), "pppm_scene_set_profiling")
 
@@ -246,6 +258,43 @@ def direct_sum_fp64(vort_pos4, alpha, eval_a, a: float, eval_b=None, is_segment:
                                  int(is_segment), float(a), _ptr(out[0]), _ptr(out[1]), _ptr(out[2]),
                                  _stream_handle(stream)), "pppm_direct_sum_fp64")
     return out.t()
+
+
+def batch_run(jobs, stream=None):
+    """Runs several independent scenes at once (pppm_batch_run).
+
+    jobs: list of (scene, pos4, alpha, eval_a or None, eval_b or None,
+    is_segment).  eval_a None evaluates at the vortices against themselves.
+    Returns a list of (M, 3) float64 velocity tensors, one per job."""
+    _require_cuda()
+    L = load()
+    items = (PppmBatchItem * len(jobs))()
+    keep, outs = [], []
+    for q, (scene, pos4, alpha, ea, eb, seg) in enumerate(jobs):
+        pos4 = _pos4(pos4)
+        N = pos4.shape[0]
+        ax, ay, az = _alpha3(alpha, N)
+        if ea is None:
+            ea, eb, seg = pos4, pos4, 1
+        ea = _pos4(ea)
+        eb = _pos4(eb) if eb is not None else None
+        M = ea.shape[0]
+        out = torch.empty((3, M), dtype=torch.float64, device=pos4.device)
+        it = items[q]
+        it.scene = scene.handle.value
+        it.N, it.pos4_dev = N, pos4.data_ptr()
+        it.ax_dev, it.ay_dev, it.az_dev = ax.data_ptr(), ay.data_ptr(), az.data_ptr()
+        it.M, it.eval_a4_dev = M, ea.data_ptr()
+        it.eval_b4_dev = eb.data_ptr() if eb is not None else None
+        it.is_segment = int(seg)
+        it.u_dev, it.v_dev, it.w_dev = out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr()
+        keep += [pos4, ax, ay, az, ea, eb]
+        outs.append(out)
+        scene.N = N
+    check(L.pppm_batch_run(items, len(jobs), _stream_handle(stream)), "pppm_batch_run")
+    torch.cuda.current_stream().synchronize() if stream is None else stream.synchronize()
+    del keep
+    return [o.t() for o in outs]
 
 
 class BiotSavartSolver:

@@ -26,7 +26,7 @@ EXPORTED = (
     "pppm_mg_full_multigrid", "pppm_hasher_create", "pppm_hasher_destroy", "pppm_hasher_run",
     "pppm_hasher_tables", "pppm_hasher_reorder", "pppm_hasher_deorder", "pppm_direct_sum_fp64",
     "pppm_scene_set_profiling", "pppm_stage_name", "pppm_get_stage_times", "pppm_kernel_launches",
-    "pppm_spatial_hash_noalloc",
+    "pppm_spatial_hash_noalloc", "pppm_advect_euler", "pppm_advect_rk2", "pppm_batch_run",
 )
 NOALLOC_MAX_PARTICLES = 1048576  # PPPM_NOALLOC_MAX_PARTICLES in include/pppm.h
 STAGES = ("domain", "vort_sort", "cells_reorder", "p2m", "multigrid", "farfield", "eval_sort", "eval")
@@ -44,6 +44,13 @@ class PppmParams(C.Structure):
         ("mg_tol", C.c_double),
         ("mg_max_cycles", C.c_int32),
     ]
+
+
+class PppmBatchItem(C.Structure):
+    _fields_ = [("scene", C.c_void_p), ("N", C.c_uint32), ("pos4_dev", C.c_void_p), ("ax_dev", C.c_void_p),
+                ("ay_dev", C.c_void_p), ("az_dev", C.c_void_p), ("M", C.c_uint32), ("eval_a4_dev", C.c_void_p),
+                ("eval_b4_dev", C.c_void_p), ("is_segment", C.c_int), ("u_dev", C.c_void_p), ("v_dev", C.c_void_p),
+                ("w_dev", C.c_void_p)]
 
 
 class PppmError(RuntimeError):
@@ -109,6 +116,9 @@ def load(build_if_missing: bool = True):
         "pppm_get_stage_times": (st, [vp, C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_int)]),
         "pppm_kernel_launches": (C.c_uint64, []),
         "pppm_spatial_hash_noalloc": (st, [u32, vp, u32, C.c_float, C.POINTER(C.c_float), vp, vp, vp, vp, vp]),
+        "pppm_advect_euler": (st, [vp, u32, vp, vp, vp, vp, C.c_double]),
+        "pppm_advect_rk2": (st, [vp, u32, vp, vp, vp, vp, C.c_double]),
+        "pppm_batch_run": (st, [C.POINTER(PppmBatchItem), u32, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

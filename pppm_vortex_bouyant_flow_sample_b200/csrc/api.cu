@@ -54,8 +54,11 @@ void free_vortex_side(pppm_scene *s) {
     cudaFree(s->vpos); s->vpos = nullptr;
     cudaFree(s->valpha); s->valpha = nullptr;
     for (int q = 0; q < 2; q++) { cudaFree(s->vkey[q]); cudaFree(s->vidx[q]); s->vkey[q] = s->vidx[q] = nullptr; }
+    for (int q = 0; q < 2; q++) { cudaFree(s->rkey[q]); cudaFree(s->ridx[q]); s->rkey[q] = s->ridx[q] = nullptr; }
+    s->ref_valid = false;
     cudaFree(s->vrec); s->vrec = nullptr;
     cudaFree(s->valf); s->valf = nullptr;
+    cudaFree(s->adv_mid); s->adv_mid = nullptr;
     cudaFree(s->bbox_partial); s->bbox_partial = nullptr;
 }
 
@@ -85,9 +88,12 @@ cudaError_t alloc_vortex_side(pppm_scene *s, uint32_t cap) {
     for (int q = 0; q < 2; q++) {
         PPPM_CUDA_TRY(dalloc(&s->vkey[q], cap));
         PPPM_CUDA_TRY(dalloc(&s->vidx[q], cap));
+        PPPM_CUDA_TRY(dalloc(&s->rkey[q], cap));
+        PPPM_CUDA_TRY(dalloc(&s->ridx[q], cap));
     }
     PPPM_CUDA_TRY(dalloc(&s->vrec, cap));
     PPPM_CUDA_TRY(dalloc(&s->valf, cap));
+    PPPM_CUDA_TRY(dalloc(&s->adv_mid, cap));
     s->bbox_blocks = 148 * 2;
     PPPM_CUDA_TRY(dalloc(&s->bbox_partial, 6 * (size_t)s->bbox_blocks));
     return alloc_hist(s);
@@ -130,11 +136,20 @@ cudaError_t alloc_grid_side(pppm_scene *s) {
     PPPM_CUDA_TRY(dalloc(&s->cell_start, s->C));
     PPPM_CUDA_TRY(dalloc(&s->cell_end, s->C));
     PPPM_CUDA_TRY(dalloc(&s->mflag, s->C));
+    PPPM_CUDA_TRY(dalloc(&s->sub_start, 8 * (size_t)s->C));
+    PPPM_CUDA_TRY(dalloc(&s->sub_end, 8 * (size_t)s->C));
     PPPM_CUDA_TRY(cudaMemset(s->mflag, 0, sizeof(uint32_t) * s->C));
     PPPM_CUDA_TRY(dalloc(&s->dparams, 1));
     PPPM_CUDA_TRY(cudaMemset(s->dparams, 0, sizeof(pppm::DevParams)));
     PPPM_CUDA_TRY(dalloc(&s->norms, 2));
     PPPM_CUDA_TRY(dalloc(&s->pair_count, 1));
+    if (s->levels >= 2) {
+        const int dc = (int)s->lv[s->levels - 1].d;
+        const size_t cc = (size_t)dc * dc * dc;
+        PPPM_CUDA_TRY(dalloc(&s->coarse_op, cc * cc));
+        PPPM_CUDA_TRY(pppm::build_coarse_operator(dc, s->coarse_op, nullptr));
+        PPPM_CUDA_TRY(cudaDeviceSynchronize());
+    }
     return cudaSuccess;
 }
 
@@ -154,9 +169,13 @@ void destroy_scene(pppm_scene *s) {
     cudaFree(s->cell_start);
     cudaFree(s->cell_end);
     cudaFree(s->mflag);
+    cudaFree(s->sub_start);
+    cudaFree(s->sub_end);
     cudaFree(s->dparams);
     cudaFree(s->norms);
     cudaFree(s->pair_count);
+    cudaFree(s->coarse_op);
+    if (s->mg_graph) cudaGraphExecDestroy(s->mg_graph);
     delete s;
 }
 
@@ -306,6 +325,7 @@ extern "C" pppm_status pppm_build_far_field(pppm_scene *s) {
     prof_end(s, kStageFar);
     if (e != cudaSuccess) return cuda_fail("pppm_build_far_field", e);
     s->far_ready = true;
+    s->ref_valid = false;
     return PPPM_OK;
 }
 
@@ -392,6 +412,56 @@ extern "C" pppm_status pppm_solve_host(pppm_scene *s, uint32_t N, const float *p
     return rc;
 }
 
+// Velocity of the vortices at positions `pos` (self evaluation) into the
+// scene's staging buffer; strengths must already be in the scene.
+static pppm_status self_velocity(pppm_scene *s, uint32_t N, const float4 *pos) {
+    cudaError_t e = cudaMemcpyAsync(s->vpos, pos, sizeof(float4) * N, cudaMemcpyDeviceToDevice, s->stream);
+    if (e != cudaSuccess) return cuda_fail("advect (positions)", e);
+    s->far_ready = false;
+    pppm_status rc = pppm_build_far_field(s);
+    if (rc != PPPM_OK) return rc;
+    if (N > s->capM) {
+        e = alloc_eval_side(s, N);
+        if (e != cudaSuccess) return cuda_fail("advect (grow eval buffers)", e);
+    }
+    const float *p = reinterpret_cast<const float *>(s->vpos);
+    return eval_common(s, N, p, p, 1, s->stage_out, s->stage_out + s->capM, s->stage_out + 2 * (size_t)s->capM,
+                       nullptr, 0);
+}
+
+static pppm_status advect_common(pppm_scene *s, uint32_t N, float *pos4, const double *ax, const double *ay,
+                                 const double *az, double dt, bool rk2) {
+    if (!s || !pos4 || !ax || !ay || !az || N == 0 || !std::isfinite(dt)) {
+        snprintf(g_err, sizeof(g_err), "pppm_advect: invalid argument");
+        return PPPM_ERR_INVALID;
+    }
+    pppm_status rc = pppm_set_vortices(s, N, pos4, ax, ay, az);
+    if (rc != PPPM_OK) return rc;
+    float4 *x = reinterpret_cast<float4 *>(pos4);
+    rc = self_velocity(s, N, x);
+    if (rc != PPPM_OK) return rc;
+    cudaError_t e;
+    if (rk2) {
+        e = pppm::launch_move(s, x, s->stage_out, s->capM, 0.5 * dt, N, s->adv_mid);
+        if (e != cudaSuccess) return cuda_fail("pppm_advect_rk2 (midpoint)", e);
+        rc = self_velocity(s, N, s->adv_mid);
+        if (rc != PPPM_OK) return rc;
+    }
+    e = pppm::launch_move(s, x, s->stage_out, s->capM, dt, N, x);
+    if (e != cudaSuccess) return cuda_fail("pppm_advect (move)", e);
+    return PPPM_OK;
+}
+
+extern "C" pppm_status pppm_advect_euler(pppm_scene *s, uint32_t N, float *pos4, const double *ax, const double *ay,
+                                         const double *az, double dt) {
+    return advect_common(s, N, pos4, ax, ay, az, dt, false);
+}
+
+extern "C" pppm_status pppm_advect_rk2(pppm_scene *s, uint32_t N, float *pos4, const double *ax, const double *ay,
+                                       const double *az, double dt) {
+    return advect_common(s, N, pos4, ax, ay, az, dt, true);
+}
+
 extern "C" pppm_status pppm_get_domain(pppm_scene *s, double origin[3], double *length, double *cell_h) {
     if (!s) return PPPM_ERR_INVALID;
     if (!s->far_ready) { snprintf(g_err, sizeof(g_err), "pppm_get_domain: no far field built"); return PPPM_ERR_STATE; }
@@ -417,8 +487,13 @@ extern "C" pppm_status pppm_get_cell_tables(pppm_scene *s, const uint32_t **star
 extern "C" pppm_status pppm_get_sorted_index(pppm_scene *s, const uint32_t **key, const uint32_t **idx) {
     if (!s) return PPPM_ERR_INVALID;
     if (!s->far_ready) { snprintf(g_err, sizeof(g_err), "pppm_get_sorted_index: no far field built"); return PPPM_ERR_STATE; }
-    if (key) *key = s->vsorted_key;
-    if (idx) *idx = s->vsorted_idx;
+    if (!s->ref_valid) {
+        cudaError_t e = pppm::launch_reference_order(s);
+        if (e != cudaSuccess) return cuda_fail("pppm_get_sorted_index", e);
+        s->ref_valid = true;
+    }
+    if (key) *key = s->ref_sorted_key;
+    if (idx) *idx = s->ref_sorted_idx;
     return PPPM_OK;
 }
 
@@ -430,6 +505,11 @@ extern "C" pppm_status pppm_get_sorted_vortices(pppm_scene *s, float *pos4, doub
     }
     double *tmp = nullptr;
     cudaError_t e = cudaSuccess;
+    if (!s->ref_valid) {
+        e = pppm::launch_reference_order(s);
+        if (e != cudaSuccess) return cuda_fail("pppm_get_sorted_vortices", e);
+        s->ref_valid = true;
+    }
     if (ax || ay || az) e = cudaMalloc(&tmp, sizeof(double) * 3 * (size_t)s->N);
     if (e == cudaSuccess) e = pppm::launch_gather_sorted(s, reinterpret_cast<float4 *>(pos4), tmp);
     const size_t N = s->N;

@@ -19,7 +19,7 @@
 //     which equals (1 - e^-(r/a)^3) / (4 pi r^3); pairs with r = 0, or (for
 //     segments) a zero distance to the other end, are skipped.
 // Pair arithmetic is FP32 (r from rsqrt, ~1 ulp); phi uses its Taylor series
-// below t = 0.5 (no cancellation) and (1 - exp(-t)) / t above.
+// below t = 0.25 (no cancellation) and (1 - exp(-t)) / t above.
 #include <climits>
 
 #include "pppm_internal.cuh"
@@ -30,27 +30,13 @@ namespace {
 
 constexpr int kEvalThreads = 128;
 
-__device__ __forceinline__ float phi_smooth(float t) {
-    if (t < 0.5f) {  // truncation error < t^8/9! <= 1.1e-8 relative
-        float p = -1.0f / 40320.0f;
-        p = fmaf(p, t, 1.0f / 5040.0f);
-        p = fmaf(p, t, -1.0f / 720.0f);
-        p = fmaf(p, t, 1.0f / 120.0f);
-        p = fmaf(p, t, -1.0f / 24.0f);
-        p = fmaf(p, t, 1.0f / 6.0f);
-        p = fmaf(p, t, -0.5f);
-        return fmaf(p, t, 1.0f);
-    }
-    return __fdividef(1.0f - __expf(-t), t);
-}
-
 __device__ __forceinline__ float3 rel_pos(float4 p, const DevParams *__restrict__ P) {
     return make_float3((float)((double)p.x - P->origin[0]), (float)((double)p.y - P->origin[1]),
                        (float)((double)p.z - P->origin[2]));
 }
 
-// Evaluation order: NGP cell * 8 + octant of the point inside its cell
-// (points outside the grid last).  A warp of consecutive points then shares
+// Evaluation order: NGP cell * 8 + Gray rank of the point's octant inside its
+// cell (points outside the grid last).  A warp of consecutive points then shares
 // one cell octant, whose near-field boxes span 2K+2 cells per axis instead of
 // the reference's 2K+3.  The order is internal: results return in caller order.
 __global__ void eval_keys_kernel(const float4 *__restrict__ eval_a, uint32_t M, const DevParams *__restrict__ P,
@@ -66,7 +52,11 @@ __global__ void eval_keys_kernel(const float4 *__restrict__ eval_a, uint32_t M, 
     uint32_t k = 8u * n * n * n;
     if (fx >= 0.0 && fx < dn && fy >= 0.0 && fy < dn && fz >= 0.0 && fz < dn) {
         const uint32_t oct = (qx - fx >= 0.5 ? 1u : 0u) | (qy - fy >= 0.5 ? 2u : 0u) | (qz - fz >= 0.5 ? 4u : 0u);
-        k = ((((uint32_t)fz * n + (uint32_t)fy) * n + (uint32_t)fx) << 3) | oct;
+        // octants in Gray-code order (0,1,3,2,6,7,5,4): neighbouring groups differ
+        // along one axis, so a warp spanning two groups widens its walk by one
+        // half-cell on one axis only
+        const uint32_t rank = (0x54672310u >> (4 * oct)) & 7u;
+        k = ((((uint32_t)fz * n + (uint32_t)fy) * n + (uint32_t)fx) << 3) | rank;
     }
     key[t] = k;
     idx[t] = t;
@@ -77,25 +67,49 @@ struct PairAcc {
     unsigned long long n = 0;
 };
 
-// One candidate pair: box test, then the smoothed Biot-Savart term.
-// SEG: test the segment's other end; COUNT: count the pairs inside the box.
-template <bool SEG, bool COUNT>
-__device__ __forceinline__ void pair_term(const float4 r, const float4 *__restrict__ al_src, bool lane_ok,
-                                          const float3 ra, const float3 rb, float cr, float inv_a3, float inv4pia3,
+// phi(t) = (1 - e^-t) / t, scaled by 1/(4 pi a^3).  Below t = 0.25 the
+// degree-5 Taylor series (relative truncation < t^6/7! < 5e-8) needs no
+// special function; above it, (1 - exp(-t)) / t.  The exp branch is taken
+// only when some lane of the warp needs it (UNIFORM: the whole warp executes
+// this call together; otherwise each lane branches on its own t).
+template <bool UNIFORM>
+__device__ __forceinline__ float smooth_coeff(float t, float inv4pia3, bool need_exp) {
+    float p = -1.0f / 720.0f;
+    p = fmaf(p, t, 1.0f / 120.0f);
+    p = fmaf(p, t, -1.0f / 24.0f);
+    p = fmaf(p, t, 1.0f / 6.0f);
+    p = fmaf(p, t, -0.5f);
+    p = fmaf(p, t, 1.0f);
+    if (need_exp) {  // uniform: no pair of the scene reaches t = 0.25 otherwise
+        const bool big = t >= 0.25f;
+        if (UNIFORM ? __any_sync(0xffffffffu, big) : big) {
+            const float e = __fdividef(1.0f - __expf(-t), fmaxf(t, 0.25f));
+            p = big ? e : p;
+        }
+    }
+    return p * inv4pia3;
+}
+
+// One candidate pair, branch free: the box test, the lane's cell range and
+// the zero-distance exclusions become a zero coefficient.  SEG: test the
+// segment's other end; COUNT: count the pairs inside the box.
+template <bool SEG, bool COUNT, bool UNIFORM>
+__device__ __forceinline__ void pair_term(const float4 r, const float4 al, bool lane_ok, const float3 ra,
+                                          const float3 rb, float cr, float inv_a3, float inv4pia3, bool need_exp,
                                           PairAcc &acc) {
     const float dx = ra.x - r.x, dy = ra.y - r.y, dz = ra.z - r.z;
-    if (!(lane_ok && fmaxf(fabsf(dx), fmaxf(fabsf(dy), fabsf(dz))) <= cr)) return;
-    if (COUNT) acc.n++;
+    const float m = fmaxf(fabsf(dx), fmaxf(fabsf(dy), fabsf(dz)));
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-    bool skip = r2 < 1e-24f;
+    const bool inbox = lane_ok && m <= cr;
+    if (COUNT) acc.n += inbox ? 1ull : 0ull;
+    bool ok = inbox && !(r2 < 1e-24f);
     if (SEG) {
         const float ex = rb.x - r.x, ey = rb.y - r.y, ez = rb.z - r.z;
-        skip |= fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < 1e-24f;
+        ok = ok && !(fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < 1e-24f);
     }
-    if (skip) return;
-    const float rr = r2 * rsqrtf(r2);  // r2 >= 1e-24 here
-    const float coeff = phi_smooth(r2 * rr * inv_a3) * inv4pia3;
-    const float4 al = *al_src;
+    const float rr = r2 * rsqrtf(fmaxf(r2, 1e-30f));
+    const float c = smooth_coeff<UNIFORM>(r2 * rr * inv_a3, inv4pia3, need_exp);
+    const float coeff = ok ? c : 0.0f;
     acc.x = fmaf(al.y * dz - al.z * dy, coeff, acc.x);
     acc.y = fmaf(al.z * dx - al.x * dz, coeff, acc.y);
     acc.z = fmaf(al.x * dy - al.y * dx, coeff, acc.z);
@@ -105,9 +119,9 @@ __device__ __forceinline__ void pair_term(const float4 r, const float4 *__restri
 template <bool SEG, bool COUNT>
 __device__ __forceinline__ void cell_pairs(const float4 *__restrict__ vrec, const float4 *__restrict__ valf,
                                            uint32_t ps, uint32_t pe, bool lane_ok, const float3 ra, const float3 rb,
-                                           float cr, float inv_a3, float inv4pia3, PairAcc &acc) {
+                                           float cr, float inv_a3, float inv4pia3, bool need_exp, PairAcc &acc) {
     for (uint32_t p = ps; p < pe; p++)
-        pair_term<SEG, COUNT>(vrec[p], valf + p, lane_ok, ra, rb, cr, inv_a3, inv4pia3, acc);
+        pair_term<SEG, COUNT, false>(vrec[p], valf[p], lane_ok, ra, rb, cr, inv_a3, inv4pia3, need_exp, acc);
 }
 
 // Warp-uniform version: the warp copies the cell's records into its shared
@@ -117,8 +131,8 @@ template <bool SEG, bool COUNT>
 __device__ __forceinline__ void cell_pairs_staged(const float4 *__restrict__ vrec, const float4 *__restrict__ valf,
                                                   uint32_t ps, uint32_t pe, bool lane_ok, const float3 ra,
                                                   const float3 rb, float cr, float inv_a3, float inv4pia3,
-                                                  float4 *__restrict__ sv, float4 *__restrict__ sa, int lane,
-                                                  PairAcc &acc) {
+                                                  bool need_exp, float4 *__restrict__ sv, float4 *__restrict__ sa,
+                                                  int lane, PairAcc &acc) {
     for (uint32_t base = ps; base < pe; base += 32) {
         const uint32_t cnt = min(32u, pe - base);
         if ((uint32_t)lane < cnt) {
@@ -126,20 +140,22 @@ __device__ __forceinline__ void cell_pairs_staged(const float4 *__restrict__ vre
             sa[lane] = valf[base + lane];
         }
         __syncwarp();
+#pragma unroll 2
         for (uint32_t q = 0; q < cnt; q++)
-            pair_term<SEG, COUNT>(sv[q], sa + q, lane_ok, ra, rb, cr, inv_a3, inv4pia3, acc);
+            pair_term<SEG, COUNT, true>(sv[q], sa[q], lane_ok, ra, rb, cr, inv_a3, inv4pia3, need_exp, acc);
         __syncwarp();
     }
 }
 
-constexpr int kUniformMaxCells = 216;  // warp-uniform walk up to 6^3 cells
+constexpr int kUniformMaxSub = 1000;  // warp-uniform walk up to 10^3 half-cells
 
 // SEG: is_segment == 1 with a distinct other-end array (with eval_b == eval_a
 // the other-end test is the r = 0 test itself, so SEG is off).
 template <bool SEG, bool COUNT>
 __global__ void eval_kernel(const uint32_t *__restrict__ eidx, uint32_t M, const float4 *__restrict__ eval_a,
             const float4 *__restrict__ eval_b, const float *__restrict__ far,
-            const uint32_t *__restrict__ start, const uint32_t *__restrict__ end, const float4 *__restrict__ vrec,
+            const uint32_t *__restrict__ start, const uint32_t *__restrict__ end,
+            const uint32_t *__restrict__ sub_start, const uint32_t *__restrict__ sub_end, const float4 *__restrict__ vrec,
             const float4 *__restrict__ valf, const DevParams *__restrict__ P, int n, int K,
             double *__restrict__ u, double *__restrict__ v, double *__restrict__ w, float *__restrict__ uf,
             unsigned long long *__restrict__ pair_count) {
@@ -179,17 +195,22 @@ __global__ void eval_kernel(const uint32_t *__restrict__ eidx, uint32_t M, const
     PairAcc acc;
     if (K >= 0) {
         const float cr = P->cr_f, inv_a3 = P->inv_a3_f, inv4pia3 = P->inv4pia3_f;
-        // The reference walks hash cells [i-K-1, i+K+1]^3.  Only cells that can
-        // hold a vortex inside the point's box are visited: the box spans
-        // (K+0.5) cells either side, widened by the hash/NGP rounding bound.
+        const bool need_exp = P->need_exp != 0;
+        // The reference walks hash cells [i-K-1, i+K+1]^3.  Only the half-cells
+        // (cell, octant runs of the vortex order) that can hold a vortex inside
+        // the point's box are visited: the box spans K+0.5 cells either side,
+        // widened by the hash/NGP rounding bound.  Coordinates below are in
+        // half cells.
         const double R = (double)K + 0.5 + P->prune_cells;
-        int lo[3], hi[3];
+        int lo[3], hi[3], rlo[3], rhi[3];
         const double qq[3] = {qx, qy, qz};
         const int cc[3] = {i, j, k};
 #pragma unroll
         for (int a = 0; a < 3; a++) {
-            lo[a] = max(max(cc[a] - K - 1, 0), (int)floor(qq[a] - R));
-            hi[a] = min(min(cc[a] + K + 1, n - 1), (int)floor(qq[a] + R));
+            rlo[a] = cc[a] - K - 1;
+            rhi[a] = cc[a] + K + 1;
+            lo[a] = max(max(2 * rlo[a], 0), (int)floor(2.0 * (qq[a] - R)));
+            hi[a] = min(min(2 * rhi[a] + 1, 2 * n - 1), (int)floor(2.0 * (qq[a] + R)));
             if (!act || lo[a] > hi[a]) { lo[a] = INT_MAX; hi[a] = INT_MIN; }
         }
         int ulo[3], uhi[3];
@@ -201,28 +222,41 @@ __global__ void eval_kernel(const uint32_t *__restrict__ eidx, uint32_t M, const
         long long vol = 1;
 #pragma unroll
         for (int a = 0; a < 3; a++) vol *= (uhi[a] >= ulo[a]) ? (long long)(uhi[a] - ulo[a] + 1) : 0ll;
-        if (vol > 0 && vol <= kUniformMaxCells) {
-            // warp-uniform walk: every lane sees the same cell and vortex at once
-            for (int kk = ulo[2]; kk <= uhi[2]; kk++)
-                for (int jj = ulo[1]; jj <= uhi[1]; jj++)
-                    for (int ii = ulo[0]; ii <= uhi[0]; ii++) {
-                        const uint32_t cell = ((uint32_t)kk * n + (uint32_t)jj) * n + (uint32_t)ii;
-                        const uint32_t ps = start[cell];
+        if (vol > 0 && vol <= kUniformMaxSub) {
+            // warp-uniform walk over half-cells: every lane sees the same vortex at once
+            for (int k2 = ulo[2]; k2 <= uhi[2]; k2++)
+                for (int j2 = ulo[1]; j2 <= uhi[1]; j2++)
+                    for (int i2 = ulo[0]; i2 <= uhi[0];) {
+                        // the two x-halves of a cell are adjacent runs: walk them as one
+                        const bool both = ((i2 & 1) == 0) && (i2 + 1 <= uhi[0]);
+                        const int ci = i2 >> 1, cj = j2 >> 1, ck = k2 >> 1;
+                        const uint32_t cell = ((uint32_t)ck * n + (uint32_t)cj) * n + (uint32_t)ci;
+                        const uint32_t k0 = (cell << 3) | ((uint32_t)(j2 & 1) << 1) | ((uint32_t)(k2 & 1) << 2) |
+                                            (uint32_t)(i2 & 1);
+                        uint32_t ps = sub_start[k0], pe = sub_end[k0];
+                        if (both) {
+                            const uint32_t s1 = sub_start[k0 | 1u];
+                            if (s1 != kEmpty) {
+                                if (ps == kEmpty) ps = s1;
+                                pe = sub_end[k0 | 1u];
+                            }
+                        }
+                        i2 += both ? 2 : 1;
                         if (ps == kEmpty) continue;
-                        const bool lane_ok = ii >= lo[0] && ii <= hi[0] && jj >= lo[1] && jj <= hi[1] &&
-                                             kk >= lo[2] && kk <= hi[2];
-                        cell_pairs_staged<SEG, COUNT>(vrec, valf, ps, end[cell], lane_ok, ra, rb, cr, inv_a3, inv4pia3, sv, sa,
-                                                      lane, acc);
+                        const bool lane_ok = act && ci >= rlo[0] && ci <= rhi[0] && cj >= rlo[1] && cj <= rhi[1] &&
+                                             ck >= rlo[2] && ck <= rhi[2];
+                        cell_pairs_staged<SEG, COUNT>(vrec, valf, ps, pe, lane_ok, ra, rb, cr, inv_a3, inv4pia3,
+                                                      need_exp, sv, sa, lane, acc);
                     }
         } else if (act && lo[0] <= hi[0]) {
             // scattered warp (points outside the grid, sparse regions): own walk
-            for (int kk = lo[2]; kk <= hi[2]; kk++)
-                for (int jj = lo[1]; jj <= hi[1]; jj++)
-                    for (int ii = lo[0]; ii <= hi[0]; ii++) {
+            for (int kk = lo[2] >> 1; kk <= (hi[2] >> 1); kk++)
+                for (int jj = lo[1] >> 1; jj <= (hi[1] >> 1); jj++)
+                    for (int ii = lo[0] >> 1; ii <= (hi[0] >> 1); ii++) {
                         const uint32_t cell = ((uint32_t)kk * n + (uint32_t)jj) * n + (uint32_t)ii;
                         const uint32_t ps = start[cell];
                         if (ps == kEmpty) continue;
-                        cell_pairs<SEG, COUNT>(vrec, valf, ps, end[cell], true, ra, rb, cr, inv_a3, inv4pia3, acc);
+                        cell_pairs<SEG, COUNT>(vrec, valf, ps, end[cell], true, ra, rb, cr, inv_a3, inv4pia3, need_exp, acc);
                     }
         }
     }
@@ -269,7 +303,8 @@ cudaError_t launch_eval(pppm_scene *s, const float4 *eval_a, const float4 *eval_
     const bool seg = (is_segment == 1) && (eval_b != eval_a);
     const unsigned grid = (M + kEvalThreads - 1) / kEvalThreads;
     unsigned long long *pc = count_pairs ? s->pair_count : nullptr;
-#define PPPM_EVAL_ARGS sidx, M, eval_a, eval_b, s->far, s->cell_start, s->cell_end, s->vrec, s->valf, s->dparams, \
+#define PPPM_EVAL_ARGS sidx, M, eval_a, eval_b, s->far, s->cell_start, s->cell_end, s->sub_start, s->sub_end, \
+                       s->vrec, s->valf, s->dparams, \
                        (int)s->n, s->prm.K, u, v, w, uf, pc
     if (seg) {
         if (count_pairs) eval_kernel<true, true><<<grid, kEvalThreads, 0, s->stream>>>(PPPM_EVAL_ARGS);

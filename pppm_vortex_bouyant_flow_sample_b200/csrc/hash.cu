@@ -116,6 +116,12 @@ __global__ void params_kernel(const float *__restrict__ partial, int nblocks, pp
     const double a = prm.a;
     P->inv_a3_f = (float)(1.0 / (a * a * a));
     P->inv4pia3_f = (float)(1.0 / (kFourPi * a * a * a));
+    {
+        // farthest pair the box admits: (K+0.5) h along each axis
+        const double rmax = ((double)prm.K + 0.5) * h * 1.7320508075688772 * 1.001;
+        const double tmax = (rmax / a) * (rmax / a) * (rmax / a);
+        P->need_exp = !(tmax < 0.25);
+    }
     // The FP32 hash coordinate fl(fl(p - o_f) / h_f) and the FP64 NGP coordinate
     // fl32(p - o) / h differ by at most a few float roundings of |p| + |o| over h;
     // 2^-20 covers them with a factor > 4 to spare.  The box test adds the
@@ -142,12 +148,39 @@ __device__ __forceinline__ uint32_t cell_key(float4 p, const float *of, float h,
     return umul24u(umul24u(uz, n), n) + umul24u(uy, n) + ux;
 }
 
+// Reference cell keys (the order getSortPos / the ParticleManager tables use).
 __global__ void keys_kernel(const float4 *__restrict__ pos, uint32_t N, const DevParams *__restrict__ P,
                             uint32_t *__restrict__ key, uint32_t *__restrict__ idx) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= N) return;
     const float of[3] = {P->origin_f[0], P->origin_f[1], P->origin_f[2]};
     key[t] = cell_key(pos[t], of, P->h_f, P->n);
+    idx[t] = t;
+}
+
+// Near-field order: the reference cell key, then the octant of the vortex
+// inside that cell (FP64 coordinate relative to the FP32 hash cell, so a
+// vortex that rounding put in a neighbouring hash cell still lands in the
+// sub-cell nearest to it).  Key = cell * 8 + octant.
+__global__ void keys_octant_kernel(const float4 *__restrict__ pos, uint32_t N, const DevParams *__restrict__ P,
+                                   uint32_t *__restrict__ key, uint32_t *__restrict__ idx) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= N) return;
+    const float4 p = pos[t];
+    const float h = P->h_f;
+    const int gx = (int)floorf(__fdiv_rn(__fsub_rn(p.x, P->origin_f[0]), h));
+    const int gy = (int)floorf(__fdiv_rn(__fsub_rn(p.y, P->origin_f[1]), h));
+    const int gz = (int)floorf(__fdiv_rn(__fsub_rn(p.z, P->origin_f[2]), h));
+    const uint32_t n = P->n;
+    const uint32_t ux = (uint32_t)gx % n, uy = (uint32_t)gy % n, uz = (uint32_t)gz % n;
+    const uint32_t ck = umul24u(umul24u(uz, n), n) + umul24u(uy, n) + ux;
+    const double invh = P->invh;
+    const double qx = (double)(float)((double)p.x - P->origin[0]) * invh;
+    const double qy = (double)(float)((double)p.y - P->origin[1]) * invh;
+    const double qz = (double)(float)((double)p.z - P->origin[2]) * invh;
+    const uint32_t oct = (qx - (double)gx >= 0.5 ? 1u : 0u) | (qy - (double)gy >= 0.5 ? 2u : 0u) |
+                         (qz - (double)gz >= 0.5 ? 4u : 0u);
+    key[t] = (ck << 3) | oct;
     idx[t] = t;
 }
 
@@ -278,22 +311,31 @@ __device__ __forceinline__ uint32_t ngp_cell(float rx, float ry, float rz, doubl
     return ((uint32_t)qz * n + (uint32_t)qy) * n + (uint32_t)qx;
 }
 
-// Cell tables + reorder + relative coordinates + NGP cell, one thread per
-// sorted slot.  start/end were set to kEmpty beforehand.
+// Cell and sub-cell tables + reorder + relative coordinates + NGP cell, one
+// thread per sorted slot (keys are cell * 8 + octant).  All tables were set
+// to kEmpty beforehand.
 __global__ void cells_reorder_kernel(const uint32_t *__restrict__ skey, const uint32_t *__restrict__ sidx,
                                      uint32_t N, const float4 *__restrict__ pos,
                                      const double *__restrict__ alpha, uint32_t capN,
                                      const DevParams *__restrict__ P, uint32_t *__restrict__ start,
-                                     uint32_t *__restrict__ end, uint32_t *__restrict__ mflag, uint32_t epoch,
+                                     uint32_t *__restrict__ end, uint32_t *__restrict__ sub_start,
+                                     uint32_t *__restrict__ sub_end, uint32_t *__restrict__ mflag, uint32_t epoch,
                                      float4 *__restrict__ vrec, float4 *__restrict__ valf) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= N) return;
-    const uint32_t key = skey[s];
-    if (s == 0 || key != skey[s - 1]) {
+    const uint32_t skk = skey[s];
+    const uint32_t prev = (s > 0) ? skey[s - 1] : 0u;
+    const uint32_t key = skk >> 3;
+    if (s == 0 || key != (prev >> 3)) {
         start[key] = s;
-        if (s > 0) end[skey[s - 1]] = s;
+        if (s > 0) end[prev >> 3] = s;
     }
     if (s == N - 1) end[key] = N;
+    if (s == 0 || skk != prev) {
+        sub_start[skk] = s;
+        if (s > 0) sub_end[prev] = s;
+    }
+    if (s == N - 1) sub_end[skk] = N;
     const uint32_t i = sidx[s];
     const float4 p = pos[i];
     const float rx = (float)((double)p.x - P->origin[0]);
@@ -391,15 +433,27 @@ cudaError_t radix_sort_pairs(cudaStream_t st, uint32_t N, uint32_t bits, uint32_
 cudaError_t launch_hash_sort(pppm_scene *s, const float4 *pos, uint32_t N, uint32_t *key[2], uint32_t *idx[2],
                              uint32_t **sorted_key, uint32_t **sorted_idx) {
     ::pppm::note_launch();
-    keys_kernel<<<blocks_for(N, 256), 256, 0, s->stream>>>(pos, N, s->dparams, key[0], idx[0]);
+    keys_octant_kernel<<<blocks_for(N, 256), 256, 0, s->stream>>>(pos, N, s->dparams, key[0], idx[0]);
     PPPM_CUDA_TRY(cudaGetLastError());
-    return radix_sort_pairs(s->stream, N, key_bits(s->n), key, idx, s->hist, sorted_key, sorted_idx);
+    return radix_sort_pairs(s->stream, N, key_bits(s->n) + 3, key, idx, s->hist, sorted_key, sorted_idx);
+}
+
+// The reference's order (stable by original index inside each cell), built
+// on request for the accessors; the near field uses the octant order.
+cudaError_t launch_reference_order(pppm_scene *s) {
+    ::pppm::note_launch();
+    keys_kernel<<<blocks_for(s->N, 256), 256, 0, s->stream>>>(s->vpos, s->N, s->dparams, s->rkey[0], s->ridx[0]);
+    PPPM_CUDA_TRY(cudaGetLastError());
+    return radix_sort_pairs(s->stream, s->N, key_bits(s->n), s->rkey, s->ridx, s->hist, &s->ref_sorted_key,
+                            &s->ref_sorted_idx);
 }
 
 cudaError_t launch_cells_reorder(pppm_scene *s) {
     const size_t tbytes = sizeof(uint32_t) * (size_t)s->C;
     PPPM_CUDA_TRY(cudaMemsetAsync(s->cell_start, 0xFF, tbytes, s->stream));
     PPPM_CUDA_TRY(cudaMemsetAsync(s->cell_end, 0xFF, tbytes, s->stream));
+    PPPM_CUDA_TRY(cudaMemsetAsync(s->sub_start, 0xFF, 8 * tbytes, s->stream));
+    PPPM_CUDA_TRY(cudaMemsetAsync(s->sub_end, 0xFF, 8 * tbytes, s->stream));
     s->epoch++;
     if (s->epoch == 0) {  // wrapped: restart the mismatch flags
         PPPM_CUDA_TRY(cudaMemsetAsync(s->mflag, 0, tbytes, s->stream));
@@ -408,14 +462,14 @@ cudaError_t launch_cells_reorder(pppm_scene *s) {
     ::pppm::note_launch();
     cells_reorder_kernel<<<blocks_for(s->N, 256), 256, 0, s->stream>>>(
         s->vsorted_key, s->vsorted_idx, s->N, s->vpos, s->valpha, s->capN, s->dparams, s->cell_start,
-        s->cell_end, s->mflag, s->epoch, s->vrec, s->valf);
+        s->cell_end, s->sub_start, s->sub_end, s->mflag, s->epoch, s->vrec, s->valf);
     return cudaGetLastError();
 }
 
 cudaError_t launch_gather_sorted(pppm_scene *s, float4 *pos_out, double *alpha_out) {
     ::pppm::note_launch();
     gather_sorted_kernel<<<blocks_for(s->N, 256), 256, 0, s->stream>>>(
-        s->vsorted_idx, s->N, s->vpos, s->valpha, s->capN, pos_out, alpha_out,
+        s->ref_sorted_idx, s->N, s->vpos, s->valpha, s->capN, pos_out, alpha_out,
         alpha_out ? alpha_out + s->N : nullptr, alpha_out ? alpha_out + 2 * (size_t)s->N : nullptr);
     return cudaGetLastError();
 }

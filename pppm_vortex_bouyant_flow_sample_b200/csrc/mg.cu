@@ -135,6 +135,48 @@ __global__ void __launch_bounds__(512) coarse_kernel(float *__restrict__ x, cons
     if (t < cells) x[comp * cells + t] = (float)cur[t];
 }
 
+// The coarsest solve always starts from x = 0 in the reference schedule at
+// two or more levels, so its 100 Jacobi sweeps are one fixed linear map
+// x = P b.  Column j of P is the sweep applied to the unit vector e_j (one
+// block per column); P is stored row-major [row][col].
+__global__ void __launch_bounds__(512) coarse_op_column_kernel(double *__restrict__ op, int d) {
+    __shared__ double xa[512], xb[512];
+    const int cells = d * d * d;
+    const int col = blockIdx.x;
+    const int t = threadIdx.x;
+    if (t < cells) xa[t] = 0.0;
+    __syncthreads();
+    const int i = t % d, j = (t / d) % d, k = t / (d * d);
+    double *cur = xa, *nxt = xb;
+    for (int it = 0; it < 100; it++) {
+        if (t < cells) {
+            double r = nb_sum64(cur, i, j, k, d, (size_t)t);
+            r -= (t == col) ? 1.0 : 0.0;
+            nxt[t] = r / 6;
+        }
+        __syncthreads();
+        double *tmp = cur; cur = nxt; nxt = tmp;
+    }
+    if (t < cells) op[(size_t)t * cells + col] = cur[t];
+}
+
+// x = P b per component: one warp per (row, component), lanes stride the row.
+__global__ void __launch_bounds__(256)
+coarse_apply_kernel(const double *__restrict__ op, float *__restrict__ x, const float *__restrict__ b, int cells,
+                    int comps) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= cells * comps) return;
+    const int row = warp % cells, comp = warp / cells;
+    const double *prow = op + (size_t)row * cells;
+    const float *bc = b + (size_t)comp * cells;
+    double acc = 0.0;
+    for (int c = lane; c < cells; c += 32) acc = fma(prow[c], (double)bc[c], acc);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) x[(size_t)comp * cells + row] = (float)acc;
+}
+
 // r = b - (sum_nbr(psi) - 6 psi) in FP64, stored as the FP32 right-hand side
 // of the correction equation.  b is read from b64 (FP64) or formed as
 // -(vort * h2f) from the FP32 P2M grid.  Optional squared norms of r and b.
@@ -185,7 +227,26 @@ __global__ void dc_update_kernel(double *__restrict__ psi, const float *__restri
 
 inline dim3 grid_for(uint32_t per, int comps) { return dim3((per + kMGThreads - 1) / kMGThreads, comps); }
 
+// Coarsest solve from x = 0: the precomputed operator when available, else
+// the sweeps themselves.
+void coarse_solve(const MGPlan &m) {
+    const Level &c = m.lv[m.levels - 1];
+    ::pppm::note_launch();
+    if (m.coarse_op && m.levels >= 2) {
+        const unsigned warps = c.cells * (unsigned)m.comps;
+        coarse_apply_kernel<<<(warps * 32 + 255) / 256, 256, 0, m.st>>>(m.coarse_op, c.x, c.b, (int)c.cells, m.comps);
+    } else {
+        coarse_kernel<<<m.comps, 512, 0, m.st>>>(c.x, c.b, (int)c.d);
+    }
+}
+
 }  // namespace
+
+cudaError_t build_coarse_operator(int d, double *op, cudaStream_t st) {
+    ::pppm::note_launch();
+    coarse_op_column_kernel<<<d * d * d, 512, 0, st>>>(op, d);
+    return cudaGetLastError();
+}
 
 int mg_level_count(uint32_t n) {
     // MG/MultiGrid.h:114-127
@@ -229,8 +290,7 @@ static cudaError_t vcycle32(const MGPlan &m, int level) {
         resid_restrict_kernel<<<grid_for(m.lv[j + 1].cells, m.comps), kMGThreads, 0, m.st>>>(
             m.lv[j].x, m.lv[j].b, m.lv[j + 1].b, (int)m.lv[j + 1].d, 0);
     }
-    ::pppm::note_launch();
-    coarse_kernel<<<m.comps, 512, 0, m.st>>>(m.lv[L - 1].x, m.lv[L - 1].b, (int)m.lv[L - 1].d);
+    coarse_solve(m);
     for (int j = L - 2; j >= level; j--) {
         const int d = (int)m.lv[j].d;
         ::pppm::note_launch();
@@ -258,8 +318,7 @@ static cudaError_t fmg32(const MGPlan &m) {
         resid_restrict_kernel<<<grid_for(m.lv[j + 1].cells, m.comps), kMGThreads, 0, m.st>>>(
             m.lv[j].x, m.lv[j].b, m.lv[j + 1].b, (int)m.lv[j + 1].d, 1);
     }
-    ::pppm::note_launch();
-    coarse_kernel<<<m.comps, 512, 0, m.st>>>(m.lv[L - 1].x, m.lv[L - 1].b, (int)m.lv[L - 1].d);
+    coarse_solve(m);
     PPPM_CUDA_TRY(cudaGetLastError());
     for (int j = L - 2; j >= 0; j--) {
         ::pppm::note_launch();
@@ -328,6 +387,28 @@ cudaError_t mg_solve(const MGPlan &m, int mode, double tol, int max_cycles, int 
     return cudaSuccess;
 }
 
+// Captures the reference-schedule solve (no host synchronisation inside) as a
+// CUDA graph on a private stream; the graph is replayed on the scene stream.
+cudaError_t mg_capture_graph(const MGPlan &m_in, cudaGraphExec_t *exec, unsigned *kernel_nodes) {
+    MGPlan m = m_in;
+    cudaStream_t cap = nullptr;
+    PPPM_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    m.st = cap;
+    cudaGraph_t g = nullptr;
+    const unsigned long long before = launch_count();
+    cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        cudaError_t body = mg_solve(m, PPPM_MG_REFERENCE, 0.0, 1, nullptr, nullptr);
+        e = cudaStreamEndCapture(cap, &g);
+        if (e == cudaSuccess) e = body;
+    }
+    *kernel_nodes = (unsigned)(launch_count() - before);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(exec, g, 0);
+    if (g) cudaGraphDestroy(g);
+    cudaStreamDestroy(cap);
+    return e;
+}
+
 cudaError_t run_multigrid(pppm_scene *s) {
     MGPlan m;
     m.levels = s->levels;
@@ -339,8 +420,17 @@ cudaError_t run_multigrid(pppm_scene *s) {
     m.vort = s->vort;
     m.P = s->dparams;
     m.norms = s->norms;
+    m.coarse_op = s->coarse_op;
     int cyc = 0;
     double rel = -1.0;
+    if (s->prm.mg_mode == PPPM_MG_REFERENCE) {
+        if (!s->mg_graph) PPPM_CUDA_TRY(mg_capture_graph(m, &s->mg_graph, &s->mg_graph_kernels));
+        PPPM_CUDA_TRY(cudaGraphLaunch(s->mg_graph, s->stream));
+        for (unsigned q = 0; q < s->mg_graph_kernels; q++) note_launch();
+        s->mg_cycles_last = 1;
+        s->mg_relres_last = -1.0;
+        return cudaSuccess;
+    }
     PPPM_CUDA_TRY(mg_solve(m, s->prm.mg_mode, s->prm.mg_tol, s->prm.mg_max_cycles, &cyc, &rel));
     s->mg_cycles_last = cyc;
     s->mg_relres_last = rel;

@@ -45,6 +45,7 @@ struct DevParams {
     float kdiag_f;      // (float)(0.5 * invh * 0.250580605913965 * h^2)
     float inv_a3_f;     // 1/a^3
     float inv4pia3_f;   // 1/(4 pi a^3)
+    int32_t need_exp;   // some pair inside the box can reach (r/a)^3 >= 0.25
     double prune_cells; // bound, in cells, on |hash cell coordinate - FP64 NGP coordinate|
                         // plus the float rounding of the box test (near-field cell pruning)
     uint32_t n;
@@ -70,7 +71,11 @@ struct MGPlan {
     const float *vort = nullptr;    // b = -(vort * h2f) from the P2M grid
     const DevParams *P = nullptr;
     double *norms = nullptr;        // [2] device scratch
+    const double *coarse_op = nullptr;  // [cells][cells] FP64 map b -> x of the coarsest solve, or null
 };
+
+cudaError_t build_coarse_operator(int d, double *op, cudaStream_t st);
+cudaError_t mg_capture_graph(const MGPlan &m, cudaGraphExec_t *exec, unsigned *kernel_nodes);
 
 }  // namespace pppm
 
@@ -97,10 +102,15 @@ struct pppm_scene {
     double *valpha = nullptr;             // caller order copy [3][capN]
     uint32_t *vkey[2] = {nullptr, nullptr};
     uint32_t *vidx[2] = {nullptr, nullptr};
-    uint32_t *vsorted_key = nullptr, *vsorted_idx = nullptr;  // point into vkey/vidx
+    uint32_t *vsorted_key = nullptr, *vsorted_idx = nullptr;  // near-field order, point into vkey/vidx
+    uint32_t *rkey[2] = {nullptr, nullptr};                   // reference order, built on request
+    uint32_t *ridx[2] = {nullptr, nullptr};
+    uint32_t *ref_sorted_key = nullptr, *ref_sorted_idx = nullptr;
+    bool ref_valid = false;
     float4 *vrec = nullptr;               // sorted {rel, ngp}
     float4 *valf = nullptr;               // sorted {alpha, 0}
     uint32_t *cell_start = nullptr, *cell_end = nullptr, *mflag = nullptr;
+    uint32_t *sub_start = nullptr, *sub_end = nullptr;   // [8 n^3] runs of (cell, octant)
     uint32_t epoch = 0;
 
     // radix-sort histogram scratch
@@ -113,6 +123,9 @@ struct pppm_scene {
     double *psi = nullptr;                // [3][C]
     float *far = nullptr;                 // [3][C]
     double *norms = nullptr;              // [2] residual / rhs squared norms
+    double *coarse_op = nullptr;          // coarsest-level operator (levels >= 2)
+    cudaGraphExec_t mg_graph = nullptr;   // reference-schedule solve, captured once
+    unsigned mg_graph_kernels = 0;
 
     // evaluation side
     uint32_t *ekey[2] = {nullptr, nullptr};
@@ -120,6 +133,7 @@ struct pppm_scene {
     uint32_t *esorted_idx = nullptr;
     float4 *stage_ea = nullptr, *stage_eb = nullptr;  // pppm_solve_host staging [capM]
     double *stage_out = nullptr;                       // [3][capM]
+    float4 *adv_mid = nullptr;                         // RK2 midpoint positions [capN]
 
     // per-stage CUDA-event timing (pppm_scene_set_profiling)
     bool profiling = false;
@@ -159,12 +173,15 @@ cudaError_t launch_bbox_and_params(pppm_scene *s);
 cudaError_t launch_hash_sort(pppm_scene *s, const float4 *pos, uint32_t N, uint32_t *key[2],
                              uint32_t *idx[2], uint32_t **sorted_key, uint32_t **sorted_idx);
 cudaError_t launch_cells_reorder(pppm_scene *s);
+cudaError_t launch_reference_order(pppm_scene *s);
 cudaError_t launch_p2m(pppm_scene *s);
 cudaError_t run_multigrid(pppm_scene *s);
 cudaError_t launch_farfield(pppm_scene *s);
 cudaError_t launch_eval(pppm_scene *s, const float4 *eval_a, const float4 *eval_b, int is_segment,
                         uint32_t M, double *u, double *v, double *w, float *uf, int count_pairs);
 cudaError_t launch_gather_sorted(pppm_scene *s, float4 *pos_out, double *alpha_out);
+cudaError_t launch_move(pppm_scene *s, const float4 *base, const double *u, size_t stride, double dt, uint32_t N,
+                        float4 *out);
 
 cudaError_t mg_solve(const MGPlan &m, int mode, double tol, int max_cycles, int *cycles_out,
                      double *relres_out);

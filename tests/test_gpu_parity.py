@@ -186,3 +186,58 @@ def test_direct_sum_gpu_matches_oracle(pb, oracle):
     u = pb.direct_sum_fp64(_dev(pos), _dev(al), _dev(pos), 0.08, _dev(pos), 1).cpu().numpy()
     ref = oracle.direct_sum(pos, al, pos, 0.08, pos, 1)
     assert rel_l2(u, ref) <= 1e-12
+
+
+def _orc_move(pos, u, dt):
+    """move_particle (HFS/GPU_kernel.cu:3118-3140): float(double(p) + u dt), w = 0."""
+    out = np.zeros_like(pos)
+    out[:, :3] = (pos[:, :3].astype(np.float64) + u * dt).astype(np.float32)
+    return out
+
+
+@pytest.mark.parametrize("method", ["euler", "rk2"])
+def test_advection_step(pb, oracle, method):
+    import torch
+    from pppm_vortex_bouyant_flow_sample_b200 import workloads as W
+    pos, al = W.vortex_ring(40000, seed=13)
+    n, dt = 64, 0.002
+    scene = pb.Scene(n, cap_vort=len(pos), cap_eval=len(pos))
+    dpos = torch.from_numpy(pos.copy()).cuda()
+    scene.advect(dpos, _dev(al), dt, method=method)
+    got = dpos.cpu().numpy()
+    prm = oracle.params(n)
+    u1, _ = oracle.pppm(prm, pos, al, pos, pos, 1)
+    if method == "rk2":
+        mid = _orc_move(pos, u1, 0.5 * dt)
+        u2, _ = oracle.pppm(prm, mid, al, mid, mid, 1)
+        ref = _orc_move(pos, u2, dt)
+    else:
+        ref = _orc_move(pos, u1, dt)
+    disp_got = got[:, :3].astype(np.float64) - pos[:, :3]
+    disp_ref = ref[:, :3].astype(np.float64) - pos[:, :3]
+    assert rel_l2(disp_got, disp_ref) <= 1e-4
+    assert np.all(got[:, 3] == 0.0)
+    scene.close()
+
+
+def test_batch_results_equal_alone(pb, oracle):
+    """Several scenes of different sizes in one pppm_batch_run give exactly
+    the velocities each scene gives alone (no cross-scene reduction)."""
+    from pppm_vortex_bouyant_flow_sample_b200 import workloads as W
+    specs = [(32, "cloud", 9000, 31), (48, "ring", 20000, 32), (64, "cloud", 15000, 33), (32, "ring", 5000, 34)]
+    alone, jobs, scenes = [], [], []
+    for n, kind, N, seed in specs:
+        pos, al = W.make_scene(kind, N, seed)
+        sc, u = _run(pb, n, pos, al)
+        alone.append(u)
+        sc.close()
+        s2 = pb.Scene(n, cap_vort=N, cap_eval=N)
+        scenes.append(s2)
+        jobs.append((s2, _dev(pos), _dev(al), None, None, 1))
+    together = pb.batch_run(jobs)
+    for u_alone, u_mix in zip(alone, together):
+        assert np.array_equal(u_alone, u_mix.cpu().numpy())
+    ref, _ = _orc(oracle, specs[1][0], *W.make_scene(specs[1][1], specs[1][2], specs[1][3]))
+    assert rel_l2(together[1].cpu().numpy(), ref) <= VEL_TOL
+    for s2 in scenes:
+        s2.close()
