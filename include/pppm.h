@@ -197,6 +197,51 @@ typedef struct pppm_batch_item {
 } pppm_batch_item;
 pppm_status pppm_batch_run(pppm_batch_item *items, uint32_t count, void *stream);
 
+/* ---- request loop over resident scenes ----------------------------------
+ * No reference counterpart.  Scenes are registered with host particles; a
+ * request asks for the velocity at a scene's particles (EVAL) or for `steps`
+ * RK2 steps of them (ADVANCE, dt).  `slots` worker threads, one CUDA stream
+ * each, serve requests as they arrive (continuous batching: new requests
+ * start as soon as a slot frees and overlap on the GPU).  A scene's device
+ * footprint is admitted against hbm_budget_bytes; idle resident scenes are
+ * evicted least recently used first, their positions saved to the host.
+ * Requests of one scene run in submission order.  Times are seconds on a
+ * monotonic host clock. */
+typedef struct pppm_server pppm_server;
+typedef struct pppm_server_config {
+    uint64_t hbm_budget_bytes;
+    uint32_t slots;
+} pppm_server_config;
+enum { PPPM_REQ_EVAL = 0, PPPM_REQ_ADVANCE = 1 };
+typedef struct pppm_request_info {
+    int32_t status;      /* pppm_status of the request */
+    double submit_s;
+    double start_s;
+    double end_s;
+} pppm_request_info;
+pppm_status pppm_server_create(const pppm_server_config *cfg, pppm_server **out);
+pppm_status pppm_server_destroy(pppm_server *srv);
+pppm_status pppm_server_add_scene(pppm_server *srv, const pppm_params *p, uint32_t N, const float *pos4_host,
+                                  const double *ax_host, const double *ay_host, const double *az_host,
+                                  uint64_t *scene_id);
+pppm_status pppm_server_submit(pppm_server *srv, uint64_t scene_id, int kind, uint32_t steps, double dt,
+                               uint64_t *ticket);
+/* Waits for a request; vel_host (3*N doubles, may be NULL) receives an EVAL
+ * result as [3][N].  Each ticket can be waited for once. */
+pppm_status pppm_server_wait(pppm_server *srv, uint64_t ticket, double timeout_s, pppm_request_info *info,
+                             double *vel_host);
+/* Current positions of a scene (after its queued requests have finished). */
+pppm_status pppm_server_read_positions(pppm_server *srv, uint64_t scene_id, float *pos4_host);
+pppm_status pppm_server_stats(pppm_server *srv, uint64_t *resident_bytes, uint64_t *completed);
+
+/* ---- frame files ----------------------------------------------------------
+ * The demo driver's output (HFS/newTest.cpp:23-36): <dir>/Particle_data%04d.bin,
+ * N raw float4 records (x, y, z, 1.0f).  pos4 may be a host or device array
+ * (on_device).  pppm_read_frame with pos4_host = NULL returns the record count. */
+pppm_status pppm_frame_path(const char *dir, int frame, char *out, size_t cap);
+pppm_status pppm_write_frame(const char *dir, int frame, uint32_t N, const float *pos4, int on_device);
+pppm_status pppm_read_frame(const char *path, float *pos4_host, uint32_t cap, uint32_t *N);
+
 /* ---- multigrid surface: gf::MultiGridSolver3DPeriod_double
  * (MG/MultiGrid.h:188-209, MG/MultiGrid.cpp:128-250) ---------------------- */
 typedef struct pppm_mg pppm_mg;

@@ -27,7 +27,11 @@ EXPORTED = (
     "pppm_hasher_tables", "pppm_hasher_reorder", "pppm_hasher_deorder", "pppm_direct_sum_fp64",
     "pppm_scene_set_profiling", "pppm_stage_name", "pppm_get_stage_times", "pppm_kernel_launches",
     "pppm_spatial_hash_noalloc", "pppm_advect_euler", "pppm_advect_rk2", "pppm_batch_run",
+    "pppm_server_create", "pppm_server_destroy", "pppm_server_add_scene", "pppm_server_submit",
+    "pppm_server_wait", "pppm_server_read_positions", "pppm_server_stats",
+    "pppm_frame_path", "pppm_write_frame", "pppm_read_frame",
 )
+REQ_EVAL, REQ_ADVANCE = 0, 1
 NOALLOC_MAX_PARTICLES = 1048576  # PPPM_NOALLOC_MAX_PARTICLES in include/pppm.h
 STAGES = ("domain", "vort_sort", "cells_reorder", "p2m", "multigrid", "farfield", "eval_sort", "eval")
 
@@ -51,6 +55,14 @@ class PppmBatchItem(C.Structure):
                 ("ay_dev", C.c_void_p), ("az_dev", C.c_void_p), ("M", C.c_uint32), ("eval_a4_dev", C.c_void_p),
                 ("eval_b4_dev", C.c_void_p), ("is_segment", C.c_int), ("u_dev", C.c_void_p), ("v_dev", C.c_void_p),
                 ("w_dev", C.c_void_p)]
+
+
+class PppmServerConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("slots", C.c_uint32)]
+
+
+class PppmRequestInfo(C.Structure):
+    _fields_ = [("status", C.c_int32), ("submit_s", C.c_double), ("start_s", C.c_double), ("end_s", C.c_double)]
 
 
 class PppmError(RuntimeError):
@@ -119,6 +131,16 @@ def load(build_if_missing: bool = True):
         "pppm_advect_euler": (st, [vp, u32, vp, vp, vp, vp, C.c_double]),
         "pppm_advect_rk2": (st, [vp, u32, vp, vp, vp, vp, C.c_double]),
         "pppm_batch_run": (st, [C.POINTER(PppmBatchItem), u32, vp]),
+        "pppm_server_create": (st, [C.POINTER(PppmServerConfig), C.POINTER(vp)]),
+        "pppm_server_destroy": (st, [vp]),
+        "pppm_server_add_scene": (st, [vp, C.POINTER(PppmParams), u32, vp, vp, vp, vp, C.POINTER(C.c_uint64)]),
+        "pppm_server_submit": (st, [vp, C.c_uint64, C.c_int, u32, C.c_double, C.POINTER(C.c_uint64)]),
+        "pppm_server_wait": (st, [vp, C.c_uint64, C.c_double, C.POINTER(PppmRequestInfo), vp]),
+        "pppm_server_read_positions": (st, [vp, C.c_uint64, vp]),
+        "pppm_server_stats": (st, [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+        "pppm_frame_path": (st, [C.c_char_p, C.c_int, C.c_char_p, C.c_size_t]),
+        "pppm_write_frame": (st, [C.c_char_p, C.c_int, u32, vp, C.c_int]),
+        "pppm_read_frame": (st, [C.c_char_p, vp, u32, C.POINTER(u32)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -70,6 +70,7 @@ void free_eval_side(pppm_scene *s) {
 }
 
 cudaError_t alloc_hist(pppm_scene *s) {
+    std::lock_guard<std::recursive_mutex> lk(pppm::device_lock());
     const size_t need = pppm::radix_hist_entries(s->capN > s->capM ? s->capN : s->capM);
     if (need <= s->hist_cap) return cudaSuccess;
     cudaFree(s->hist);
@@ -81,6 +82,7 @@ cudaError_t alloc_hist(pppm_scene *s) {
 }
 
 cudaError_t alloc_vortex_side(pppm_scene *s, uint32_t cap) {
+    std::lock_guard<std::recursive_mutex> lk(pppm::device_lock());
     free_vortex_side(s);
     s->capN = cap;
     PPPM_CUDA_TRY(dalloc(&s->vpos, cap));
@@ -100,6 +102,7 @@ cudaError_t alloc_vortex_side(pppm_scene *s, uint32_t cap) {
 }
 
 cudaError_t alloc_eval_side(pppm_scene *s, uint32_t cap) {
+    std::lock_guard<std::recursive_mutex> lk(pppm::device_lock());
     free_eval_side(s);
     s->capM = cap;
     for (int q = 0; q < 2; q++) {
@@ -140,21 +143,28 @@ cudaError_t alloc_grid_side(pppm_scene *s) {
     PPPM_CUDA_TRY(dalloc(&s->sub_end, 8 * (size_t)s->C));
     PPPM_CUDA_TRY(cudaMemset(s->mflag, 0, sizeof(uint32_t) * s->C));
     PPPM_CUDA_TRY(dalloc(&s->dparams, 1));
-    PPPM_CUDA_TRY(cudaMemset(s->dparams, 0, sizeof(pppm::DevParams)));
     PPPM_CUDA_TRY(dalloc(&s->norms, 2));
     PPPM_CUDA_TRY(dalloc(&s->pair_count, 1));
     if (s->levels >= 2) {
         const int dc = (int)s->lv[s->levels - 1].d;
         const size_t cc = (size_t)dc * dc * dc;
         PPPM_CUDA_TRY(dalloc(&s->coarse_op, cc * cc));
-        PPPM_CUDA_TRY(pppm::build_coarse_operator(dc, s->coarse_op, nullptr));
-        PPPM_CUDA_TRY(cudaDeviceSynchronize());
     }
-    return cudaSuccess;
+    // initialise on a private stream (no device-wide synchronisation)
+    cudaStream_t st = nullptr;
+    PPPM_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    cudaError_t e = cudaMemsetAsync(s->mflag, 0, sizeof(uint32_t) * s->C, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->dparams, 0, sizeof(pppm::DevParams), st);
+    if (e == cudaSuccess && s->coarse_op)
+        e = pppm::build_coarse_operator((int)s->lv[s->levels - 1].d, s->coarse_op, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    return e;
 }
 
 void destroy_scene(pppm_scene *s) {
     if (!s) return;
+    std::lock_guard<std::recursive_mutex> lk(pppm::device_lock());
     for (int i = 0; i < 16; i++) {
         if (s->ev_begin[i]) cudaEventDestroy(s->ev_begin[i]);
         if (s->ev_end[i]) cudaEventDestroy(s->ev_end[i]);
@@ -239,6 +249,7 @@ extern "C" pppm_status pppm_scene_create(const pppm_params *p, uint32_t cap_vort
         snprintf(g_err, sizeof(g_err), "pppm_scene_create: %s", why);
         return PPPM_ERR_INVALID;
     }
+    std::lock_guard<std::recursive_mutex> lk(pppm::device_lock());
     pppm_scene *s = new pppm_scene();
     s->prm = *p;
     s->n = p->n;
@@ -247,6 +258,7 @@ extern "C" pppm_status pppm_scene_create(const pppm_params *p, uint32_t cap_vort
     cudaError_t e = alloc_grid_side(s);
     if (e == cudaSuccess) e = alloc_vortex_side(s, cap_vort ? cap_vort : 1);
     if (e == cudaSuccess) e = alloc_eval_side(s, cap_eval ? cap_eval : 1);
+    if (e == cudaSuccess) e = pppm::prepare_multigrid_graph(s);
     if (e != cudaSuccess) {
         pppm_status st = cuda_fail("pppm_scene_create", e);
         destroy_scene(s);
@@ -341,6 +353,7 @@ extern "C" pppm_status pppm_eval_f32(pppm_scene *s, uint32_t M, const float *ea,
 
 extern "C" pppm_status pppm_count_pairs(pppm_scene *s, uint32_t M, const float *ea, uint64_t *pairs) {
     if (!s || !pairs) return PPPM_ERR_INVALID;
+    std::lock_guard<std::recursive_mutex> lk(pppm::device_lock());
     float *tmp = nullptr;
     cudaError_t e = cudaMalloc(&tmp, sizeof(float) * 3 * (size_t)(M ? M : 1));
     if (e != cudaSuccess) return cuda_fail("pppm_count_pairs", e);
@@ -503,6 +516,7 @@ extern "C" pppm_status pppm_get_sorted_vortices(pppm_scene *s, float *pos4, doub
         snprintf(g_err, sizeof(g_err), "pppm_get_sorted_vortices: no far field built");
         return PPPM_ERR_STATE;
     }
+    std::lock_guard<std::recursive_mutex> lk(pppm::device_lock());
     double *tmp = nullptr;
     cudaError_t e = cudaSuccess;
     if (!s->ref_valid) {
@@ -535,6 +549,11 @@ extern "C" pppm_status pppm_get_grid(pppm_scene *s, int which, const void **ptr)
 }
 
 namespace pppm {
+
+std::recursive_mutex &device_lock() {
+    static std::recursive_mutex m;
+    return m;
+}
 
 static std::atomic<unsigned long long> g_launches{0};
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
@@ -624,6 +643,7 @@ extern "C" pppm_status pppm_mg_create(uint32_t n, void *stream, pppm_mg **out) {
         snprintf(g_err, sizeof(g_err), "pppm_mg_create: unsupported grid edge %u", n);
         return PPPM_ERR_INVALID;
     }
+    std::lock_guard<std::recursive_mutex> lk(pppm::device_lock());
     pppm_mg *m = new pppm_mg();
     m->n = n;
     pppm::MGPlan &P = m->plan;
@@ -659,6 +679,7 @@ extern "C" pppm_status pppm_mg_create(uint32_t n, void *stream, pppm_mg **out) {
 extern "C" pppm_status pppm_mg_destroy(pppm_mg *m) {
     if (!m) return PPPM_OK;
     if (m->plan.st) cudaStreamSynchronize(m->plan.st);
+    std::lock_guard<std::recursive_mutex> lk(pppm::device_lock());
     cudaFree(m->pool);
     cudaFree(m->plan.norms);
     delete m;

@@ -495,6 +495,7 @@ extern "C" pppm_status pppm_hasher_create(uint32_t cap, uint32_t n, void *stream
         pppm_set_error("pppm_hasher_create: invalid argument");
         return PPPM_ERR_INVALID;
     }
+    std::lock_guard<std::recursive_mutex> lk(pppm::device_lock());
     pppm_hasher *h = new pppm_hasher();
     h->stream = (cudaStream_t)stream;
     h->cap = cap;
@@ -519,6 +520,7 @@ extern "C" pppm_status pppm_hasher_create(uint32_t cap, uint32_t n, void *stream
 
 extern "C" pppm_status pppm_hasher_destroy(pppm_hasher *h) {
     if (!h) return PPPM_OK;
+    std::lock_guard<std::recursive_mutex> lk(pppm::device_lock());
     for (int q = 0; q < 2; q++) {
         cudaFree(h->key[q]);
         cudaFree(h->idx[q]);

@@ -409,6 +409,29 @@ cudaError_t mg_capture_graph(const MGPlan &m_in, cudaGraphExec_t *exec, unsigned
     return e;
 }
 
+static MGPlan scene_plan(pppm_scene *s) {
+    MGPlan m;
+    m.levels = s->levels;
+    for (int l = 0; l < s->levels; l++) m.lv[l] = s->lv[l];
+    m.comps = 3;
+    m.st = s->stream;
+    m.psi = s->psi;
+    m.b64 = nullptr;
+    m.vort = s->vort;
+    m.P = s->dparams;
+    m.norms = s->norms;
+    m.coarse_op = s->coarse_op;
+    return m;
+}
+
+// Captures the scene's reference-schedule graph (called at scene creation,
+// under the device lock).
+cudaError_t prepare_multigrid_graph(pppm_scene *s) {
+    if (s->prm.mg_mode != PPPM_MG_REFERENCE || s->mg_graph) return cudaSuccess;
+    std::lock_guard<std::recursive_mutex> lk(device_lock());
+    return mg_capture_graph(scene_plan(s), &s->mg_graph, &s->mg_graph_kernels);
+}
+
 cudaError_t run_multigrid(pppm_scene *s) {
     MGPlan m;
     m.levels = s->levels;
@@ -424,7 +447,7 @@ cudaError_t run_multigrid(pppm_scene *s) {
     int cyc = 0;
     double rel = -1.0;
     if (s->prm.mg_mode == PPPM_MG_REFERENCE) {
-        if (!s->mg_graph) PPPM_CUDA_TRY(mg_capture_graph(m, &s->mg_graph, &s->mg_graph_kernels));
+        if (!s->mg_graph) PPPM_CUDA_TRY(prepare_multigrid_graph(s));
         PPPM_CUDA_TRY(cudaGraphLaunch(s->mg_graph, s->stream));
         for (unsigned q = 0; q < s->mg_graph_kernels; q++) note_launch();
         s->mg_cycles_last = 1;

@@ -15,6 +15,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #include "../../include/pppm.h"
 
 namespace pppm {
@@ -161,6 +163,13 @@ enum Stage {
     kNumStages = 8
 };
 const char *stage_name(int i);
+
+// Library-wide lock held around CUDA graph capture and around every call that
+// can synchronise the whole device (cudaMalloc, cudaFree, scene creation and
+// destruction), so that no capture in one thread is ever invalidated by an
+// implicit device synchronisation in another thread.
+std::recursive_mutex &device_lock();
+cudaError_t prepare_multigrid_graph(pppm_scene *s);
 
 // Process-wide count of kernel launches issued by this library.
 void note_launch();
