@@ -69,25 +69,27 @@ struct PairAcc {
 
 // phi(t) = (1 - e^-t) / t, scaled by 1/(4 pi a^3).  Below t = 0.25 the
 // degree-5 Taylor series (relative truncation < t^6/7! < 5e-8) needs no
-// special function; above it, (1 - exp(-t)) / t.  The exp branch is taken
-// only when some lane of the warp needs it (UNIFORM: the whole warp executes
-// this call together; otherwise each lane branches on its own t).
+// special function; its coefficients arrive pre-scaled by 1/(4 pi a^3) in
+// cf[0..5] (cf[k] = (-1)^k / (k+1)! / (4 pi a^3)).  Above t = 0.25,
+// (1 - exp(-t)) / t.  The exp branch runs only when the scene can reach it
+// and some lane of the warp needs it (UNIFORM: the whole warp executes this
+// call together; otherwise each lane branches on its own t).
 template <bool UNIFORM>
-__device__ __forceinline__ float smooth_coeff(float t, float inv4pia3, bool need_exp) {
-    float p = -1.0f / 720.0f;
-    p = fmaf(p, t, 1.0f / 120.0f);
-    p = fmaf(p, t, -1.0f / 24.0f);
-    p = fmaf(p, t, 1.0f / 6.0f);
-    p = fmaf(p, t, -0.5f);
-    p = fmaf(p, t, 1.0f);
-    if (need_exp) {  // uniform: no pair of the scene reaches t = 0.25 otherwise
+__device__ __forceinline__ float smooth_coeff(float t, const float *cf, float inv4pia3, bool need_exp) {
+    float p = cf[5];
+    p = fmaf(p, t, cf[4]);
+    p = fmaf(p, t, cf[3]);
+    p = fmaf(p, t, cf[2]);
+    p = fmaf(p, t, cf[1]);
+    p = fmaf(p, t, cf[0]);
+    if (need_exp) {
         const bool big = t >= 0.25f;
         if (UNIFORM ? __any_sync(0xffffffffu, big) : big) {
-            const float e = __fdividef(1.0f - __expf(-t), fmaxf(t, 0.25f));
+            const float e = __fdividef(1.0f - __expf(-t), fmaxf(t, 0.25f)) * inv4pia3;
             p = big ? e : p;
         }
     }
-    return p * inv4pia3;
+    return p;
 }
 
 // One candidate pair, branch free: the box test, the lane's cell range and
@@ -95,8 +97,8 @@ __device__ __forceinline__ float smooth_coeff(float t, float inv4pia3, bool need
 // segment's other end; COUNT: count the pairs inside the box.
 template <bool SEG, bool COUNT, bool UNIFORM>
 __device__ __forceinline__ void pair_term(const float4 r, const float4 al, bool lane_ok, const float3 ra,
-                                          const float3 rb, float cr, float inv_a3, float inv4pia3, bool need_exp,
-                                          PairAcc &acc) {
+                                          const float3 rb, float cr, float inv_a3, const float *cf, float inv4pia3,
+                                          bool need_exp, PairAcc &acc) {
     const float dx = ra.x - r.x, dy = ra.y - r.y, dz = ra.z - r.z;
     const float m = fmaxf(fabsf(dx), fmaxf(fabsf(dy), fabsf(dz)));
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
@@ -108,7 +110,7 @@ __device__ __forceinline__ void pair_term(const float4 r, const float4 al, bool 
         ok = ok && !(fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < 1e-24f);
     }
     const float rr = r2 * rsqrtf(fmaxf(r2, 1e-30f));
-    const float c = smooth_coeff<UNIFORM>(r2 * rr * inv_a3, inv4pia3, need_exp);
+    const float c = smooth_coeff<UNIFORM>(r2 * rr * inv_a3, cf, inv4pia3, need_exp);
     const float coeff = ok ? c : 0.0f;
     acc.x = fmaf(al.y * dz - al.z * dy, coeff, acc.x);
     acc.y = fmaf(al.z * dx - al.x * dz, coeff, acc.y);
@@ -119,9 +121,10 @@ __device__ __forceinline__ void pair_term(const float4 r, const float4 al, bool 
 template <bool SEG, bool COUNT>
 __device__ __forceinline__ void cell_pairs(const float4 *__restrict__ vrec, const float4 *__restrict__ valf,
                                            uint32_t ps, uint32_t pe, bool lane_ok, const float3 ra, const float3 rb,
-                                           float cr, float inv_a3, float inv4pia3, bool need_exp, PairAcc &acc) {
+                                           float cr, float inv_a3, const float *cf, float inv4pia3, bool need_exp,
+                                           PairAcc &acc) {
     for (uint32_t p = ps; p < pe; p++)
-        pair_term<SEG, COUNT, false>(vrec[p], valf[p], lane_ok, ra, rb, cr, inv_a3, inv4pia3, need_exp, acc);
+        pair_term<SEG, COUNT, false>(vrec[p], valf[p], lane_ok, ra, rb, cr, inv_a3, cf, inv4pia3, need_exp, acc);
 }
 
 // Warp-uniform version: the warp copies the cell's records into its shared
@@ -130,9 +133,9 @@ __device__ __forceinline__ void cell_pairs(const float4 *__restrict__ vrec, cons
 template <bool SEG, bool COUNT>
 __device__ __forceinline__ void cell_pairs_staged(const float4 *__restrict__ vrec, const float4 *__restrict__ valf,
                                                   uint32_t ps, uint32_t pe, bool lane_ok, const float3 ra,
-                                                  const float3 rb, float cr, float inv_a3, float inv4pia3,
-                                                  bool need_exp, float4 *__restrict__ sv, float4 *__restrict__ sa,
-                                                  int lane, PairAcc &acc) {
+                                                  const float3 rb, float cr, float inv_a3, const float *cf,
+                                                  float inv4pia3, bool need_exp, float4 *__restrict__ sv,
+                                                  float4 *__restrict__ sa, int lane, PairAcc &acc) {
     for (uint32_t base = ps; base < pe; base += 32) {
         const uint32_t cnt = min(32u, pe - base);
         if ((uint32_t)lane < cnt) {
@@ -142,7 +145,7 @@ __device__ __forceinline__ void cell_pairs_staged(const float4 *__restrict__ vre
         __syncwarp();
 #pragma unroll 2
         for (uint32_t q = 0; q < cnt; q++)
-            pair_term<SEG, COUNT, true>(sv[q], sa[q], lane_ok, ra, rb, cr, inv_a3, inv4pia3, need_exp, acc);
+            pair_term<SEG, COUNT, true>(sv[q], sa[q], lane_ok, ra, rb, cr, inv_a3, cf, inv4pia3, need_exp, acc);
         __syncwarp();
     }
 }
@@ -151,8 +154,14 @@ constexpr int kUniformMaxSub = 1000;  // warp-uniform walk up to 10^3 half-cells
 
 // SEG: is_segment == 1 with a distinct other-end array (with eval_b == eval_a
 // the other-end test is the r = 0 test itself, so SEG is off).
+// Series coefficients of the smoothing kernel, known on the host from a alone;
+// passed by value so they sit in the constant bank.
+struct SmoothSeries {
+    float c[6];
+};
+
 template <bool SEG, bool COUNT>
-__global__ void eval_kernel(const uint32_t *__restrict__ eidx, uint32_t M, const float4 *__restrict__ eval_a,
+__global__ void eval_kernel(const SmoothSeries sc, const uint32_t *__restrict__ eidx, uint32_t M, const float4 *__restrict__ eval_a,
             const float4 *__restrict__ eval_b, const float *__restrict__ far,
             const uint32_t *__restrict__ start, const uint32_t *__restrict__ end,
             const uint32_t *__restrict__ sub_start, const uint32_t *__restrict__ sub_end, const float4 *__restrict__ vrec,
@@ -196,6 +205,7 @@ __global__ void eval_kernel(const uint32_t *__restrict__ eidx, uint32_t M, const
     if (K >= 0) {
         const float cr = P->cr_f, inv_a3 = P->inv_a3_f, inv4pia3 = P->inv4pia3_f;
         const bool need_exp = P->need_exp != 0;
+        const float *cf = sc.c;
         // The reference walks hash cells [i-K-1, i+K+1]^3.  Only the half-cells
         // (cell, octant runs of the vortex order) that can hold a vortex inside
         // the point's box are visited: the box spans K+0.5 cells either side,
@@ -245,7 +255,7 @@ __global__ void eval_kernel(const uint32_t *__restrict__ eidx, uint32_t M, const
                         if (ps == kEmpty) continue;
                         const bool lane_ok = act && ci >= rlo[0] && ci <= rhi[0] && cj >= rlo[1] && cj <= rhi[1] &&
                                              ck >= rlo[2] && ck <= rhi[2];
-                        cell_pairs_staged<SEG, COUNT>(vrec, valf, ps, pe, lane_ok, ra, rb, cr, inv_a3, inv4pia3,
+                        cell_pairs_staged<SEG, COUNT>(vrec, valf, ps, pe, lane_ok, ra, rb, cr, inv_a3, cf, inv4pia3,
                                                       need_exp, sv, sa, lane, acc);
                     }
         } else if (act && lo[0] <= hi[0]) {
@@ -256,7 +266,7 @@ __global__ void eval_kernel(const uint32_t *__restrict__ eidx, uint32_t M, const
                         const uint32_t cell = ((uint32_t)kk * n + (uint32_t)jj) * n + (uint32_t)ii;
                         const uint32_t ps = start[cell];
                         if (ps == kEmpty) continue;
-                        cell_pairs<SEG, COUNT>(vrec, valf, ps, end[cell], true, ra, rb, cr, inv_a3, inv4pia3, need_exp, acc);
+                        cell_pairs<SEG, COUNT>(vrec, valf, ps, end[cell], true, ra, rb, cr, inv_a3, cf, inv4pia3, need_exp, acc);
                     }
         }
     }
@@ -303,7 +313,14 @@ cudaError_t launch_eval(pppm_scene *s, const float4 *eval_a, const float4 *eval_
     const bool seg = (is_segment == 1) && (eval_b != eval_a);
     const unsigned grid = (M + kEvalThreads - 1) / kEvalThreads;
     unsigned long long *pc = count_pairs ? s->pair_count : nullptr;
-#define PPPM_EVAL_ARGS sidx, M, eval_a, eval_b, s->far, s->cell_start, s->cell_end, s->sub_start, s->sub_end, \
+    SmoothSeries sc;
+    {
+        const double a = s->prm.a;
+        const double k = 1.0 / (kFourPi * a * a * a);
+        const double f[6] = {1.0, -1.0 / 2, 1.0 / 6, -1.0 / 24, 1.0 / 120, -1.0 / 720};
+        for (int q = 0; q < 6; q++) sc.c[q] = (float)(k * f[q]);
+    }
+#define PPPM_EVAL_ARGS sc, sidx, M, eval_a, eval_b, s->far, s->cell_start, s->cell_end, s->sub_start, s->sub_end, \
                        s->vrec, s->valf, s->dparams, \
                        (int)s->n, s->prm.K, u, v, w, uf, pc
     if (seg) {
