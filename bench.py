@@ -300,6 +300,32 @@ def run_b200(args, world, rank, local):
     rk2_ms = statistics.median(rk_ms)
     del rk_pos
 
+    # one vortex-segment time step (the reference's solveTimeStep without
+    # boundary or heat): 2N end evaluations, segment update, rehash, smoothing
+    vs_pos, vs_al = dpos.clone(), dal.clone()
+    scene.vortex_step(vs_pos, vs_al, 1e-3)
+    torch.cuda.synchronize()
+    vs_ms, vs_stage = [], {}
+    scene.set_profiling(True)
+    for _ in range(3):
+        vs_pos.copy_(dpos)
+        vs_al.copy_(dal)
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        scene.vortex_step(vs_pos, vs_al, 1e-3)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        vs_ms.append(e0.elapsed_time(e1))
+        for k, v in scene.stage_times().items():
+            if v >= 0:
+                vs_stage.setdefault(k, []).append(v)
+    scene.set_profiling(False)
+    vortex_step_ms = statistics.median(vs_ms)
+    vortex_step_stages = {k: statistics.median(v) for k, v in vs_stage.items()}
+    del vs_pos, vs_al
+
     # accuracy on a fixed 1% subsample (every 100th particle) vs the FP64 direct sum
     sub = dpos[::100].contiguous()
     u_gpu = out.t()[::100].cpu().numpy()
@@ -349,6 +375,8 @@ def run_b200(args, world, rank, local):
             "stages_ms": stages,
             "err_vs_direct_fp64": err,
             "rk2_step_ms": rk2_ms,
+            "vortex_step_ms": vortex_step_ms,
+            "vortex_step_stages_ms": vortex_step_stages,
             "near_field_pairs": pairs,
         }
         print(json.dumps(line), flush=True)

@@ -142,6 +142,52 @@ pppm_status pppm_advect_euler(pppm_scene *s, uint32_t N, float *pos4_dev, const 
 pppm_status pppm_advect_rk2(pppm_scene *s, uint32_t N, float *pos4_dev, const double *ax_dev,
                             const double *ay_dev, const double *az_dev, double dt);
 
+/* One vortex-segment time step, VortexSimulationSystem::solveTimeStep
+ * (HFS/VortexSimulationSystemImp.cpp:90-125) for a system without solid
+ * boundary or shedding (call pppm_baroclinic first for the buoyancy source):
+ *   convertVortToSeg  (:127-140, ComputePosb HFS/GPU_kernel.cu:3184-3229):
+ *       s = alpha capped to length h_seg, endb = c + s/2, enda = c - s/2,
+ *       kappa = max(|alpha| / h_seg, 1)
+ *   computeURotation  (:142-228): far field of the blobs, velocity at endb and
+ *       at enda, each a segment against the centre; with P > 0 also at the
+ *       passive points passive4 (tracers, heat particles; evaluateBiotSavart
+ *       :1195-1244), which receive their velocity in pu/pv/pw and move by it
+ *       (p <- float(p + u dt), w = 0)
+ *   applyFlow         (:277-314): both ends move (p <- float(p + u dt)), the
+ *       centre becomes their midpoint
+ *   convertSegToVort  (:315-331): dalpha = kappa (endb - enda) - alpha
+ *   computeStretching (:466-525): alpha + dalpha is hashed at the new centres
+ *       and smoothed with exp(-d^2 / (2 nu^2)) over the 5^3 hash cells around
+ *       each centre (ParticleGaussianSmooth, HFS/GPU_kernel.cu:3327-3438).
+ * cent4 (centres, w kept) and ax/ay/az (strengths) are updated in place on the
+ * device.  enda4 / endb4 (N float4 each, may be NULL) receive the moved ends.
+ * The reference passes h_seg = d_h (0.1 in its setups) and nu = 0.1.  Afterwards
+ * the scene holds the hash of the new centres (cell tables, sorted index) but
+ * no far field: call pppm_set_vortices before pppm_build_far_field. */
+pppm_status pppm_vortex_step(pppm_scene *s, uint32_t N, float *cent4_dev, double *ax_dev, double *ay_dev,
+                             double *az_dev, double dt, double h_seg, double nu, float *enda4_dev,
+                             float *endb4_dev, uint32_t P, float *passive4_dev, double *pu_dev,
+                             double *pv_dev, double *pw_dev);
+
+/* Buoyancy source, VortexSimulationSystem::addBaroclinicForce
+ * (HFS/VortexSimulationSystemImp.cpp:369-465): H heat particles (positions,
+ * heat value per particle, cpu_heat_life in the reference) are deposited on a
+ * density grid of edge min(floor(L / 0.2) + 1, 200) over 1.2 x their bounding
+ * box (setDensityDomain :336-366; AssignDensity HFS/GPU_kernel.cu:3655-3740),
+ * differentiated (GradDensity :3742-3797, periodic), and the gradient
+ * interpolated at each of the N vortices adds 5 dt * 0.1 * (grad rho x (0,10,0))
+ * to its strength (ParticleGetBaroclinic :3800-3898).  The reference applies
+ * nothing for N > 262,144 (its launch has block and grid swapped); here every
+ * vortex gets the force.  One stream synchronisation (the grid size depends on
+ * the bounding box).  H == 0 or a zero-size box: no change. */
+pppm_status pppm_baroclinic(pppm_scene *s, uint32_t H, const float *heat4_dev, const float *heat_dev,
+                            uint32_t N, const float *cent4_dev, double *ax_dev, double *ay_dev,
+                            double *az_dev, double dt);
+/* The last density grid pppm_baroclinic built: edge, origin, cell size, and
+ * device pointers to rho [dim^3] and grad rho [3][dim^3] (float, x-fastest). */
+pppm_status pppm_get_density(pppm_scene *s, uint32_t *dim, double origin[3], double *h,
+                             const float **rho_dev, const float **grad_dev);
+
 /* Accessors matching BiotSavartSolver::getOrigin / getCellh
  * (HFS/BiotSavartSolver.h:34-35); synchronises the stream. */
 pppm_status pppm_get_domain(pppm_scene *s, double origin[3], double *length, double *cell_h);
@@ -241,6 +287,41 @@ pppm_status pppm_server_stats(pppm_server *srv, uint64_t *resident_bytes, uint64
 pppm_status pppm_frame_path(const char *dir, int frame, char *out, size_t cap);
 pppm_status pppm_write_frame(const char *dir, int frame, uint32_t N, const float *pos4, int on_device);
 pppm_status pppm_read_frame(const char *path, float *pos4_host, uint32_t cap, uint32_t *N);
+
+/* SGI image file as Particle_renderer/.../write_sgi.cpp:6-67 writes it
+ * (host pixels, i-fastest, `channels` 1 or 3 interleaved per pixel; 8-bit, or
+ * 16-bit with high_precision). */
+pppm_status pppm_write_sgi(const char *path, uint32_t ni, uint32_t nj, int channels, const float *pix_host,
+                           int high_precision);
+
+/* --- headless splatting renderer (Particle_renderer/particle_renderer/
+ * particle_renderer/shadow.cpp, render.cpp) ------------------------------
+ * Positions are float4 records (w ignored); per-particle density / opacity
+ * factors and colours are float arrays on the device.  Work runs on the
+ * renderer's stream; each call reads sizes back to the host once or twice. */
+typedef struct pppm_renderer pppm_renderer;
+pppm_status pppm_renderer_create(void *stream, pppm_renderer **out);
+pppm_status pppm_renderer_destroy(pppm_renderer *r);
+/* compute_shadows (shadow.cpp:56-145): the particles, nearest to the light
+ * first, darken a perspective shadow map seen from the light by
+ * exp(-opacity * dens * (1 - d^2/r^2)^2) per pixel; illum_dev[i] receives the map
+ * at particle i's pixel before its own disc.  Map edge = int(quality * R /
+ * radius) for the bounding-sphere radius R.  PPPM_ERR_DOMAIN when the light is
+ * inside 1.25 R (the reference returns false there). */
+pppm_status pppm_render_shadows(pppm_renderer *r, uint32_t n, const float *pos4_dev, const float *dens_dev,
+                                float radius, float opacity, const float light[3], float quality,
+                                float *illum_dev, uint32_t *npix);
+/* The last shadow map (npix x npix floats, i-fastest, device). */
+pppm_status pppm_render_shadow_map(pppm_renderer *r, const float **map_dev, uint32_t *npix);
+/* render_smoke (render.cpp:61-125): back-to-front over-compositing of
+ * (1 - illum) base_rgb + illum lit_rgb discs into a width x height RGB image
+ * (image_dev[3 * (i + width * j) + c]) that starts as the background; camera
+ * at `camera` looking at `target`, perspective factor `perspective`. */
+pppm_status pppm_render_smoke(pppm_renderer *r, uint32_t n, const float *pos4_dev, const float *illum_dev,
+                              const float *base_rgb_dev, const float *lit_rgb_dev, float radius, float opacity,
+                              const float *den_dev, const float background[3], const float camera[3],
+                              const float target[3], float perspective, uint32_t width, uint32_t height,
+                              float *image_dev);
 
 /* ---- multigrid surface: gf::MultiGridSolver3DPeriod_double
  * (MG/MultiGrid.h:188-209, MG/MultiGrid.cpp:128-250) ---------------------- */

@@ -733,6 +733,171 @@ extern "C" int orc_pppm(const orc_params *prm, uint32_t N, const float *vort_pos
     return 0;
 }
 
+/* BiotSavartSolver::sortVort (HFS/BiotSavartSolverImp.cpp:733-755) on the
+ * centres, then ParticleGaussianSmooth (HFS/GPU_kernel.cu:3327-3438): for each
+ * centre t, with (i, j, k) = floor(float(x_t - origin) / h), the weighted mean
+ * of the strengths d over all vortices hashed into the 5^3 cells around
+ * (i, j, k) inside the grid, weights exp(-|x_p - x_t|^2 / (2 nu^2)); a weight
+ * sum below 1e-12 is replaced by 1e24. */
+extern "C" void orc_gaussian_smooth(const orc_params *prm, uint32_t N, const float *cent4_in, const double *dx_,
+                                    const double *dy_, const double *dz_, double nu, double *ox, double *oy,
+                                    double *oz) {
+    const F4 *cent = reinterpret_cast<const F4 *>(cent4_in);
+    const float *cent4 = cent4_in;
+    double origin[3], L;
+    if (prm->domain_mode == 1) {
+        origin[0] = prm->fixed_origin[0]; origin[1] = prm->fixed_origin[1];
+        origin[2] = prm->fixed_origin[2]; L = prm->fixed_length;
+    } else {
+        orc_set_domain(cent4, N, origin, &L);
+    }
+    const uint32_t n = prm->n;
+    const size_t C = (size_t)n * n * n;
+    const float h_f = (float)(L / (double)n);
+    const float of[3] = {(float)origin[0], (float)origin[1], (float)origin[2]};
+    const double invh = 1.0 / (double)h_f;
+    std::vector<uint32_t> key(N), idx(N), start(C), end(C);
+    orc_calc_hash(cent4, N, n, h_f, of, key.data(), idx.data());
+    orc_sort_by_key(key.data(), idx.data(), N);
+    orc_find_cell_start(key.data(), N, (uint32_t)C, start.data(), end.data());
+    const int d = (int)n;
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t t = 0; t < (int64_t)N; t++) {
+        const float ax = (float)((double)cent[t].x - origin[0]);
+        const float ay = (float)((double)cent[t].y - origin[1]);
+        const float az = (float)((double)cent[t].z - origin[2]);
+        // a cell more than two outside the grid sees no in-grid cell; clamping
+        // keeps the int conversion defined for centres far outside a fixed domain
+        auto cell = [&](float r) {
+            const double q = std::floor((double)r * invh);
+            return !(q >= -3.0) ? -3 : (q > (double)(d + 2) ? d + 2 : (int)q);
+        };
+        const int i = cell(ax), j = cell(ay), k = cell(az);
+        double wx = 0, wy = 0, wz = 0, tw = 0;
+        for (int kk = k - 2; kk <= k + 2; kk++)
+            for (int jj = j - 2; jj <= j + 2; jj++)
+                for (int ii = i - 2; ii <= i + 2; ii++) {
+                    if (!(kk >= 0 && kk < d && jj >= 0 && jj < d && ii >= 0 && ii < d)) continue;
+                    const size_t c = gidx(ii, jj, kk, d);
+                    if (start[c] == 0xFFFFFFFFu) continue;
+                    for (uint32_t p = start[c]; p < end[c]; p++) {
+                        const uint32_t q = idx[p];
+                        const float bx = (float)((double)cent[q].x - origin[0]);
+                        const float by = (float)((double)cent[q].y - origin[1]);
+                        const float bz = (float)((double)cent[q].z - origin[2]);
+                        const double dx = (double)(float)(bx - ax), dy = (double)(float)(by - ay),
+                                     dz = (double)(float)(bz - az);
+                        const double dsq = dx * dx + dy * dy + dz * dz;
+                        const double w = std::exp(-dsq / (2 * nu * nu));
+                        tw += w;
+                        wx += w * dx_[q];
+                        wy += w * dy_[q];
+                        wz += w * dz_[q];
+                    }
+                }
+        if (tw < 1e-12) tw = 1e+24;
+        ox[t] = wx / tw;
+        oy[t] = wy / tw;
+        oz[t] = wz / tw;
+    }
+}
+
+/* HFS/VortexSimulationSystemImp.cpp:90-125 and 127-143, 277-336, 466-525;
+ * HFS/GPU_kernel.cu:3118-3254 (move, ComputeVortex, ComputePosb, ComputePosa),
+ * 3327-3438 (ParticleGaussianSmooth), 3440-3459 (VectorAdd). */
+extern "C" int orc_vortex_step(const orc_params *prm, uint32_t N, float *cent4, double *vx, double *vy,
+                               double *vz, double dt, double h_seg, double nu, float *enda4_out,
+                               float *endb4_out, uint32_t P, float *passive4, double *pu, double *pv,
+                               double *pw) {
+    if (!prm || N == 0) return 1;
+    F4 *cent = reinterpret_cast<F4 *>(cent4);
+    std::vector<F4> enda(N), endb(N);
+    std::vector<double> kappa(N);
+    // convertVortToSeg: ComputePosb(posa = cent, posc = enda, posb = endb)
+    for (uint32_t i = 0; i < N; i++) {
+        const double sx = vx[i], sy = vy[i], sz = vz[i];
+        const double l = std::sqrt(sx * sx + sy * sy + sz * sz);
+        enda[i] = cent[i];
+        endb[i] = cent[i];
+        if (l < h_seg) {
+            kappa[i] = 1;
+            endb[i].x = (float)(cent[i].x + 0.5 * sx);
+            endb[i].y = (float)(cent[i].y + 0.5 * sy);
+            endb[i].z = (float)(cent[i].z + 0.5 * sz);
+            enda[i].x = (float)(cent[i].x - 0.5 * sx);
+            enda[i].y = (float)(cent[i].y - 0.5 * sy);
+            enda[i].z = (float)(cent[i].z - 0.5 * sz);
+        } else {
+            kappa[i] = l / h_seg;
+            endb[i].x = (float)(cent[i].x + 0.5 * sx / l * h_seg);
+            endb[i].y = (float)(cent[i].y + 0.5 * sy / l * h_seg);
+            endb[i].z = (float)(cent[i].z + 0.5 * sz / l * h_seg);
+            enda[i].x = (float)(cent[i].x - 0.5 * sx / l * h_seg);
+            enda[i].y = (float)(cent[i].y - 0.5 * sy / l * h_seg);
+            enda[i].z = (float)(cent[i].z - 0.5 * sz / l * h_seg);
+        }
+    }
+    // computeURotation: velocities at both ends, segment mode against the centre
+    std::vector<double> ub(3 * (size_t)N), ua(3 * (size_t)N);
+    orc_pppm(prm, N, cent4, vx, vy, vz, N, reinterpret_cast<const float *>(endb.data()), cent4, 1, ub.data(),
+             ub.data() + N, ub.data() + 2 * (size_t)N, nullptr);
+    orc_pppm(prm, N, cent4, vx, vy, vz, N, reinterpret_cast<const float *>(enda.data()), cent4, 1, ua.data(),
+             ua.data() + N, ua.data() + 2 * (size_t)N, nullptr);
+    // computeURotation, tracers and heat (evaluateBiotSavart, VSSImp.cpp:1195-1244):
+    // plain evaluation (is_segment 0) with the same far field, then move_particle
+    if (P > 0) {
+        orc_pppm(prm, N, cent4, vx, vy, vz, P, passive4, passive4, 0, pu, pv, pw, nullptr);
+        F4 *q = reinterpret_cast<F4 *>(passive4);
+        for (uint32_t i = 0; i < P; i++) {
+            const double x = (double)q[i].x + pu[i] * dt;
+            const double y = (double)q[i].y + pv[i] * dt;
+            const double z = (double)q[i].z + pw[i] * dt;
+            q[i].x = (float)x; q[i].y = (float)y; q[i].z = (float)z; q[i].w = 0.f;
+        }
+    }
+    // applyFlow: move_particle on both ends (w = 0), then ComputePosa
+    auto move = [&](std::vector<F4> &p, const std::vector<double> &u) {
+        for (uint32_t i = 0; i < N; i++) {
+            const double x = (double)p[i].x + u[i] * dt;
+            const double y = (double)p[i].y + u[N + i] * dt;
+            const double z = (double)p[i].z + u[2 * (size_t)N + i] * dt;
+            p[i].x = (float)x; p[i].y = (float)y; p[i].z = (float)z; p[i].w = 0.f;
+        }
+    };
+    move(enda, ua);
+    move(endb, ub);
+    for (uint32_t i = 0; i < N; i++) {
+        cent[i].x = (float)(0.5 * (double)(endb[i].x + enda[i].x));
+        cent[i].y = (float)(0.5 * (double)(endb[i].y + enda[i].y));
+        cent[i].z = (float)(0.5 * (double)(endb[i].z + enda[i].z));
+    }
+    // convertSegToVort: dvort = kappa * (endb - enda) - vort; computeStretching:
+    // dvort = 1 * vort + 1 * dvort
+    std::vector<double> dv(3 * (size_t)N);
+    for (uint32_t i = 0; i < N; i++) {
+        const double s[3] = {(double)(float)(endb[i].x - enda[i].x), (double)(float)(endb[i].y - enda[i].y),
+                             (double)(float)(endb[i].z - enda[i].z)};
+        const double v[3] = {vx[i], vy[i], vz[i]};
+        for (int c = 0; c < 3; c++) {
+            const double d = kappa[i] * s[c] - v[c];
+            dv[c * (size_t)N + i] = 1 * v[c] + 1 * d;
+        }
+    }
+    // computeStretching: hash of the new centres + ParticleGaussianSmooth
+    std::vector<double> out(3 * (size_t)N);
+    orc_gaussian_smooth(prm, N, cent4, dv.data(), dv.data() + N, dv.data() + 2 * (size_t)N, nu, out.data(),
+                        out.data() + N, out.data() + 2 * (size_t)N);
+    // vort = 0 * vort + 1 * dvort
+    for (uint32_t i = 0; i < N; i++) {
+        vx[i] = 0 * vx[i] + 1 * out[i];
+        vy[i] = 0 * vy[i] + 1 * out[N + i];
+        vz[i] = 0 * vz[i] + 1 * out[2 * (size_t)N + i];
+    }
+    if (enda4_out) std::memcpy(enda4_out, enda.data(), sizeof(F4) * N);
+    if (endb4_out) std::memcpy(endb4_out, endb.data(), sizeof(F4) * N);
+    return 0;
+}
+
 /* FP64 O(N*M) sum with the same smoothing kernel as the near field,
  * c(r) = (1 - exp(-(r/a)^3)) / (4 pi r^3), on the float input positions
  * promoted to double; r = 0 and (for segments) |x_b - y_p| = 0 excluded. */
@@ -768,4 +933,157 @@ extern "C" void orc_direct_sum(uint32_t N, const float *vort_pos4, const double 
         }
         u[t] = sx; v[t] = sy; w[t] = sz;
     }
+}
+
+/* VortexSimulationSystem::setDensityDomain (HFS/VortexSimulationSystemImp.cpp:
+ * 336-366): 1.2 x the largest bounding-box edge, centred on the box. */
+extern "C" void orc_density_domain(const float *pos4, uint32_t N, double *origin3, double *length) {
+    const F4 *pos = as_f4(pos4);
+    double maxx, minx, maxy, miny, maxz, minz;
+    maxx = minx = pos[0].x;
+    maxy = miny = pos[0].y;
+    maxz = minz = pos[0].z;
+    for (uint32_t i = 1; i < N; i++) {
+        if (pos[i].x < minx) minx = pos[i].x; else if (pos[i].x > maxx) maxx = pos[i].x;
+        if (pos[i].y < miny) miny = pos[i].y; else if (pos[i].y > maxy) maxy = pos[i].y;
+        if (pos[i].z < minz) minz = pos[i].z; else if (pos[i].z > maxz) maxz = pos[i].z;
+    }
+    const double L = 1.2 * std::max(std::max(maxx - minx, maxy - miny), maxz - minz);
+    origin3[0] = (minx + 0.5 * (maxx - minx)) - 0.5 * L;
+    origin3[1] = (miny + 0.5 * (maxy - miny)) - 0.5 * L;
+    origin3[2] = (minz + 0.5 * (maxz - minz)) - 0.5 * L;
+    *length = L;
+}
+
+/* HFS/GPU_kernel.cu:79-110 interpolate_weights2 / poly_shape2: (1 - r)^4 of the
+ * squared distance r in cells, zero for r >= 1. */
+static double weight_quartic(double gx, double gy, double gz, double px, double py, double pz) {
+    const double dx = gx - px, dy = gy - py, dz = gz - pz;
+    const double r = dx * dx + dy * dy + dz * dz;
+    const double rr = std::fabs(r);
+    const double r1 = 1 - rr;
+    const double r2 = r1 * r1;
+    const double r4 = r2 * r2;
+    return rr < 1 ? r4 : 0.0;
+}
+
+/* HFS/GPU_kernel.cu:52-90 interpolate_weights / poly_shape: trilinear hat. */
+static double hat(double r) {
+    const double rr = std::fabs(r);
+    return rr < 1 ? 1 - rr : 0.0;
+}
+
+/* VortexSimulationSystem::addBaroclinicForce (HFS/VortexSimulationSystemImp.cpp:
+ * 369-465): density grid of edge min(floor(L / 0.2) + 1, 200) over the heat
+ * particles' 1.2 x box; the heat particles hashed on it; AssignDensity
+ * (HFS/GPU_kernel.cu:3655-3740) = quartic-weighted mean of the particles' heat
+ * over the 5^3 hash cells around each grid cell, an empty hash cell adding its
+ * centre's weight with zero heat; GradDensity (3742-3797) = periodic central
+ * differences; ParticleGetBaroclinic (3800-3898) = the gradient interpolated
+ * (trilinear hat over 5^3 cells) at each vortex, crossed with (0, 10, 0), times
+ * 5 dt * 0.1, added to the strength.  Returns the grid edge (0 = nothing done:
+ * no heat particles or a zero-size box).  rho / grad (may be NULL) receive the
+ * grids when dim^3 <= cap. */
+extern "C" uint32_t orc_baroclinic(uint32_t H, const float *heat4, const float *life, uint32_t N,
+                                   const float *cent4, double *vx, double *vy, double *vz, double dt,
+                                   double *origin_out, double *h_out, float *rho_out, float *grad_out,
+                                   size_t cap) {
+    if (H == 0) return 0;
+    double origin[3], L;
+    orc_density_domain(heat4, H, origin, &L);
+    if (!(L > 0.0)) return 0;
+    double h = 0.2;
+    uint32_t dim = (uint32_t)(std::floor(L / h) + 1);
+    dim = std::min(std::max((uint32_t)0, dim), (uint32_t)200);
+    h = L / (double)dim;
+    const int d = (int)dim;
+    const size_t C = (size_t)dim * dim * dim;
+    const float h_f = (float)(L / (double)dim);
+    const float of[3] = {(float)origin[0], (float)origin[1], (float)origin[2]};
+    std::vector<uint32_t> key(H), idx(H), start(C), end(C);
+    orc_calc_hash(heat4, H, dim, h_f, of, key.data(), idx.data());
+    orc_sort_by_key(key.data(), idx.data(), H);
+    orc_find_cell_start(key.data(), H, (uint32_t)C, start.data(), end.data());
+    const F4 *hp = as_f4(heat4);
+    // AssignDensity
+    std::vector<float> rho(C);
+    const double invh = 1.0 / h;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t c = 0; c < (int64_t)C; c++) {
+        const int i = (int)(c % d), j = (int)((c / d) % d), k = (int)(c / ((int64_t)d * d));
+        const double gx = i + 0.5, gy = j + 0.5, gz = k + 0.5;
+        double sum = 0, tw = 0;
+        for (int kk = k - 2; kk <= k + 2; kk++)
+            for (int jj = j - 2; jj <= j + 2; jj++)
+                for (int ii = i - 2; ii <= i + 2; ii++) {
+                    if (!(kk >= 0 && kk < d && jj >= 0 && jj < d && ii >= 0 && ii < d)) continue;
+                    const size_t r = gidx(ii, jj, kk, d);
+                    if (start[r] != 0xFFFFFFFFu) {
+                        for (uint32_t p = start[r]; p < end[r]; p++) {
+                            const uint32_t q = idx[p];
+                            const float px = (float)((double)hp[q].x - origin[0]);
+                            const float py = (float)((double)hp[q].y - origin[1]);
+                            const float pz = (float)((double)hp[q].z - origin[2]);
+                            const double w = weight_quartic(gx, gy, gz, px * invh, py * invh, pz * invh);
+                            sum += w * (double)life[q];
+                            tw += w;
+                        }
+                    } else {
+                        // empty hash cell: its centre's weight, zero heat
+                        tw += weight_quartic(gx, gy, gz, ii + 0.5, jj + 0.5, kk + 0.5);
+                    }
+                }
+        if (tw < 1e-12) tw = 1e+24;
+        rho[c] = (float)(sum / tw);
+    }
+    // GradDensity (periodic)
+    std::vector<float> grad(3 * C);
+    for (int k = 0; k < d; k++)
+        for (int j = 0; j < d; j++)
+            for (int i = 0; i < d; i++) {
+                const size_t c = gidx(i, j, k, d);
+                const double t = rho[gidx(i, (j + 1) % d, k, d)], dn = rho[gidx(i, (j + d - 1) % d, k, d)];
+                const double l = rho[gidx((i + d - 1) % d, j, k, d)], r = rho[gidx((i + 1) % d, j, k, d)];
+                const double f = rho[gidx(i, j, (k + d - 1) % d, d)], b = rho[gidx(i, j, (k + 1) % d, d)];
+                grad[3 * c + 0] = (float)((r - l) * 0.5 * invh);
+                grad[3 * c + 1] = (float)((t - dn) * 0.5 * invh);
+                grad[3 * c + 2] = (float)((b - f) * 0.5 * invh);
+            }
+    // ParticleGetBaroclinic
+    const double inv_hf = 1.0 / (double)h_f;
+    const double dt_beta = dt * 5.0;
+    const F4 *cp = as_f4(cent4);
+#pragma omp parallel for schedule(static)
+    for (int64_t t = 0; t < (int64_t)N; t++) {
+        const float px = (float)((double)cp[t].x - origin[0]);
+        const float py = (float)((double)cp[t].y - origin[1]);
+        const float pz = (float)((double)cp[t].z - origin[2]);
+        auto cell = [&](float r) {
+            const double q = std::floor(r * inv_hf);
+            return !(q >= -3.0) ? -3 : (q > (double)(d + 2) ? d + 2 : (int)q);
+        };
+        const int i = cell(px), j = cell(py), k = cell(pz);
+        double sx = 0, sy = 0, sz = 0;
+        for (int kk = k - 2; kk <= k + 2; kk++)
+            for (int jj = j - 2; jj <= j + 2; jj++)
+                for (int ii = i - 2; ii <= i + 2; ii++) {
+                    if (!(kk >= 0 && kk < d && jj >= 0 && jj < d && ii >= 0 && ii < d)) continue;
+                    const size_t c = gidx(ii, jj, kk, d);
+                    const double w = hat((ii + 0.5) - px * inv_hf) * hat((jj + 0.5) - py * inv_hf) *
+                                     hat((kk + 0.5) - pz * inv_hf);
+                    sx += grad[3 * c + 0] * w;
+                    sy += grad[3 * c + 1] * w;
+                    sz += grad[3 * c + 2] * w;
+                }
+        const double v[3] = {0, 10, 0};
+        const double bx = sy * v[2] - sz * v[1], by = sz * v[0] - sx * v[2], bz = sx * v[1] - sy * v[0];
+        vx[t] += dt_beta * 0.1 * bx;
+        vy[t] += dt_beta * 0.1 * by;
+        vz[t] += dt_beta * 0.1 * bz;
+    }
+    if (origin_out) { origin_out[0] = origin[0]; origin_out[1] = origin[1]; origin_out[2] = origin[2]; }
+    if (h_out) *h_out = h;
+    if (rho_out && C <= cap) std::memcpy(rho_out, rho.data(), sizeof(float) * C);
+    if (grad_out && C <= cap) std::memcpy(grad_out, grad.data(), sizeof(float) * 3 * C);
+    return dim;
 }

@@ -26,6 +26,7 @@
 #ifndef PPPM_ORACLE_H
 #define PPPM_ORACLE_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -104,6 +105,32 @@ int orc_pppm(const orc_params *p, uint32_t N, const float *vort_pos4,
              const double *ax, const double *ay, const double *az,
              uint32_t M, const float *eval_a4, const float *eval_b4,
              int is_segment, double *u, double *v, double *w, orc_dump *dump);
+
+/* --- one vortex-segment time step (no boundary, heat or emitters) --------
+ * HFS/VortexSimulationSystemImp.cpp:90-125 solveTimeStep: convertVortToSeg
+ * (ComputePosb, HFS/GPU_kernel.cu:3184-3229, segment length cap h_seg),
+ * computeURotation (velocity at both segment ends, other end = centre),
+ * applyFlow (move_particle both ends, ComputePosa), convertSegToVort
+ * (ComputeVortex), computeStretching (VectorAdd, hash of the new centres,
+ * ParticleGaussianSmooth with width nu over the 5^3 hash cells,
+ * HFS/GPU_kernel.cu:3327-3438).  cent4 and vort (x,y,z arrays) are updated
+ * in place; enda4 / endb4 (optional, N float4) receive the moved ends.
+ * P passive points (tracers, heat particles; may be 0) are evaluated with the
+ * same far field (is_segment 0) and moved: pu/pv/pw receive their velocity. */
+void orc_gaussian_smooth(const orc_params *p, uint32_t N, const float *cent4, const double *dx, const double *dy,
+                         const double *dz, double nu, double *ox, double *oy, double *oz);
+int orc_vortex_step(const orc_params *p, uint32_t N, float *cent4, double *vx, double *vy, double *vz,
+                    double dt, double h_seg, double nu, float *enda4, float *endb4, uint32_t P,
+                    float *passive4, double *pu, double *pv, double *pw);
+
+/* --- buoyancy: heat particles -> density grid -> baroclinic vorticity ----
+ * HFS/VortexSimulationSystemImp.cpp:336-465, HFS/GPU_kernel.cu:3655-3898.
+ * Returns the density grid edge (0: nothing done). */
+void orc_density_domain(const float *pos4, uint32_t N, double *origin3, double *length);
+uint32_t orc_baroclinic(uint32_t H, const float *heat4, const float *life, uint32_t N,
+                        const float *cent4, double *vx, double *vy, double *vz, double dt,
+                        double *origin_out, double *h_out, float *rho_out, float *grad_out,
+                        size_t cap);
 
 /* --- FP64 O(N*M) smoothed Biot-Savart sum (accuracy ground truth) ------- */
 void orc_direct_sum(uint32_t N, const float *vort_pos4, const double *ax,

@@ -83,6 +83,18 @@ def lib():
         L.orc_direct_sum.argtypes = [C.c_uint32, f32p, f64p, f64p, f64p, C.c_uint32, f32p, f32p,
                                      C.c_int, C.c_double, f64p, f64p, f64p]
         L.orc_num_threads.restype = C.c_int
+        L.orc_vortex_step.argtypes = [C.POINTER(OrcParams), C.c_uint32, f32p, f64p, f64p, f64p, C.c_double,
+                                      C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_vortex_step.restype = C.c_int
+        L.orc_gaussian_smooth.argtypes = [C.POINTER(OrcParams), C.c_uint32, f32p, f64p, f64p, f64p, C.c_double,
+                                          f64p, f64p, f64p]
+        L.orc_gaussian_smooth.restype = None
+        L.orc_baroclinic.argtypes = [C.c_uint32, f32p, f32p, C.c_uint32, f32p, f64p, f64p, f64p, C.c_double,
+                                     f64p, f64p, C.c_void_p, C.c_void_p, C.c_size_t]
+        L.orc_baroclinic.restype = C.c_uint32
+        L.orc_density_domain.argtypes = [f32p, C.c_uint32, f64p, f64p]
+        L.orc_density_domain.restype = None
         _lib = L
     return _lib
 
@@ -228,6 +240,57 @@ def direct_sum(vort_pos4, alpha3, eval_a4, a, eval_b4=None, is_segment=0):
     lib().orc_direct_sum(vp.shape[0], vp, _c(al[:, 0], np.float64), _c(al[:, 1], np.float64),
                          _c(al[:, 2], np.float64), M, ea, eb, int(is_segment), float(a), u, v, w)
     return np.stack([u, v, w], axis=1)
+
+
+def vortex_step(prm: OrcParams, cent4, alpha3, dt, h_seg=0.1, nu=0.1, passive4=None):
+    """One reference time step; returns (cent4, alpha (N,3), enda4, endb4), plus
+    (passive4 moved, passive velocity (P,3)) when passive points are given."""
+    cent = np.array(cent4, dtype=np.float32, order="C", copy=True)
+    al = np.ascontiguousarray(alpha3, dtype=np.float64)
+    vx, vy, vz = (np.ascontiguousarray(al[:, c]) for c in range(3))
+    N = cent.shape[0]
+    ea = np.zeros((N, 4), np.float32)
+    eb = np.zeros((N, 4), np.float32)
+    P = 0 if passive4 is None else len(passive4)
+    pas = np.array(passive4, dtype=np.float32, order="C", copy=True) if P else np.zeros((1, 4), np.float32)
+    pvel = [np.zeros(max(P, 1)) for _ in range(3)]
+    rc = lib().orc_vortex_step(C.byref(prm), N, cent, vx, vy, vz, float(dt), float(h_seg), float(nu),
+                               ea.ctypes.data, eb.ctypes.data, P, pas.ctypes.data,
+                               *(v.ctypes.data for v in pvel))
+    if rc != 0:
+        raise RuntimeError("orc_vortex_step failed")
+    out = (cent, np.stack([vx, vy, vz], axis=1), ea, eb)
+    if P:
+        out = out + (pas, np.stack(pvel, axis=1))
+    return out
+
+
+def baroclinic(heat4, life, cent4, alpha3, dt, cap=0):
+    """addBaroclinicForce; returns (alpha (N,3), dim, origin, h, rho, grad) (grids when dim^3 <= cap)."""
+    heat = np.ascontiguousarray(heat4, dtype=np.float32)
+    lf = np.ascontiguousarray(life, dtype=np.float32)
+    cent = np.ascontiguousarray(cent4, dtype=np.float32)
+    al = np.ascontiguousarray(alpha3, dtype=np.float64)
+    vx, vy, vz = (np.ascontiguousarray(al[:, c]) for c in range(3))
+    o = np.zeros(3); h = np.zeros(1)
+    rho = np.zeros(max(cap, 1), np.float32)
+    grad = np.zeros(3 * max(cap, 1), np.float32)
+    dim = lib().orc_baroclinic(len(heat), heat, lf, len(cent), cent, vx, vy, vz, float(dt), o, h,
+                               rho.ctypes.data, grad.ctypes.data, cap)
+    c = dim ** 3
+    g = (rho[:c].copy(), grad[:3 * c].reshape(c, 3).copy()) if dim and c <= cap else (None, None)
+    return np.stack([vx, vy, vz], axis=1), dim, o, float(h[0]), g[0], g[1]
+
+
+def gaussian_smooth(prm: OrcParams, cent4, d3, nu=0.1):
+    """Hash of cent4 + Gaussian-weighted mean of d3 (N, 3) over 5^3 cells; returns (N, 3)."""
+    cent = np.ascontiguousarray(cent4, dtype=np.float32)
+    d = np.ascontiguousarray(d3, dtype=np.float64)
+    dx, dy, dz = (np.ascontiguousarray(d[:, c]) for c in range(3))
+    N = cent.shape[0]
+    out = [np.zeros(N) for _ in range(3)]
+    lib().orc_gaussian_smooth(C.byref(prm), N, cent, dx, dy, dz, float(nu), *out)
+    return np.stack(out, axis=1)
 
 
 def num_threads():

@@ -204,6 +204,83 @@ class Scene:
         self.N = N
         return pos4
 
+    def vortex_step(self, pos4: torch.Tensor, alpha: torch.Tensor, dt: float, h_seg: float = 0.1,
+                    nu: float = 0.1, return_ends: bool = False, passive: torch.Tensor | None = None):
+        """One vortex-segment time step of the reference's solveTimeStep (pppm_vortex_step).
+
+        pos4 (CUDA float32 (N, 4)) and alpha (CUDA float64 (N, 3) or (3, N)) are
+        updated in place.  passive (CUDA float32 (P, 4), tracers or heat
+        particles) is moved in place with the velocity of the same far field.
+        Returns (pos4, alpha), then (enda, endb) with return_ends, then the
+        passive velocity (P, 3) float64 when passive points are given.
+        """
+        if pos4.dtype != torch.float32 or not pos4.is_cuda or not pos4.is_contiguous() or pos4.shape[1] != 4:
+            raise ValueError("pos4 must be a contiguous CUDA float32 (N, 4) tensor (updated in place)")
+        N = pos4.shape[0]
+        P = 0 if passive is None else passive.shape[0]
+        if P and (passive.dtype != torch.float32 or not passive.is_cuda or not passive.is_contiguous()
+                  or passive.shape[1] != 4):
+            raise ValueError("passive must be a contiguous CUDA float32 (P, 4) tensor (updated in place)")
+        with torch.cuda.stream(self.stream):
+            ax, ay, az = _alpha3(alpha, N)
+            ea = eb = None
+            if return_ends:
+                ea = torch.empty((N, 4), dtype=torch.float32, device=pos4.device)
+                eb = torch.empty((N, 4), dtype=torch.float32, device=pos4.device)
+            pvel = torch.empty((3, max(P, 1)), dtype=torch.float64, device=pos4.device)
+            check(self._lib.pppm_vortex_step(self._h, N, _ptr(pos4), _ptr(ax), _ptr(ay), _ptr(az), float(dt),
+                                             float(h_seg), float(nu), _ptr(ea), _ptr(eb), P,
+                                             _ptr(passive) if P else None, _ptr(pvel[0]) if P else None,
+                                             _ptr(pvel[1]) if P else None, _ptr(pvel[2]) if P else None),
+                  "pppm_vortex_step")
+            if alpha.shape == (N, 3):
+                alpha.copy_(torch.stack([ax, ay, az], dim=1))
+            else:
+                alpha.copy_(torch.stack([ax, ay, az], dim=0))
+        self.N = N
+        out = (pos4, alpha)
+        if return_ends:
+            out = out + (ea, eb)
+        if P:
+            out = out + (pvel.t()[:P].contiguous(),)
+        return out
+
+    def baroclinic(self, heat4: torch.Tensor, heat: torch.Tensor, pos4: torch.Tensor, alpha: torch.Tensor,
+                   dt: float):
+        """Buoyancy source (pppm_baroclinic): adds the baroclinic vorticity of the
+        heat particles (heat4 (H, 4) float32, heat (H,) float32) to alpha (in place)."""
+        N = pos4.shape[0]
+        H = heat4.shape[0]
+        for t, nm in ((heat4, "heat4"), (pos4, "pos4")):
+            if t.dtype != torch.float32 or not t.is_cuda or not t.is_contiguous() or t.shape[1] != 4:
+                raise ValueError(f"{nm} must be a contiguous CUDA float32 (n, 4) tensor")
+        if heat.dtype != torch.float32 or not heat.is_cuda or heat.shape != (H,):
+            raise ValueError("heat must be a CUDA float32 (H,) tensor")
+        hc = heat.contiguous()
+        with torch.cuda.stream(self.stream):
+            ax, ay, az = _alpha3(alpha, N)
+            check(self._lib.pppm_baroclinic(self._h, H, _ptr(heat4), _ptr(hc), N, _ptr(pos4),
+                                            _ptr(ax), _ptr(ay), _ptr(az), float(dt)), "pppm_baroclinic")
+            if alpha.shape == (N, 3):
+                alpha.copy_(torch.stack([ax, ay, az], dim=1))
+            else:
+                alpha.copy_(torch.stack([ax, ay, az], dim=0))
+        return alpha
+
+    def density(self):
+        """(dim, origin, h, rho (dim^3,) float32, grad (3, dim^3) float32) of the last pppm_baroclinic."""
+        dim = C.c_uint32()
+        org = (C.c_double * 3)()
+        h = C.c_double()
+        r = C.c_void_p()
+        g = C.c_void_p()
+        check(self._lib.pppm_get_density(self._h, C.byref(dim), org, C.byref(h), C.byref(r), C.byref(g)),
+              "pppm_get_density")
+        c = dim.value ** 3
+        rho = _copy_dev(r.value, c, torch.float32, self.stream)
+        grad = _copy_dev(g.value, 3 * c, torch.float32, self.stream).reshape(3, c)
+        return dim.value, tuple(org), h.value, rho, grad
+
     def set_profiling(self, on: bool = True):
         check(self._lib.pppm_scene_set_profiling(self._h, int(on)), "pppm_scene_set_profiling")
 

@@ -29,11 +29,14 @@ EXPORTED = (
     "pppm_spatial_hash_noalloc", "pppm_advect_euler", "pppm_advect_rk2", "pppm_batch_run",
     "pppm_server_create", "pppm_server_destroy", "pppm_server_add_scene", "pppm_server_submit",
     "pppm_server_wait", "pppm_server_read_positions", "pppm_server_stats",
-    "pppm_frame_path", "pppm_write_frame", "pppm_read_frame",
+    "pppm_frame_path", "pppm_write_frame", "pppm_read_frame", "pppm_vortex_step",
+    "pppm_baroclinic", "pppm_get_density", "pppm_write_sgi", "pppm_renderer_create", "pppm_renderer_destroy",
+    "pppm_render_shadows", "pppm_render_shadow_map", "pppm_render_smoke",
 )
 REQ_EVAL, REQ_ADVANCE = 0, 1
 NOALLOC_MAX_PARTICLES = 1048576  # PPPM_NOALLOC_MAX_PARTICLES in include/pppm.h
-STAGES = ("domain", "vort_sort", "cells_reorder", "p2m", "multigrid", "farfield", "eval_sort", "eval")
+STAGES = ("domain", "vort_sort", "cells_reorder", "p2m", "multigrid", "farfield", "eval_sort", "eval",
+          "segments", "seg_to_blob", "rehash", "gaussian_smooth")
 
 
 class PppmParams(C.Structure):
@@ -130,6 +133,19 @@ def load(build_if_missing: bool = True):
         "pppm_spatial_hash_noalloc": (st, [u32, vp, u32, C.c_float, C.POINTER(C.c_float), vp, vp, vp, vp, vp]),
         "pppm_advect_euler": (st, [vp, u32, vp, vp, vp, vp, C.c_double]),
         "pppm_advect_rk2": (st, [vp, u32, vp, vp, vp, vp, C.c_double]),
+        "pppm_vortex_step": (st, [vp, u32, vp, vp, vp, vp, C.c_double, C.c_double, C.c_double, vp, vp, u32, vp,
+                                  vp, vp, vp]),
+        "pppm_baroclinic": (st, [vp, u32, vp, vp, u32, vp, vp, vp, vp, C.c_double]),
+        "pppm_write_sgi": (st, [C.c_char_p, u32, u32, C.c_int, vp, C.c_int]),
+        "pppm_renderer_create": (st, [vp, C.POINTER(vp)]),
+        "pppm_renderer_destroy": (st, [vp]),
+        "pppm_render_shadows": (st, [vp, u32, vp, vp, C.c_float, C.c_float, C.POINTER(C.c_float), C.c_float, vp,
+                                     C.POINTER(u32)]),
+        "pppm_render_shadow_map": (st, [vp, C.POINTER(vp), C.POINTER(u32)]),
+        "pppm_render_smoke": (st, [vp, u32, vp, vp, vp, vp, C.c_float, C.c_float, vp, C.POINTER(C.c_float),
+                                   C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_float, u32, u32, vp]),
+        "pppm_get_density": (st, [vp, C.POINTER(u32), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                  C.POINTER(vp), C.POINTER(vp)]),
         "pppm_batch_run": (st, [C.POINTER(PppmBatchItem), u32, vp]),
         "pppm_server_create": (st, [C.POINTER(PppmServerConfig), C.POINTER(vp)]),
         "pppm_server_destroy": (st, [vp]),

@@ -1,5 +1,6 @@
 // C ABI of the PPPM path: scene lifecycle, the BiotSavartSolver entry points,
 // the standalone multigrid object, and the FP64 direct sum.
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdarg>
@@ -59,6 +60,7 @@ void free_vortex_side(pppm_scene *s) {
     cudaFree(s->vrec); s->vrec = nullptr;
     cudaFree(s->valf); s->valf = nullptr;
     cudaFree(s->adv_mid); s->adv_mid = nullptr;
+    cudaFree(s->ts_kappa); s->ts_kappa = nullptr;
     cudaFree(s->bbox_partial); s->bbox_partial = nullptr;
 }
 
@@ -96,6 +98,7 @@ cudaError_t alloc_vortex_side(pppm_scene *s, uint32_t cap) {
     PPPM_CUDA_TRY(dalloc(&s->vrec, cap));
     PPPM_CUDA_TRY(dalloc(&s->valf, cap));
     PPPM_CUDA_TRY(dalloc(&s->adv_mid, cap));
+    PPPM_CUDA_TRY(dalloc(&s->ts_kappa, cap));
     s->bbox_blocks = 148 * 2;
     PPPM_CUDA_TRY(dalloc(&s->bbox_partial, 6 * (size_t)s->bbox_blocks));
     return alloc_hist(s);
@@ -186,6 +189,7 @@ void destroy_scene(pppm_scene *s) {
     cudaFree(s->pair_count);
     cudaFree(s->coarse_op);
     if (s->mg_graph) cudaGraphExecDestroy(s->mg_graph);
+    pppm::free_buoyancy(s->buoy);
     delete s;
 }
 
@@ -475,6 +479,78 @@ extern "C" pppm_status pppm_advect_rk2(pppm_scene *s, uint32_t N, float *pos4, c
     return advect_common(s, N, pos4, ax, ay, az, dt, true);
 }
 
+// One vortex-segment time step (HFS/VortexSimulationSystemImp.cpp:90-125 without
+// boundary, buoyancy, heat or shedding).  The kernels and the order of the
+// reference's sub-steps are described in timestep.cu.
+extern "C" pppm_status pppm_vortex_step(pppm_scene *s, uint32_t N, float *cent4, double *ax, double *ay, double *az,
+                                        double dt, double h_seg, double nu, float *enda4, float *endb4, uint32_t P,
+                                        float *passive4, double *pu, double *pv, double *pw) {
+    if (!s || !cent4 || !ax || !ay || !az || N == 0) {
+        snprintf(g_err, sizeof(g_err), "pppm_vortex_step: NULL pointer or N == 0");
+        return PPPM_ERR_INVALID;
+    }
+    if (!std::isfinite(dt) || !(h_seg > 0.0) || !std::isfinite(h_seg) || !(nu > 0.0) || !std::isfinite(nu)) {
+        snprintf(g_err, sizeof(g_err), "pppm_vortex_step: dt must be finite, h_seg and nu finite and > 0");
+        return PPPM_ERR_INVALID;
+    }
+    if (P > 0 && (!passive4 || !pu || !pv || !pw)) {
+        snprintf(g_err, sizeof(g_err), "pppm_vortex_step: passive points need positions and velocity arrays");
+        return PPPM_ERR_INVALID;
+    }
+    if ((uint64_t)N * 2u > 0xFFFFFFFFull) {
+        snprintf(g_err, sizeof(g_err), "pppm_vortex_step: N=%u too large (2N evaluation points)", N);
+        return PPPM_ERR_INVALID;
+    }
+    using namespace pppm;
+    pppm_status rc = pppm_set_vortices(s, N, cent4, ax, ay, az);
+    if (rc != PPPM_OK) return rc;
+    const uint32_t M = 2 * N;
+    cudaError_t e = cudaSuccess;
+    if (std::max(M, P) > s->capM) e = alloc_eval_side(s, std::max(M, P));
+    if (e != cudaSuccess) return cuda_fail("pppm_vortex_step (grow eval buffers)", e);
+    float4 *ends = s->stage_ea, *other = s->stage_eb;
+    double *u = s->stage_out;
+    const size_t us = s->capM;
+    prof_begin(s, kStageSegments);
+    e = launch_segments(s, h_seg, N, ends, other, s->ts_kappa);
+    prof_end(s, kStageSegments);
+    if (e != cudaSuccess) return cuda_fail("pppm_vortex_step (segments)", e);
+    rc = pppm_build_far_field(s);
+    if (rc != PPPM_OK) return rc;
+    rc = eval_common(s, M, reinterpret_cast<const float *>(ends), reinterpret_cast<const float *>(other), 1, u,
+                     u + us, u + 2 * us, nullptr, 0);
+    if (rc != PPPM_OK) return rc;
+    // tracers and heat particles: plain evaluation with the same far field,
+    // then move_particle (evaluateBiotSavart, VSSImp.cpp:1195-1244)
+    if (P > 0) {
+        rc = eval_common(s, P, passive4, passive4, 0, pu, pv, pw, nullptr, 0);
+        if (rc != PPPM_OK) return rc;
+        e = launch_move3(s, reinterpret_cast<float4 *>(passive4), pu, pv, pw, dt, P);
+        if (e != cudaSuccess) return cuda_fail("pppm_vortex_step (passive move)", e);
+    }
+    // From here the scene's vortex copy holds the moved centres and the
+    // unsmoothed strengths: its far field no longer matches them.
+    s->far_ready = false;
+    s->vort_set = false;
+    s->ref_valid = false;
+    prof_begin(s, kStageSegToBlob);
+    e = launch_segment_to_blob(s, ends, u, us, s->ts_kappa, dt, N, reinterpret_cast<float4 *>(cent4),
+                               reinterpret_cast<float4 *>(enda4), reinterpret_cast<float4 *>(endb4));
+    prof_end(s, kStageSegToBlob);
+    if (e != cudaSuccess) return cuda_fail("pppm_vortex_step (move)", e);
+    prof_begin(s, kStageRehash);
+    e = launch_bbox_and_params(s);
+    if (e == cudaSuccess) e = launch_hash_sort(s, s->vpos, N, s->vkey, s->vidx, &s->vsorted_key, &s->vsorted_idx);
+    if (e == cudaSuccess) e = launch_cells_reorder(s);
+    prof_end(s, kStageRehash);
+    if (e != cudaSuccess) return cuda_fail("pppm_vortex_step (hash)", e);
+    prof_begin(s, kStageSmooth);
+    e = launch_gaussian_smooth(s, nu, N, ax, ay, az);
+    prof_end(s, kStageSmooth);
+    if (e != cudaSuccess) return cuda_fail("pppm_vortex_step (smoothing)", e);
+    return PPPM_OK;
+}
+
 extern "C" pppm_status pppm_get_domain(pppm_scene *s, double origin[3], double *length, double *cell_h) {
     if (!s) return PPPM_ERR_INVALID;
     if (!s->far_ready) { snprintf(g_err, sizeof(g_err), "pppm_get_domain: no far field built"); return PPPM_ERR_STATE; }
@@ -561,7 +637,8 @@ unsigned long long launch_count() { return g_launches.load(std::memory_order_rel
 
 const char *stage_name(int i) {
     static const char *names[kNumStages] = {"domain", "vort_sort", "cells_reorder", "p2m",
-                                            "multigrid", "farfield", "eval_sort", "eval"};
+                                            "multigrid", "farfield", "eval_sort", "eval",
+                                            "segments", "seg_to_blob", "rehash", "gaussian_smooth"};
     return (i >= 0 && i < kNumStages) ? names[i] : "";
 }
 

@@ -87,3 +87,54 @@ extern "C" pppm_status pppm_read_frame(const char *path, float *pos4_host, uint3
     std::fclose(f);
     return got == n ? PPPM_OK : PPPM_ERR_INVALID;
 }
+
+// SGI image files, as Particle_renderer/.../write_sgi.cpp writes them: a
+// 512-byte big-endian header (magic 474, verbatim storage, 1 or 2 bytes per
+// channel, dimension 2 or 3, width, height, channels, pixmin 0, pixmax 255 or
+// 65535, zero padding), then each channel as rows bottom-up, value =
+// trunc(clamp(pixel * 256 (or 65536), 0, 255 (or 65535))).
+extern "C" pppm_status pppm_write_sgi(const char *path, uint32_t ni, uint32_t nj, int channels, const float *pix,
+                                      int high_precision) {
+    if (!path || !pix || (channels != 1 && channels != 3) || ni == 0 || nj == 0 || ni > 65535 || nj > 65535) {
+        pppm_set_error("pppm_write_sgi: invalid argument");
+        return PPPM_ERR_INVALID;
+    }
+    const bool hp = high_precision != 0;
+    std::vector<unsigned char> out;
+    out.reserve(512 + (size_t)ni * nj * channels * (hp ? 2 : 1));
+    auto u16 = [&](unsigned v) { out.push_back((unsigned char)(v >> 8)); out.push_back((unsigned char)v); };
+    auto u32 = [&](unsigned v) { u16(v >> 16); u16(v & 0xFFFFu); };
+    u16(474);
+    out.push_back(0);
+    out.push_back(hp ? 2 : 1);
+    u16(channels == 1 ? 2 : 3);
+    u16(ni);
+    u16(nj);
+    u16((unsigned)channels);
+    u32(0);
+    u32(hp ? 65535u : 255u);
+    out.insert(out.end(), 492, 0);
+    const float scale = hp ? 65536.0f : 256.0f;
+    for (int c = 0; c < channels; c++)
+        for (uint32_t j = 0; j < nj; j++)
+            for (uint32_t i = 0; i < ni; i++) {
+                float v = pix[(size_t)channels * (i + (size_t)ni * j) + c] * scale;
+                if (!(v >= 0.0f)) v = 0.0f;  // negative (or NaN) -> 0
+                else if (!hp && v > 255.0f) v = 255.0f;
+                else if (hp && v > 65535.0f) v = 65535.0f;
+                if (hp) u16((unsigned short)v);
+                else out.push_back((unsigned char)v);
+            }
+    FILE *f = std::fopen(path, "wb");
+    if (!f) {
+        pppm_set_error("pppm_write_sgi: cannot open %s", path);
+        return PPPM_ERR_INVALID;
+    }
+    const size_t wrote = std::fwrite(out.data(), 1, out.size(), f);
+    std::fclose(f);
+    if (wrote != out.size()) {
+        pppm_set_error("pppm_write_sgi: short write to %s", path);
+        return PPPM_ERR_INVALID;
+    }
+    return PPPM_OK;
+}

@@ -474,6 +474,24 @@ cudaError_t launch_gather_sorted(pppm_scene *s, float4 *pos_out, double *alpha_o
     return cudaGetLastError();
 }
 
+cudaError_t launch_explicit_hash(cudaStream_t st, const float4 *pos, uint32_t N, float h, const float of[3],
+                                 uint32_t n, uint32_t *key[2], uint32_t *idx[2], uint32_t *hist,
+                                 uint32_t **skey, uint32_t **sidx, uint32_t *start, uint32_t *end) {
+    ::pppm::note_launch();
+    keys_explicit_kernel<<<blocks_for(N, 256), 256, 0, st>>>(pos, N, h, of[0], of[1], of[2], n, key[0], idx[0]);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = radix_sort_pairs(st, N, key_bits(n), key, idx, hist, skey, sidx);
+    const size_t C = (size_t)n * n * n;
+    if (e == cudaSuccess) e = cudaMemsetAsync(start, 0xFF, sizeof(uint32_t) * C, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(end, 0xFF, sizeof(uint32_t) * C, st);
+    if (e == cudaSuccess) {
+        ::pppm::note_launch();
+        cells_only_kernel<<<blocks_for(N, 256), 256, 0, st>>>(*skey, N, start, end);
+        e = cudaGetLastError();
+    }
+    return e;
+}
+
 }  // namespace pppm
 
 // ---------------------------------------------------------------------------

@@ -79,6 +79,11 @@ struct MGPlan {
 cudaError_t build_coarse_operator(int d, double *op, cudaStream_t st);
 cudaError_t mg_capture_graph(const MGPlan &m, cudaGraphExec_t *exec, unsigned *kernel_nodes);
 
+// Density grid and heat-particle hash of the buoyancy source (buoyancy.cu),
+// allocated on first use.
+struct Buoyancy;
+void free_buoyancy(Buoyancy *b);
+
 }  // namespace pppm
 
 // Scene: every buffer is sized at creation (or on growth in
@@ -136,6 +141,8 @@ struct pppm_scene {
     float4 *stage_ea = nullptr, *stage_eb = nullptr;  // pppm_solve_host staging [capM]
     double *stage_out = nullptr;                       // [3][capM]
     float4 *adv_mid = nullptr;                         // RK2 midpoint positions [capN]
+    double *ts_kappa = nullptr;                        // segment stretch factor [capN]
+    pppm::Buoyancy *buoy = nullptr;                    // heat -> density grid, on first use
 
     // per-stage CUDA-event timing (pppm_scene_set_profiling)
     bool profiling = false;
@@ -160,7 +167,11 @@ enum Stage {
     kStageFar = 5,         // curl + far-field correction
     kStageEvalSort = 6,    // evaluation-point keys + radix sort
     kStageEval = 7,        // interpolation + near field + deorder
-    kNumStages = 8
+    kStageSegments = 8,    // vortex step: blobs -> segments
+    kStageSegToBlob = 9,   // vortex step: move ends, midpoint, strength update
+    kStageRehash = 10,     // vortex step: domain + hash of the moved centres
+    kStageSmooth = 11,     // vortex step: Gaussian smoothing of the strengths
+    kNumStages = 12
 };
 const char *stage_name(int i);
 
@@ -191,6 +202,18 @@ cudaError_t launch_eval(pppm_scene *s, const float4 *eval_a, const float4 *eval_
 cudaError_t launch_gather_sorted(pppm_scene *s, float4 *pos_out, double *alpha_out);
 cudaError_t launch_move(pppm_scene *s, const float4 *base, const double *u, size_t stride, double dt, uint32_t N,
                         float4 *out);
+
+// Reference hash (keys, stable sort, start/end tables) on an explicit grid.
+cudaError_t launch_explicit_hash(cudaStream_t st, const float4 *pos, uint32_t N, float h, const float of[3],
+                                 uint32_t n, uint32_t *key[2], uint32_t *idx[2], uint32_t *hist,
+                                 uint32_t **skey, uint32_t **sidx, uint32_t *start, uint32_t *end);
+cudaError_t launch_segments(pppm_scene *s, double h_seg, uint32_t N, float4 *ends, float4 *other, double *kappa);
+cudaError_t launch_segment_to_blob(pppm_scene *s, const float4 *ends, const double *u, size_t ustride,
+                                   const double *kappa, double dt, uint32_t N, float4 *cent, float4 *enda_out,
+                                   float4 *endb_out);
+cudaError_t launch_gaussian_smooth(pppm_scene *s, double nu, uint32_t N, double *ox, double *oy, double *oz);
+cudaError_t launch_move3(pppm_scene *s, float4 *pos, const double *u, const double *v, const double *w, double dt,
+                         uint32_t N);
 
 cudaError_t mg_solve(const MGPlan &m, int mode, double tol, int max_cycles, int *cycles_out,
                      double *relres_out);
