@@ -57,7 +57,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--particles", type=int, default=N_PART)
     ap.add_argument("--grid", type=int, default=GRID)
-    ap.add_argument("--workload", default="ring", choices=["ring", "mix", "serve"],
+    ap.add_argument("--workload", default="ring", choices=["ring", "mix", "serve", "render"],
                     help="ring: the at-scale single scene (default); mix: 64 independent scenes, "
                          "one after another vs in one batch")
     ap.add_argument("--scenes", type=int, default=64)
@@ -512,6 +512,86 @@ def run_serve(args, world, rank, local):
     srv.close()
 
 
+def run_render(args, world, rank, local):
+    """One rendered frame of the ring (1,048,576 particles by default):
+    the shadow pass seen from the light, then the smoke pass into a 1440 x 960
+    image (the reference renderer's frame size), device-timed per frame with
+    the particles resident; e2e adds the position / density upload and the
+    image download.  The reference's own CPU renderer (oracle/_ref, compiled
+    from its sources) renders the same frame once on the host as the CPU
+    baseline."""
+    import torch
+    from pppm_vortex_bouyant_flow_sample_b200 import workloads as W
+    from pppm_vortex_bouyant_flow_sample_b200.render import Renderer
+    torch.cuda.set_device(local)
+    N = args.particles
+    pos, _ = W.vortex_ring(N, seed=1)
+    dens = np.ones(N, np.float32)
+    base = np.tile(np.array([[0.5, 0.7, 0.9]], np.float32), (N, 1))
+    lit = np.tile(np.array([[0.9, 0.9, 0.99]], np.float32), (N, 1))
+    view = dict(radius=0.004, opacity=0.02, light=(0.5, 6.0, -3.0), quality=2.0, background=(0.0, 0.0, 0.0),
+                camera=(0.5, 0.9, -1.5), target=(0.5, 0.5, 0.5), perspective=2.0, width=1440, height=960)
+    rnd = Renderer()
+    dpos, ddens = torch.from_numpy(pos).cuda(), torch.from_numpy(dens).cuda()
+    dbase, dlit = torch.from_numpy(base).cuda(), torch.from_numpy(lit).cuda()
+    stream = torch.cuda.current_stream()
+
+    def frame(p, d):
+        illum, _ = rnd.shadows(p, d, view["radius"], view["opacity"], view["light"], view["quality"])
+        return rnd.smoke(p, illum, dbase, dlit, view["radius"], view["opacity"], d, view["background"],
+                         view["camera"], view["target"], view["perspective"], view["width"], view["height"])
+
+    for _ in range(max(args.warmup, 3)):
+        frame(dpos, ddens)
+    torch.cuda.synchronize()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        frame(dpos, ddens)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    frame_ms = statistics.median(ms)
+    hpos, hdens = torch.from_numpy(pos).pin_memory(), torch.from_numpy(dens).pin_memory()
+    e2e = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        img = frame(hpos.cuda(non_blocking=True), hdens.cuda(non_blocking=True)).cpu()
+        e2e.append(time.perf_counter() - t0)
+    e2e_s = statistics.median(e2e)
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import pyrender_ref as R
+        if R.available():
+            t0 = time.perf_counter()
+            ok, il, _ = R.compute_shadows(pos, view["radius"], view["opacity"], dens, view["light"], view["quality"])
+            ref = R.render_smoke(pos, il, base, lit, view["radius"], view["opacity"], dens, view["light"],
+                                 view["background"], view["camera"], view["target"], view["perspective"],
+                                 view["width"], view["height"])
+            sec = time.perf_counter() - t0
+            err = float(np.abs(ref - img.numpy()).max())
+            cpu = {"value": 1.0 / sec, "unit": "frames/s", "cores": 1, "kind": "reference",
+                   "sample": f"one full frame ({N:,} particles) by the reference's CPU renderer (oracle/_ref), "
+                             f"max |image difference| vs this frame {err:.2e}"}
+    if rank == 0:
+        print(json.dumps({
+            "metric": "rendered frames/s (shadow + smoke splatting)", "value": 1000.0 / frame_ms,
+            "unit": "frames/s", "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3),
+            "ms_per_step": frame_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"vortex ring frame, {N:,} particles, 1440x960 image, shadow map quality 2",
+                       "l2": "flushed between timed frames (512 MB write)"},
+            "e2e": {"value": 1.0 / e2e_s, "unit": "frames/s", "h2d_bytes_per_step": N * 20,
+                    "d2h_bytes_per_step": 1440 * 960 * 12},
+            "cpu_baseline": cpu}), flush=True)
+    rnd.close()
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
@@ -523,6 +603,9 @@ def main():
         return
     if args.workload == "serve":
         run_serve(args, world, rank, local)
+        return
+    if args.workload == "render":
+        run_render(args, world, rank, local)
         return
     run_b200(args, world, rank, local)
 

@@ -48,6 +48,26 @@ def lib():
     return _lib
 
 
+class _quiet_stdout:
+    """The reference renderer prints progress with printf; send the process's
+    fd 1 to /dev/null around its calls so callers' stdout stays clean."""
+
+    def __enter__(self):
+        import sys
+        sys.stdout.flush()
+        self._saved = os.dup(1)
+        self._null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self._null, 1)
+        return self
+
+    def __exit__(self, *exc):
+        C.CDLL(None).fflush(None)
+        os.dup2(self._saved, 1)
+        os.close(self._saved)
+        os.close(self._null)
+        return False
+
+
 def _v3(v):
     return np.asarray(v, dtype=np.float32).reshape(3).copy()
 
@@ -60,8 +80,9 @@ def compute_shadows(xyz, radius, opacity, dens, light, quality=1.0, cap=4096 * 4
     illum = np.zeros(max(n, 1), np.float32)
     npix = C.c_int(0)
     sm = np.zeros(cap, np.float32)
-    ok = lib().ref_compute_shadows(n, x, float(radius), float(opacity), d, _v3(light), float(quality), illum,
-                                   C.byref(npix), sm, cap)
+    with _quiet_stdout():
+        ok = lib().ref_compute_shadows(n, x, float(radius), float(opacity), d, _v3(light), float(quality), illum,
+                                       C.byref(npix), sm, cap)
     k = npix.value
     return bool(ok), illum[:n], sm[:k * k].reshape(k, k)
 
@@ -71,11 +92,12 @@ def render_smoke(xyz, illum, base_rgb, lit_rgb, radius, opacity, den, light, bac
     """Returns the image as (height, width, 3) float32."""
     x = np.ascontiguousarray(np.asarray(xyz, dtype=np.float32)[:, :3])
     img = np.zeros((height, width, 3), np.float32)
-    lib().ref_render_smoke(len(x), x, np.ascontiguousarray(illum, dtype=np.float32),
-                           np.ascontiguousarray(base_rgb, dtype=np.float32),
-                           np.ascontiguousarray(lit_rgb, dtype=np.float32), float(radius), float(opacity),
-                           np.ascontiguousarray(den, dtype=np.float32), _v3(light), _v3(background), _v3(camera),
-                           _v3(target), float(perspective), int(width), int(height), img)
+    with _quiet_stdout():
+        lib().ref_render_smoke(len(x), x, np.ascontiguousarray(illum, dtype=np.float32),
+                               np.ascontiguousarray(base_rgb, dtype=np.float32),
+                               np.ascontiguousarray(lit_rgb, dtype=np.float32), float(radius), float(opacity),
+                               np.ascontiguousarray(den, dtype=np.float32), _v3(light), _v3(background),
+                               _v3(camera), _v3(target), float(perspective), int(width), int(height), img)
     return img
 
 

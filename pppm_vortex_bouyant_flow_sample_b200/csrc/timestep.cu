@@ -23,8 +23,9 @@
 // The two end evaluations run as one launch over 2N points.  The segment
 // conversion, the move, the midpoint and the strength update are fused into
 // two elementwise kernels.  The smoothing walks the vortices in hash order, a
-// warp at a time, staging 32 records of a cell in shared memory and summing
-// weights in FP32 per staged chunk and in FP64 across chunks.
+// warp at a time, staging 32 records of a cell in shared memory as 16 record
+// pairs that Blackwell's packed f32x2 instructions process two at a time, and
+// sums the weights in FP32 per staged chunk and in FP64 across chunks.
 #include <cmath>
 
 #include "pppm_internal.cuh"
@@ -116,6 +117,27 @@ __global__ void move3_kernel(float4 *__restrict__ pos, const double *__restrict_
     pos[t] = moved(pos[t], u[t], v[t], w[t], dt);
 }
 
+// 2^x by the MUFU.EX2 instruction (PTX ex2.approx.ftz.f32, relative error about
+// 2^-22; results below 2^-126 flush to zero, weights negligible beside the
+// vortex's own weight 1).
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// Shared staging of a chunk of 32 records as 16 pairs: slot p holds records
+// 2p (.x, .z halves) and 2p+1 (.y, .w halves).  Planes: {-x, -y}, {-z, ax},
+// {ay, az}.
+constexpr int kSlots = 16;
+__device__ __forceinline__ void stage_pair(float *__restrict__ pk, int slot, int half, float nx, float ny, float nz,
+                                           float ax, float ay, float az) {
+    float *A = pk + 4 * slot, *B = pk + 4 * (kSlots + slot), *Cc = pk + 4 * (2 * kSlots + slot);
+    A[half] = nx; A[2 + half] = ny;
+    B[half] = nz; B[2 + half] = ax;
+    Cc[half] = ay; Cc[2 + half] = az;
+}
+
 __device__ __forceinline__ int clamp_cell(double q, int n) {
     // cells more than two outside the grid see no in-grid cell: any value past
     // that behaves the same, so clamp before converting to int
@@ -134,10 +156,10 @@ __global__ void __launch_bounds__(kSmoothThreads) gaussian_smooth_kernel(
     const float4 *__restrict__ vrec, const float4 *__restrict__ valf, const uint32_t *__restrict__ sidx,
     const uint32_t *__restrict__ cstart, const uint32_t *__restrict__ cend, const DevParams *__restrict__ P,
     float wscale, uint32_t N, double *__restrict__ ox, double *__restrict__ oy, double *__restrict__ oz) {
-    __shared__ float4 s_rec[kSmoothThreads];
-    __shared__ float4 s_alf[kSmoothThreads];
+    __shared__ float4 s_pk[(kSmoothThreads / 32) * 3 * kSlots];
     const int lane = threadIdx.x & 31;
     const int wbase = threadIdx.x & ~31;
+    const int wpk = (threadIdx.x >> 5) * 3 * kSlots;
     const uint32_t t0 = (blockIdx.x * blockDim.x) + wbase;
     if (t0 >= N) return;
     const uint32_t t = t0 + lane;
@@ -169,6 +191,8 @@ __global__ void __launch_bounds__(kSmoothThreads) gaussian_smooth_kernel(
     const int zhi = min(__reduce_max_sync(0xffffffffu, ck) + 2, n - 1);
 
     double tw = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
+    const float2 tx = make_float2(ra.x, ra.x), ty = make_float2(ra.y, ra.y), tz = make_float2(ra.z, ra.z);
+    const float2 ws2 = make_float2(wscale, wscale);
     auto walk = [&](int x0, int x1, int y0, int y1, int z0, int z1, bool member) {
         for (int z = z0; z <= z1; z++)
             for (int y = y0; y <= y1; y++)
@@ -181,28 +205,39 @@ __global__ void __launch_bounds__(kSmoothThreads) gaussian_smooth_kernel(
                     if (!__any_sync(0xffffffffu, ok)) continue;
                     for (uint32_t base = s0; base < s1; base += 32) {
                         const uint32_t cnt = min(32u, s1 - base);
+                        // stage the chunk as 16 record pairs (records 2p, 2p+1 in
+                        // the .x / .y halves) for packed f32x2 arithmetic; an odd
+                        // chunk is padded with a record at 1e18 and zero strength
+                        float *pk = reinterpret_cast<float *>(s_pk + wpk);
                         if ((uint32_t)lane < cnt) {
-                            s_rec[wbase + lane] = vrec[base + lane];
-                            s_alf[wbase + lane] = valf[base + lane];
+                            const float4 b = vrec[base + lane];
+                            const float4 al = valf[base + lane];
+                            stage_pair(pk, lane >> 1, lane & 1, -b.x, -b.y, -b.z, al.x, al.y, al.z);
+                        } else if ((uint32_t)lane == cnt && (cnt & 1u)) {
+                            stage_pair(pk, lane >> 1, 1, 1e18f, 1e18f, 1e18f, 0.f, 0.f, 0.f);
                         }
                         __syncwarp();
                         if (ok) {
-                            float pw = 0.f, px = 0.f, py = 0.f, pz = 0.f;
-                            for (uint32_t j = 0; j < cnt; j++) {
-                                const float4 b = s_rec[wbase + j];
-                                const float4 al = s_alf[wbase + j];
-                                const float dx = b.x - ra.x, dy = b.y - ra.y, dz = b.z - ra.z;
-                                const float dsq = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                                const float w = exp2f(dsq * wscale);
-                                pw += w;
-                                px = fmaf(w, al.x, px);
-                                py = fmaf(w, al.y, py);
-                                pz = fmaf(w, al.z, pz);
+                            float2 pw = make_float2(0.f, 0.f), px = pw, py = pw, pz = pw;
+                            const uint32_t np = (cnt + 1) >> 1;
+                            for (uint32_t p = 0; p < np; p++) {
+                                const float4 A = s_pk[wpk + p], B = s_pk[wpk + kSlots + p];
+                                const float4 Cc = s_pk[wpk + 2 * kSlots + p];
+                                const float2 dx = __fadd2_rn(tx, make_float2(A.x, A.y));
+                                const float2 dy = __fadd2_rn(ty, make_float2(A.z, A.w));
+                                const float2 dz = __fadd2_rn(tz, make_float2(B.x, B.y));
+                                const float2 dsq = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+                                const float2 arg = __fmul2_rn(dsq, ws2);
+                                const float2 w = make_float2(ex2_approx(arg.x), ex2_approx(arg.y));
+                                pw = __fadd2_rn(pw, w);
+                                px = __ffma2_rn(w, make_float2(B.z, B.w), px);
+                                py = __ffma2_rn(w, make_float2(Cc.x, Cc.y), py);
+                                pz = __ffma2_rn(w, make_float2(Cc.z, Cc.w), pz);
                             }
-                            tw += (double)pw;
-                            wx += (double)px;
-                            wy += (double)py;
-                            wz += (double)pz;
+                            tw += (double)pw.x + (double)pw.y;
+                            wx += (double)px.x + (double)px.y;
+                            wy += (double)py.x + (double)py.y;
+                            wz += (double)pz.x + (double)pz.y;
                         }
                         __syncwarp();
                     }
