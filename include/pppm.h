@@ -330,12 +330,53 @@ typedef struct pppm_mg pppm_mg;
 pppm_status pppm_mg_create(uint32_t n, void *stream, pppm_mg **out);
 pppm_status pppm_mg_destroy(pppm_mg *mg);
 /* m_FullMultiGrid(x, b, tol, residual) on FP64 device arrays of n^3: solves
- * sum_nbr(x) - 6x = b with zero ghost values.  mode = PPPM_MG_REFERENCE runs
- * the reference schedule (tol ignored, as in the reference); CONVERGED adds
- * defect-correction cycles until the relative residual meets tol.
- * *relres (may be NULL) receives ||b - A x|| / ||b||. */
+ * sum_nbr(x) - 6x = b with zero ghost values, starting from the x given (the
+ * reference's first residual is b - A x): x <- x + FMG(0, b - A x).
+ * mode = PPPM_MG_REFERENCE runs the reference schedule (tol ignored, as in the
+ * reference); CONVERGED adds defect-correction cycles until the residual is
+ * below tol relative to ||b - A x_initial||, which *relres (may be NULL)
+ * receives. */
 pppm_status pppm_mg_full_multigrid(pppm_mg *mg, double *x_dev, const double *b_dev,
                                    int mode, double tol, int max_cycles, double *relres);
+
+/* ---- scalar PPPM: PotentialFieldSolver (HFS/PotentialFieldSolver.h:10-91,
+ * HFS/PotentialFieldSolver.cpp:45-739) ------------------------------------
+ * Masses on a 2 x bounding-box grid of edge n, the monopole as Dirichlet
+ * data, three full-multigrid calls, and evaluation of the single-layer
+ * potential or its gradient with a near-field particle correction over K
+ * cells.  Grids and sums are FP64 as in the reference. */
+typedef struct pppm_potential pppm_potential;
+/* initializeSolver(n, n, n, K, M, N). */
+pppm_status pppm_potential_create(uint32_t n, int K, uint32_t cap_mass, uint32_t cap_eval, void *stream,
+                                  pppm_potential **out);
+pppm_status pppm_potential_destroy(pppm_potential *p);
+/* setMassParameter (:344-392): N float4 positions and N double masses (device). */
+pppm_status pppm_potential_set_masses(pppm_potential *p, uint32_t N, const float *pos4_dev,
+                                      const double *mass_dev);
+/* computeFarFieldBuffer (scalar = 0, :695-707) or
+ * computeFarFieldPotentialBuffer (scalar = 1, :726-737).  One stream
+ * synchronisation (the grid spacing comes from the bounding box). */
+pppm_status pppm_potential_build(pppm_potential *p, int scalar);
+/* evaluateGradient (:441-526): gradient at M points (device), caller order;
+ * zero at points outside the grid box.  Needs the gradient buffer. */
+pppm_status pppm_potential_eval_gradient(pppm_potential *p, uint32_t M, const float *eval4_dev,
+                                         double *gx_dev, double *gy_dev, double *gz_dev);
+/* evaluateScalarPotential (:708-739): potential at M points.  Needs the
+ * scalar buffer. */
+pppm_status pppm_potential_eval_scalar(pppm_potential *p, uint32_t M, const float *eval4_dev, double *phi_dev);
+/* computeDphiDn (:621-626, HFS/GPU_kernel.cu:1719-1740):
+ * out = -0.5 mass / area + n . grad per panel. */
+pppm_status pppm_potential_dphidn(pppm_potential *p, uint32_t M, const double *nx_dev, const double *ny_dev,
+                                  const double *nz_dev, const double *gx_dev, const double *gy_dev,
+                                  const double *gz_dev, const double *mass_dev, const double *area_dev,
+                                  double *out_dev);
+/* Inspection: origin and edge L of the last build, device pointers to the
+ * density, right-hand side (with the Dirichlet data), potential and
+ * far-field buffer ([3][n^3] gradient or [n^3] scalar), and the monopole
+ * (centre x, y, z, total mass) copied to the host. */
+pppm_status pppm_potential_grids(pppm_potential *p, double origin_length[4], const double **density_dev,
+                                 const double **rhs_dev, const double **phi_dev, const double **far_dev,
+                                 double monopole_host[4]);
 
 /* ---- spatial hash surface: ParticleManager (PH/SpaceHashClass.h:10-84) and
  * the extern "C" calcHash / sortParticles / FindCellStart / reorder / deorder

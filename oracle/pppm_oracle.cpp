@@ -390,6 +390,17 @@ extern "C" void orc_mg_vcycle(double *x, const double *b, uint32_t n, int coarse
 
 /* HFS/BiotSavartSolverImp.cpp:603-620: psi = 0, then m_FullMultiGrid.  In
  * mode 1 further V-cycles run until the relative residual meets tol. */
+/* MultiGridSolver3DPeriod_double::m_FullMultiGrid called `repeats` times
+ * from the x given (MG/MultiGrid.cpp:202-250: its first residual is b - A x). */
+extern "C" void orc_mg_fmg(double *x, const double *b, uint32_t n, int repeats, int coarse_mode) {
+    MG mg((int)n, coarse_mode);
+    const size_t C = (size_t)n * n * n;
+    std::memcpy(mg.lv[0].x.data(), x, sizeof(double) * C);
+    std::memcpy(mg.lv[0].b.data(), b, sizeof(double) * C);
+    for (int r = 0; r < repeats; r++) mg.fmg();
+    std::memcpy(x, mg.lv[0].x.data(), sizeof(double) * C);
+}
+
 extern "C" void orc_mg_solve(double *x, const double *b, uint32_t n, int mg_mode,
                              int coarse_mode, double tol, int max_cycles,
                              int32_t *cycles_out, double *relres_out) {
@@ -1086,4 +1097,305 @@ extern "C" uint32_t orc_baroclinic(uint32_t H, const float *heat4, const float *
     if (rho_out && C <= cap) std::memcpy(rho_out, rho.data(), sizeof(float) * C);
     if (grad_out && C <= cap) std::memcpy(grad_out, grad.data(), sizeof(float) * 3 * C);
     return dim;
+}
+
+/* ------------------------------------------------------------------------
+ * Scalar PPPM: PotentialFieldSolver (HFS/PotentialFieldSolver.cpp:45-739),
+ * kernels HFS/GPU_kernel.cu:524-1748 and 2977-3115.
+ * ------------------------------------------------------------------------ */
+namespace {
+
+/* HFS/GPU_kernel.cu:204-211 compute_r: 4 pi |r1 - r2|, or 1e12 when coincident. */
+double compute_r_dev(double ax, double ay, double az, double bx, double by, double bz) {
+    const double r_sqr = (ax - bx) * (ax - bx) + (ay - by) * (ay - by) + (az - bz) * (az - bz);
+    return r_sqr > 1e-12 ? kFourPi * std::sqrt(r_sqr) : 1e+12;
+}
+
+/* HFS/GPU_kernel.cu:546-601 compute_gradient_kernel: periodic central
+ * differences, direction * (right - left) * 0.5 * invh per axis. */
+void periodic_gradient(const double *phi, double *g3, int d, double invh, double direction) {
+    const size_t C = (size_t)d * d * d;
+    for (int k = 0; k < d; k++)
+        for (int j = 0; j < d; j++)
+            for (int i = 0; i < d; i++) {
+                const size_t c = gidx(i, j, k, d);
+                const double t = phi[gidx(i, (j + 1) % d, k, d)], dn = phi[gidx(i, (j + d - 1) % d, k, d)];
+                const double l = phi[gidx((i + d - 1) % d, j, k, d)], r = phi[gidx((i + 1) % d, j, k, d)];
+                const double f = phi[gidx(i, j, (k + d - 1) % d, d)], b = phi[gidx(i, j, (k + 1) % d, d)];
+                g3[c] = direction * (r - l) * 0.5 * invh;
+                g3[C + c] = direction * (t - dn) * 0.5 * invh;
+                g3[2 * C + c] = direction * (b - f) * 0.5 * invh;
+            }
+}
+
+/* Trilinear hat weights over the 5^3 cells around the point's cell
+ * (HFS/GPU_kernel.cu:1520-1676); no write when the point's cell is outside
+ * the grid (the caller's value stays 0). */
+template <typename Get>
+bool interp5(float px, float py, float pz, double invh, int d, Get get) {
+    const int i = (int)std::floor((double)px * invh), j = (int)std::floor((double)py * invh),
+              k = (int)std::floor((double)pz * invh);
+    if (!(i >= 0 && i < d && j >= 0 && j < d && k >= 0 && k < d)) return false;
+    for (int kk = k - 2; kk <= k + 2; kk++)
+        for (int jj = j - 2; jj <= j + 2; jj++)
+            for (int ii = i - 2; ii <= i + 2; ii++) {
+                if (!(kk >= 0 && kk < d && jj >= 0 && jj < d && ii >= 0 && ii < d)) continue;
+                const double gx = (double)(float)((double)ii + 0.5), gy = (double)(float)((double)jj + 0.5),
+                             gz = (double)(float)((double)kk + 0.5);
+                auto hat = [](double r) { const double rr = std::fabs(r); return rr < 1 ? 1 - rr : 0.0; };
+                const double w = hat(gx - (double)px * invh) * hat(gy - (double)py * invh) * hat(gz - (double)pz * invh);
+                get(gidx(ii, jj, kk, d), w);
+            }
+    return true;
+}
+
+}  // namespace
+
+/* PotentialFieldSolver::setDomain (:343-373): 2 x the bounding box. */
+extern "C" void orc_potential_domain(const float *pos4, uint32_t N, double *origin3, double *length) {
+    const F4 *pos = as_f4(pos4);
+    double maxx, minx, maxy, miny, maxz, minz;
+    maxx = minx = pos[0].x;
+    maxy = miny = pos[0].y;
+    maxz = minz = pos[0].z;
+    for (uint32_t i = 1; i < N; i++) {
+        if (pos[i].x < minx) minx = pos[i].x; else if (pos[i].x > maxx) maxx = pos[i].x;
+        if (pos[i].y < miny) miny = pos[i].y; else if (pos[i].y > maxy) maxy = pos[i].y;
+        if (pos[i].z < minz) minz = pos[i].z; else if (pos[i].z > maxz) maxz = pos[i].z;
+    }
+    const double dl = 2.0 * std::max(std::max(maxx - minx, maxy - miny), maxz - minz);
+    origin3[0] = (minx + 0.5 * (maxx - minx)) - 0.5 * dl;
+    origin3[1] = (miny + 0.5 * (maxy - miny)) - 0.5 * dl;
+    origin3[2] = (minz + 0.5 * (maxz - minz)) - 0.5 * dl;
+    *length = dl;
+}
+
+/* computeFarFieldBuffer (:695-707) + evaluateGradient (:441-526), or with
+ * scalar != 0 computeFarFieldPotentialBuffer (:726-737) +
+ * evaluateScalarPotential (:708-739).  Masses at pos4 (N), evaluation points
+ * eval4 (M); out receives the gradient (3 x M, caller order) or the potential
+ * (M).  dump (optional) receives origin[3], L, density[C], rhs[C] (after the
+ * Dirichlet data), phi[C] (after the three full-multigrid calls), and for
+ * the gradient far[3C]. */
+extern "C" int orc_potential(uint32_t n, int K, int scalar, uint32_t N, const float *pos4, const double *mass,
+                             uint32_t M, const float *eval4, double *out, double *dump_origin, double *dump_density,
+                             double *dump_rhs, double *dump_phi, double *dump_far, double *dump_monopole) {
+    if (N == 0 || n < 2) return 1;
+    const int d = (int)n;
+    const size_t C = (size_t)d * d * d;
+    double origin[3], L;
+    orc_potential_domain(pos4, N, origin, &L);
+    // m_ParticleToMesh (:527-609): hash, reorder, P2M, RHS, monopole, Dirichlet data
+    const float h_f = (float)(L / (double)n);
+    const float of[3] = {(float)origin[0], (float)origin[1], (float)origin[2]};
+    const double cell_h = (double)h_f;
+    std::vector<uint32_t> key(N), idx(N), start(C), end(C);
+    orc_calc_hash(pos4, N, n, h_f, of, key.data(), idx.data());
+    orc_sort_by_key(key.data(), idx.data(), N);
+    orc_find_cell_start(key.data(), N, (uint32_t)C, start.data(), end.data());
+    const F4 *pos = as_f4(pos4);
+    std::vector<F4> spos(N);
+    std::vector<double> smass(N);
+    for (uint32_t s = 0; s < N; s++) { spos[s] = pos[idx[s]]; smass[s] = mass[idx[s]]; }
+    std::vector<double> density(C), rhs(C);
+    orc_p2m(start.data(), end.data(), reinterpret_cast<const float *>(spos.data()), smass.data(), cell_h, n, N,
+            origin, density.data());
+    const double h2 = (double)(h_f * h_f);
+    for (size_t c = 0; c < C; c++) rhs[c] = density[c] * h2 * -1.0;
+    double total_weight = 0, total_mass = 0;
+    for (uint32_t s = 0; s < N; s++) { total_weight += std::fabs(smass[s]); total_mass += smass[s]; }
+    double cx = 0, cy = 0, cz = 0;
+    for (uint32_t s = 0; s < N; s++) {
+        cx += spos[s].x * std::fabs(smass[s]);
+        cy += spos[s].y * std::fabs(smass[s]);
+        cz += spos[s].z * std::fabs(smass[s]);
+    }
+    cx = cx / total_weight; cy = cy / total_weight; cz = cz / total_weight;
+    // applyDirichlet (HFS/GPU_kernel.cu:2977-3115): ghost values of the
+    // monopole moved to the right-hand side of the boundary cells
+    for (int k = 0; k < d; k++)
+        for (int j = 0; j < d; j++)
+            for (int i = 0; i < d; i++) {
+                const size_t c = gidx(i, j, k, d);
+                auto ghost = [&](double gi, double gj, double gk) {
+                    const double wx = gi * cell_h + origin[0], wy = gj * cell_h + origin[1], wz = gk * cell_h + origin[2];
+                    rhs[c] -= total_mass / compute_r_dev(wx, wy, wz, cx, cy, cz);
+                };
+                if (i == 0) ghost((double)i - 1.0 + 0.5, (double)j + 0.5, (double)k + 0.5);
+                if (i == d - 1) ghost((double)i + 1.0 + 0.5, (double)j + 0.5, (double)k + 0.5);
+                if (j == 0) ghost((double)i + 0.5, (double)j - 1.0 + 0.5, (double)k + 0.5);
+                if (j == d - 1) ghost((double)i + 0.5, (double)j + 1.0 + 0.5, (double)k + 0.5);
+                if (k == 0) ghost((double)i + 0.5, (double)j + 0.5, (double)k - 1.0 + 0.5);
+                if (k == d - 1) ghost((double)i + 0.5, (double)j + 0.5, (double)k + 1.0 + 0.5);
+            }
+    // m_SolvePoisson (:610-621): phi = 0, three full-multigrid calls
+    std::vector<double> phi(C, 0.0);
+    {
+        MG mg(d, 1);
+        std::memcpy(mg.lv[0].b.data(), rhs.data(), sizeof(double) * C);
+        for (int it = 0; it < 3; it++) mg.fmg();
+        std::memcpy(phi.data(), mg.lv[0].x.data(), sizeof(double) * C);
+    }
+    if (dump_origin) { dump_origin[0] = origin[0]; dump_origin[1] = origin[1]; dump_origin[2] = origin[2]; dump_origin[3] = L; }
+    if (dump_density) std::memcpy(dump_density, density.data(), sizeof(double) * C);
+    if (dump_rhs) std::memcpy(dump_rhs, rhs.data(), sizeof(double) * C);
+    if (dump_phi) std::memcpy(dump_phi, phi.data(), sizeof(double) * C);
+    if (dump_monopole) { dump_monopole[0] = cx; dump_monopole[1] = cy; dump_monopole[2] = cz; dump_monopole[3] = total_mass; }
+    const double invh = 1.0 / cell_h;
+    const F4 *ev = as_f4(eval4);
+    const double G = 1.0;
+    if (!scalar) {
+        // m_ComputeGradient + PotentialComputeFarField (HFS/GPU_kernel.cu:988-1197)
+        std::vector<double> grad(3 * C), far(3 * C);
+        periodic_gradient(phi.data(), grad.data(), d, invh, 1.0);
+        const size_t W3 = K >= 0 ? (size_t)(2 * K + 1) * (2 * K + 1) * (2 * K + 1) : 1;
+        std::vector<double> table(3 * W3);
+        if (K >= 0) orc_farfield_table(K, cell_h, table.data());
+        const int W = 2 * K + 1;
+        for (int k = 0; k < d; k++)
+            for (int j = 0; j < d; j++)
+                for (int i = 0; i < d; i++) {
+                    const size_t c = gidx(i, j, k, d);
+                    double fm[3] = {0, 0, 0};
+                    if (K >= 0)
+                        for (int kk = k - K; kk <= k + K; kk++)
+                            for (int jj = j - K; jj <= j + K; jj++)
+                                for (int ii = i - K; ii <= i + K; ii++) {
+                                    double m = 0, dx[3] = {0, 0, 0};
+                                    if (kk >= 0 && kk < d && jj >= 0 && jj < d && ii >= 0 && ii < d) {
+                                        m = G * density[gidx(ii, jj, kk, d)] * (cell_h * cell_h * cell_h);
+                                        if (!(kk == k && jj == j && ii == i)) {
+                                            const double *t = &table[3 * ((size_t)((kk - k + K) * W + (jj - j + K)) * W + (ii - i + K))];
+                                            dx[0] = t[0]; dx[1] = t[1]; dx[2] = t[2];
+                                        }
+                                    }
+                                    for (int q = 0; q < 3; q++) fm[q] += dx[q] * m;
+                                }
+                    for (int q = 0; q < 3; q++) far[q * C + c] = grad[q * C + c] - fm[q];
+                }
+        if (K >= 0) {
+            std::vector<double> phid(C), gd(3 * C);
+            for (size_t c = 0; c < C; c++) phid[c] = 0.250580605913965 * density[c] * (cell_h * cell_h) * G;
+            periodic_gradient(phid.data(), gd.data(), d, invh, 1.0);
+            for (size_t q = 0; q < 3 * C; q++) far[q] -= gd[q];
+        } else {
+            far = grad;
+        }
+        if (dump_far) std::memcpy(dump_far, far.data(), sizeof(double) * 3 * C);
+        // evaluateGradient: interpolation + Potential_PPCorrMN (a = 0.05) + outside points
+        const double cr = ((double)K + 0.5) / invh;
+        const float bbmin[3] = {of[0], of[1], of[2]};
+        const float bbmax[3] = {(float)(of[0] + L), (float)(of[1] + L), (float)(of[2] + L)};
+#pragma omp parallel for schedule(dynamic, 64)
+        for (int64_t t = 0; t < (int64_t)M; t++) {
+            const float px = (float)((double)ev[t].x - origin[0]), py = (float)((double)ev[t].y - origin[1]),
+                        pz = (float)((double)ev[t].z - origin[2]);
+            double g[3] = {0, 0, 0};
+            interp5(px, py, pz, invh, d, [&](size_t c, double w) {
+                g[0] += far[c] * w; g[1] += far[C + c] * w; g[2] += far[2 * C + c] * w;
+            });
+            if (K >= 0) {
+                const int i = (int)std::floor((double)px * invh), j = (int)std::floor((double)py * invh),
+                          k = (int)std::floor((double)pz * invh);
+                const double a = 0.05;
+                double f[3] = {0, 0, 0};
+                for (int kk = k - K - 1; kk <= k + K + 1; kk++)
+                    for (int jj = j - K - 1; jj <= j + K + 1; jj++)
+                        for (int ii = i - K - 1; ii <= i + K + 1; ii++) {
+                            if (!(kk >= 0 && kk < d && jj >= 0 && jj < d && ii >= 0 && ii < d)) continue;
+                            const size_t c = gidx(ii, jj, kk, d);
+                            if (start[c] == 0xFFFFFFFFu) continue;
+                            for (uint32_t p = start[c]; p < end[c]; p++) {
+                                const float qx = (float)((double)spos[p].x - origin[0]);
+                                const float qy = (float)((double)spos[p].y - origin[1]);
+                                const float qz = (float)((double)spos[p].z - origin[2]);
+                                if (!(std::fabs((double)(float)(qx - px)) < cr && std::fabs((double)(float)(qy - py)) < cr &&
+                                      std::fabs((double)(float)(qz - pz)) < cr))
+                                    continue;
+                                const double dx = (float)(qx - px), dy = (float)(qy - py), dz = (float)(qz - pz);
+                                const double r1 = std::sqrt(dx * dx + dy * dy + dz * dz);
+                                double r3;
+                                if (r1 > a) r3 = kFourPi * r1 * r1 * r1;
+                                else r3 = (r1 < 1e-12) ? 1e+14 : kFourPi * a * a * a;
+                                f[0] += G * dx / r3 * smass[p];
+                                f[1] += G * dy / r3 * smass[p];
+                                f[2] += G * dz / r3 * smass[p];
+                            }
+                        }
+                for (int q = 0; q < 3; q++) g[q] += f[q];
+            }
+            // Potentialparticle_outside_kernel (HFS/GPU_kernel.cu:1678-1716): zero outside the grid box
+            const double ex = ev[t].x, ey = ev[t].y, ez = ev[t].z;
+            if (ex < bbmin[0] || ex > bbmax[0] || ey < bbmin[1] || ey > bbmax[1] || ez < bbmin[2] || ez > bbmax[2])
+                g[0] = g[1] = g[2] = 0;
+            out[t] = g[0]; out[M + t] = g[1]; out[2 * (size_t)M + t] = g[2];
+        }
+    } else {
+        // PotentialComputeScalarFarField (HFS/GPU_kernel.cu:1200-1298)
+        std::vector<double> sphi(phi);
+        if (K >= 0)
+            for (int k = 0; k < d; k++)
+                for (int j = 0; j < d; j++)
+                    for (int i = 0; i < d; i++) {
+                        double s = 0;
+                        for (int kk = k - K; kk <= k + K; kk++)
+                            for (int jj = j - K; jj <= j + K; jj++)
+                                for (int ii = i - K; ii <= i + K; ii++) {
+                                    if (!(kk >= 0 && kk < d && jj >= 0 && jj < d && ii >= 0 && ii < d)) continue;
+                                    const double m = G * density[gidx(ii, jj, kk, d)] * (cell_h * cell_h);
+                                    double w;
+                                    if (i == ii && j == jj && k == kk) w = 0.25;
+                                    else {
+                                        const double x = (double)ii - (double)i, y = (double)jj - (double)j,
+                                                     z = (double)kk - (double)k;
+                                        w = 1.0 / (kFourPi * std::sqrt(x * x + y * y + z * z));
+                                    }
+                                    s += w * m;
+                                }
+                        sphi[gidx(i, j, k, d)] = phi[gidx(i, j, k, d)] - s;
+                    }
+        if (dump_far) std::memcpy(dump_far, sphi.data(), sizeof(double) * C);
+        const double cr = ((double)K + 0.5) / invh;
+#pragma omp parallel for schedule(dynamic, 64)
+        for (int64_t t = 0; t < (int64_t)M; t++) {
+            const float px = (float)((double)ev[t].x - origin[0]), py = (float)((double)ev[t].y - origin[1]),
+                        pz = (float)((double)ev[t].z - origin[2]);
+            double v = 0;
+            interp5(px, py, pz, invh, d, [&](size_t c, double w) { v += sphi[c] * w; });
+            if (K >= 0) {
+                const int i = (int)std::floor((double)px * invh), j = (int)std::floor((double)py * invh),
+                          k = (int)std::floor((double)pz * invh);
+                const double qx0 = (double)px * invh, qy0 = (double)py * invh, qz0 = (double)pz * invh;
+                const int ilo = qx0 > i + 0.5 ? i - K : i - K - 1, ihi = qx0 > i + 0.5 ? i + K + 1 : i + K;
+                const int jlo = qy0 > j + 0.5 ? j - K : j - K - 1, jhi = qy0 > j + 0.5 ? j + K + 1 : j + K;
+                const int klo = qz0 > k + 0.5 ? k - K : k - K - 1, khi = qz0 > k + 0.5 ? k + K + 1 : k + K;
+                const double a = 0.125;
+                double s = 0;
+                for (int kk = klo; kk <= khi; kk++)
+                    for (int jj = jlo; jj <= jhi; jj++)
+                        for (int ii = ilo; ii <= ihi; ii++) {
+                            if (!(kk >= 0 && kk < d && jj >= 0 && jj < d && ii >= 0 && ii < d)) continue;
+                            const size_t c = gidx(ii, jj, kk, d);
+                            if (start[c] == 0xFFFFFFFFu) continue;
+                            for (uint32_t p = start[c]; p < end[c]; p++) {
+                                const float qx = (float)((double)spos[p].x - origin[0]);
+                                const float qy = (float)((double)spos[p].y - origin[1]);
+                                const float qz = (float)((double)spos[p].z - origin[2]);
+                                if (!(std::fabs((double)(float)(qx - px)) < cr && std::fabs((double)(float)(qy - py)) < cr &&
+                                      std::fabs((double)(float)(qz - pz)) < cr))
+                                    continue;
+                                const double dx = (float)(qx - px), dy = (float)(qy - py), dz = (float)(qz - pz);
+                                const double r1 = std::sqrt(dx * dx + dy * dy + dz * dz);
+                                double r2;
+                                if (r1 > a) r2 = kFourPi * r1;
+                                else r2 = (r1 < 1e-12) ? 1e+14 : kFourPi * a;
+                                s += G / r2 * smass[p];
+                            }
+                        }
+                v += s;
+            }
+            out[t] = v;
+        }
+    }
+    return 0;
 }

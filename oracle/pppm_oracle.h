@@ -86,6 +86,7 @@ void orc_mg_solve(double *x, const double *b, uint32_t n, int mg_mode,
                   int coarse_mode, double tol, int max_cycles,
                   int32_t *cycles_out, double *relres_out);
 void orc_mg_vcycle(double *x, const double *b, uint32_t n, int coarse_mode);
+void orc_mg_fmg(double *x, const double *b, uint32_t n, int repeats, int coarse_mode);
 double orc_residual_norm(const double *x, const double *b, uint32_t n);
 void orc_apply_laplacian(const double *x, double *y, uint32_t n);
 void orc_curl(const double *psi3, double *u3, uint32_t n, double h);
@@ -137,6 +138,12 @@ void orc_direct_sum(uint32_t N, const float *vort_pos4, const double *ax,
                     const double *ay, const double *az, uint32_t M,
                     const float *eval_a4, const float *eval_b4, int is_segment,
                     double a, double *u, double *v, double *w);
+
+/* --- scalar PPPM: PotentialFieldSolver (HFS/PotentialFieldSolver.cpp) --- */
+void orc_potential_domain(const float *pos4, uint32_t N, double *origin3, double *length);
+int orc_potential(uint32_t n, int K, int scalar, uint32_t N, const float *pos4, const double *mass, uint32_t M,
+                  const float *eval4, double *out, double *dump_origin4, double *dump_density, double *dump_rhs,
+                  double *dump_phi, double *dump_far, double *dump_monopole4);
 
 int orc_num_threads(void);
 

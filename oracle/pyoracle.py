@@ -93,6 +93,11 @@ def lib():
         L.orc_baroclinic.argtypes = [C.c_uint32, f32p, f32p, C.c_uint32, f32p, f64p, f64p, f64p, C.c_double,
                                      f64p, f64p, C.c_void_p, C.c_void_p, C.c_size_t]
         L.orc_baroclinic.restype = C.c_uint32
+        L.orc_potential.argtypes = [C.c_uint32, C.c_int, C.c_int, C.c_uint32, f32p, f64p, C.c_uint32, f32p, f64p,
+                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_potential.restype = C.c_int
+        L.orc_mg_fmg.argtypes = [f64p, f64p, C.c_uint32, C.c_int, C.c_int]
+        L.orc_mg_fmg.restype = None
         L.orc_density_domain.argtypes = [f32p, C.c_uint32, f64p, f64p]
         L.orc_density_domain.restype = None
         _lib = L
@@ -291,6 +296,35 @@ def gaussian_smooth(prm: OrcParams, cent4, d3, nu=0.1):
     out = [np.zeros(N) for _ in range(3)]
     lib().orc_gaussian_smooth(C.byref(prm), N, cent, dx, dy, dz, float(nu), *out)
     return np.stack(out, axis=1)
+
+
+def mg_fmg(x0, b, n, repeats=1, coarse_mode=1):
+    """m_FullMultiGrid called `repeats` times from x0."""
+    x = np.array(x0, dtype=np.float64, copy=True)
+    lib().orc_mg_fmg(x, np.ascontiguousarray(b, dtype=np.float64), n, repeats, coarse_mode)
+    return x
+
+
+def potential(n, K, pos4, mass, eval4, scalar=False, dump=False):
+    """PotentialFieldSolver: gradient (M, 3) or scalar potential (M,) at eval4;
+    with dump, also a dict of the intermediate grids."""
+    pos = np.ascontiguousarray(pos4, dtype=np.float32)
+    m = np.ascontiguousarray(mass, dtype=np.float64)
+    ev = np.ascontiguousarray(eval4, dtype=np.float32)
+    M = len(ev)
+    C3 = n ** 3
+    out = np.zeros(M if scalar else 3 * M)
+    d = {}
+    if dump:
+        d = {"origin": np.zeros(4), "density": np.zeros(C3), "rhs": np.zeros(C3), "phi": np.zeros(C3),
+             "far": np.zeros(C3 if scalar else 3 * C3), "monopole": np.zeros(4)}
+    ptr = (lambda k: d[k].ctypes.data) if dump else (lambda k: None)
+    rc = lib().orc_potential(n, K, int(scalar), len(pos), pos, m, M, ev, out, ptr("origin"), ptr("density"),
+                             ptr("rhs"), ptr("phi"), ptr("far"), ptr("monopole"))
+    if rc != 0:
+        raise RuntimeError("orc_potential failed")
+    res = out if scalar else out.reshape(3, M).T.copy()
+    return (res, d) if dump else res
 
 
 def num_threads():

@@ -568,8 +568,10 @@ class MultiGridSolver3DPeriod_double:
 
     def m_FullMultiGrid(self, x: torch.Tensor, b: torch.Tensor, tol: float = 1e-10,
                         mode: int = MG_REFERENCE, max_cycles: int = 50) -> float:
-        """Solves sum_nbr(x) - 6x = b (zero ghosts) into x; returns the
-        relative residual (-1 in reference mode, which does not measure it)."""
+        """Solves sum_nbr(x) - 6x = b (zero ghosts) into x, starting from the x
+        given (x <- x + FMG(0, b - A x), as the reference's first residual is
+        b - A x); returns the relative residual (-1 in reference mode, which
+        does not measure it)."""
         if x.dtype != torch.float64 or b.dtype != torch.float64 or not x.is_cuda:
             raise ValueError("x and b must be CUDA float64 tensors")
         rr = C.c_double()

@@ -31,7 +31,9 @@ EXPORTED = (
     "pppm_server_wait", "pppm_server_read_positions", "pppm_server_stats",
     "pppm_frame_path", "pppm_write_frame", "pppm_read_frame", "pppm_vortex_step",
     "pppm_baroclinic", "pppm_get_density", "pppm_write_sgi", "pppm_renderer_create", "pppm_renderer_destroy",
-    "pppm_render_shadows", "pppm_render_shadow_map", "pppm_render_smoke",
+    "pppm_render_shadows", "pppm_render_shadow_map", "pppm_render_smoke", "pppm_potential_create",
+    "pppm_potential_destroy", "pppm_potential_set_masses", "pppm_potential_build", "pppm_potential_eval_gradient",
+    "pppm_potential_eval_scalar", "pppm_potential_dphidn", "pppm_potential_grids",
 )
 REQ_EVAL, REQ_ADVANCE = 0, 1
 NOALLOC_MAX_PARTICLES = 1048576  # PPPM_NOALLOC_MAX_PARTICLES in include/pppm.h
@@ -137,6 +139,15 @@ def load(build_if_missing: bool = True):
                                   vp, vp, vp]),
         "pppm_baroclinic": (st, [vp, u32, vp, vp, u32, vp, vp, vp, vp, C.c_double]),
         "pppm_write_sgi": (st, [C.c_char_p, u32, u32, C.c_int, vp, C.c_int]),
+        "pppm_potential_create": (st, [u32, C.c_int, u32, u32, vp, C.POINTER(vp)]),
+        "pppm_potential_destroy": (st, [vp]),
+        "pppm_potential_set_masses": (st, [vp, u32, vp, vp]),
+        "pppm_potential_build": (st, [vp, C.c_int]),
+        "pppm_potential_eval_gradient": (st, [vp, u32, vp, vp, vp, vp]),
+        "pppm_potential_eval_scalar": (st, [vp, u32, vp, vp]),
+        "pppm_potential_dphidn": (st, [vp, u32, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
+        "pppm_potential_grids": (st, [vp, C.POINTER(C.c_double), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
+                                      C.POINTER(vp), C.POINTER(C.c_double)]),
         "pppm_renderer_create": (st, [vp, C.POINTER(vp)]),
         "pppm_renderer_destroy": (st, [vp]),
         "pppm_render_shadows": (st, [vp, u32, vp, vp, C.c_float, C.c_float, C.POINTER(C.c_float), C.c_float, vp,

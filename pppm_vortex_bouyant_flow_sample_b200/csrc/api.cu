@@ -705,6 +705,7 @@ extern "C" pppm_status pppm_get_stats(pppm_scene *s, uint64_t *pairs, int32_t *m
 struct pppm_mg {
     pppm::MGPlan plan;
     float *pool = nullptr;
+    double *r64 = nullptr, *e64 = nullptr;  // residual of the initial guess, its correction
     uint32_t n = 0;
 };
 
@@ -712,6 +713,28 @@ namespace {
 __global__ void to_float_kernel(const double *__restrict__ in, float *__restrict__ out, size_t count) {
     const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t < count) out[t] = (float)in[t];
+}
+
+// r = b - (sum_nbr(x) - 6x) with zero ghost values, FP64; the FP32 copy seeds
+// the finest multigrid level.
+__global__ void residual64_kernel(const double *__restrict__ x, const double *__restrict__ b, double *__restrict__ r,
+                                  float *__restrict__ r32, int d) {
+    const size_t C = (size_t)d * d * d;
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= C) return;
+    const int i = (int)(t % d), j = (int)((t / d) % d), k = (int)(t / ((size_t)d * d));
+    const size_t dd = (size_t)d * d;
+    const double lv = (i > 0) ? x[t - 1] : 0.0, rv = (i < d - 1) ? x[t + 1] : 0.0;
+    const double uv = (j < d - 1) ? x[t + d] : 0.0, dv = (j > 0) ? x[t - d] : 0.0;
+    const double fv = (k > 0) ? x[t - dd] : 0.0, bv = (k < d - 1) ? x[t + dd] : 0.0;
+    const double v = b[t] - ((((lv + rv) + (uv + dv)) + (fv + bv)) - 6.0 * x[t]);
+    r[t] = v;
+    r32[t] = (float)v;
+}
+
+__global__ void add64_kernel(double *__restrict__ x, const double *__restrict__ e, size_t count) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < count) x[t] += e[t];
 }
 }  // namespace
 
@@ -737,10 +760,14 @@ extern "C" pppm_status pppm_mg_create(uint32_t n, void *stream, pppm_mg **out) {
     }
     cudaError_t e = dalloc(&m->pool, pool);
     if (e == cudaSuccess) e = dalloc(&P.norms, 2);
+    if (e == cudaSuccess) e = dalloc(&m->r64, P.lv[0].cells);
+    if (e == cudaSuccess) e = dalloc(&m->e64, P.lv[0].cells);
     if (e != cudaSuccess) {
         pppm_status st = cuda_fail("pppm_mg_create", e);
         cudaFree(m->pool);
         cudaFree(P.norms);
+        cudaFree(m->r64);
+        cudaFree(m->e64);
         delete m;
         return st;
     }
@@ -759,6 +786,8 @@ extern "C" pppm_status pppm_mg_destroy(pppm_mg *m) {
     std::lock_guard<std::recursive_mutex> lk(pppm::device_lock());
     cudaFree(m->pool);
     cudaFree(m->plan.norms);
+    cudaFree(m->r64);
+    cudaFree(m->e64);
     delete m;
     return PPPM_OK;
 }
@@ -769,18 +798,27 @@ extern "C" pppm_status pppm_mg_full_multigrid(pppm_mg *m, double *x, const doubl
         snprintf(g_err, sizeof(g_err), "pppm_mg_full_multigrid: invalid argument");
         return PPPM_ERR_INVALID;
     }
+    // The reference's full multigrid starts from the x it is given (its first
+    // residual is b - A x, MG/MultiGrid.cpp:211-226): solve for the correction
+    // e of r = b - A x and add it, x + FMG(0, r), which is the same linear
+    // iteration (and exactly the plain solve when x = 0).
     pppm::MGPlan P = m->plan;
-    P.psi = x;
-    P.b64 = b;
+    P.psi = m->e64;
+    P.b64 = m->r64;
     P.vort = nullptr;
     P.P = nullptr;
     const size_t C = P.lv[0].cells;
     ::pppm::note_launch();
-    to_float_kernel<<<(unsigned)((C + 255) / 256), 256, 0, P.st>>>(b, P.lv[0].b, C);
+    residual64_kernel<<<(unsigned)((C + 255) / 256), 256, 0, P.st>>>(x, b, m->r64, P.lv[0].b, (int)P.lv[0].d);
     cudaError_t e = cudaGetLastError();
     int cyc = 0;
     double rel = -1.0;
     if (e == cudaSuccess) e = pppm::mg_solve(P, mode, tol, max_cycles > 0 ? max_cycles : 1, &cyc, &rel);
+    if (e == cudaSuccess) {
+        ::pppm::note_launch();
+        add64_kernel<<<(unsigned)((C + 255) / 256), 256, 0, P.st>>>(x, m->e64, C);
+        e = cudaGetLastError();
+    }
     if (e != cudaSuccess) return cuda_fail("pppm_mg_full_multigrid", e);
     if (relres) *relres = rel;
     return PPPM_OK;

@@ -211,7 +211,10 @@ __device__ __forceinline__ void cell_pairs_packed(const float4 *__restrict__ vre
                 ok0 = ok0 && !(e2.x < 1e-24f);
                 ok1 = ok1 && !(e2.y < 1e-24f);
             }
-            const float2 rs = make_float2(rsqrtf(fmaxf(r2.x, 1e-30f)), rsqrtf(fmaxf(r2.y, 1e-30f)));
+            // 1e-30 keeps rsqrt finite at r = 0 (that pair's term is zero anyway);
+            // it changes r2 only below 2e-23, i.e. r < 5e-12
+            const float2 r2g = __fadd2_rn(r2, make_float2(1e-30f, 1e-30f));
+            const float2 rs = make_float2(rsqrtf(r2g.x), rsqrtf(r2g.y));
             const float2 t = __fmul2_rn(__fmul2_rn(r2, __fmul2_rn(r2, rs)), inv_a3);
             float2 c = __ffma2_rn(cf[4], t, cf[3]);
             c = __ffma2_rn(c, t, cf[2]);
@@ -249,7 +252,7 @@ struct SmoothSeries {
 };
 
 template <bool SEG, bool COUNT>
-__global__ void eval_kernel(const SmoothSeries sc, const uint32_t *__restrict__ eidx, uint32_t M, const float4 *__restrict__ eval_a,
+__global__ void __launch_bounds__(kEvalThreads, 8) eval_kernel(const SmoothSeries sc, const uint32_t *__restrict__ eidx, uint32_t M, const float4 *__restrict__ eval_a,
             const float4 *__restrict__ eval_b, const float *__restrict__ far,
             const uint32_t *__restrict__ start, const uint32_t *__restrict__ end,
             const uint32_t *__restrict__ sub_start, const uint32_t *__restrict__ sub_end, const float4 *__restrict__ vrec,

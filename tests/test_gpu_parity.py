@@ -177,6 +177,13 @@ def test_mg_standalone_reference_and_converged(pb, oracle):
     assert 0 <= rr <= 1e-10
     xc, _, rc = oracle.mg_solve(b, n, mg_mode=1, tol=1e-12)
     assert rel_l2(x.cpu().numpy(), xc) <= 1e-9
+    # repeated calls continue from the x they are given (the scalar PPPM
+    # calls the full multigrid three times in a row)
+    x.zero_()
+    for _ in range(3):
+        mg.m_FullMultiGrid(x, _dev(b), mode=pb.MG_REFERENCE)
+    x3 = oracle.mg_fmg(np.zeros(n ** 3), b, n, repeats=3)
+    assert rel_l2(x.cpu().numpy(), x3) <= 1e-6
     mg.m_FinalMemoryEachLevel()
 
 
