@@ -361,6 +361,10 @@ pppm_status pppm_potential_build(pppm_potential *p, int scalar);
  * zero at points outside the grid box.  Needs the gradient buffer. */
 pppm_status pppm_potential_eval_gradient(pppm_potential *p, uint32_t M, const float *eval4_dev,
                                          double *gx_dev, double *gy_dev, double *gz_dev);
+/* The same with the gradient interleaved per point (x, y, z), the layout of
+ * the reference's GpuArrayd3 m_particle_gradPhi. */
+pppm_status pppm_potential_eval_gradient3(pppm_potential *p, uint32_t M, const float *eval4_dev,
+                                          double *grad3_dev);
 /* evaluateScalarPotential (:708-739): potential at M points.  Needs the
  * scalar buffer. */
 pppm_status pppm_potential_eval_scalar(pppm_potential *p, uint32_t M, const float *eval4_dev, double *phi_dev);

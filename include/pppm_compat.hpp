@@ -5,6 +5,7 @@
 //   BiotSavartSolver              hybridFastSummation/BiotSavartSolver.h:16-38
 //   ParticleManager               particle_hash/SpaceHashClass.h:10-84
 //   MultiGridSolver3DPeriod_double multigrid/MultiGrid.h:188-209
+//   PotentialFieldSolver          hybridFastSummation/PotentialFieldSolver.h:10-91
 //
 // The reference passes gf::gf_GpuArray<T> objects (multigrid/gfGpuArray.h:
 // 26-89); DeviceArray<T> below keeps the two members its call sites use,
@@ -238,6 +239,82 @@ private:
     float origin_[3] = {0.f, 0.f, 0.f};
 };
 
+struct double3_ { double x, y, z; };
+typedef DeviceArray<double3_> GpuArrayd3;
+
+// HFS/PotentialFieldSolver.h:10-91.  Output arrays are owned by the solver, as
+// m_particle_gradPhi / m_particle_dphidn are in the reference.
+class PotentialFieldSolver {
+public:
+    PotentialFieldSolver() = default;
+    ~PotentialFieldSolver() { shutdown(); }
+    PotentialFieldSolver(const PotentialFieldSolver &) = delete;
+    PotentialFieldSolver &operator=(const PotentialFieldSolver &) = delete;
+
+    // :45-255 (cubic grids only)
+    bool initializeSolver(uint gdx, uint gdy, uint gdz, uint K, uint M, uint N, void *stream = nullptr) {
+        if (gdx != gdy || gdy != gdz) return false;
+        shutdown();
+        if (pppm_potential_create(gdx, (int)K, N ? N : 1, M ? M : 1, stream, &p_) != PPPM_OK) return false;
+        n_ = gdx;
+        return true;
+    }
+    // :344-392
+    bool setMassParameter(uint n, GpuArrayf4 *pos, GpuArrayd *mass) {
+        mass_ = mass->getDevicePtr();
+        return pppm_potential_set_masses(p_, n, reinterpret_cast<const float *>(pos->getDevicePtr()),
+                                         mass->getDevicePtr()) == PPPM_OK;
+    }
+    // :302-343
+    bool setEvalParameter(uint m, GpuArrayf4 *pos) {
+        M_ = m;
+        eval_ = reinterpret_cast<const float *>(pos->getDevicePtr());
+        return ensure_out(m);
+    }
+    bool setEvalNormals(uint, GpuArrayd3 *normals) { normals_ = normals->getDevicePtr(); return true; }
+    bool setEvalAreas(uint, GpuArrayd *areas) { areas_ = areas->getDevicePtr(); return true; }
+    // :695-707
+    void computeFarFieldBuffer() { ok_ = pppm_potential_build(p_, 0) == PPPM_OK; }
+    // :726-737
+    void computeFarFieldPotentialBuffer() { ok_ = pppm_potential_build(p_, 1) == PPPM_OK; }
+    // :441-526 (large_eval only changes the reference's evaluation order)
+    bool evaluateGradient(bool /*large_eval*/) {
+        return pppm_potential_eval_gradient3(p_, M_, eval_, reinterpret_cast<double *>(grad_)) == PPPM_OK;
+    }
+    // :708-739
+    void evaluateScalarPotential() { ok_ = pppm_potential_eval_scalar(p_, M_, eval_, dphidn_) == PPPM_OK; }
+    // :621-626; normals and gradients as double3 records
+    bool computeDphiDn();
+    GpuArrayd3 *getGradPhi() { grad_arr_ = GpuArrayd3(grad_, M_); return &grad_arr_; }
+    GpuArrayd *getDpDn() { dp_arr_ = GpuArrayd(dphidn_, M_); return &dp_arr_; }
+    GpuArrayd *getScalarPhi() { return getDpDn(); }
+    double getCellh() {
+        double ol[4] = {0, 0, 0, 0};
+        pppm_potential_grids(p_, ol, nullptr, nullptr, nullptr, nullptr, nullptr);
+        return (double)(float)(ol[3] / (double)n_);
+    }
+    double4_ getOrigin() {
+        double ol[4] = {0, 0, 0, 0};
+        pppm_potential_grids(p_, ol, nullptr, nullptr, nullptr, nullptr, nullptr);
+        return double4_{ol[0], ol[1], ol[2], 0.0};
+    }
+    bool shutdown();
+    bool lastOk() const { return ok_; }
+
+private:
+    bool ensure_out(uint m);
+    pppm_potential *p_ = nullptr;
+    uint n_ = 0, M_ = 0, cap_ = 0;
+    const float *eval_ = nullptr;
+    const double *mass_ = nullptr, *areas_ = nullptr;
+    const double3_ *normals_ = nullptr;
+    double3_ *grad_ = nullptr;
+    double *dphidn_ = nullptr, *split_ = nullptr;  // split_: [6][cap] SoA scratch for computeDphiDn
+    GpuArrayd3 grad_arr_;
+    GpuArrayd dp_arr_;
+    bool ok_ = true;
+};
+
 }  // namespace pppm_compat
 
 // Out-of-line members that allocate: kept here so the header stays self
@@ -286,3 +363,48 @@ inline void BiotSavartSolver::free_buffers() {
 }
 
 }  // namespace pppm_compat
+
+inline bool pppm_compat::PotentialFieldSolver::ensure_out(uint m) {
+    if (m <= cap_) return true;
+    cudaFree(grad_);
+    cudaFree(dphidn_);
+    cudaFree(split_);
+    grad_ = nullptr;
+    dphidn_ = nullptr;
+    split_ = nullptr;
+    const size_t k = m ? m : 1;
+    if (cudaMalloc(&grad_, sizeof(double3_) * k) != cudaSuccess) return false;
+    if (cudaMalloc(&dphidn_, sizeof(double) * k) != cudaSuccess) return false;
+    if (cudaMalloc(&split_, sizeof(double) * 6 * k) != cudaSuccess) return false;
+    cap_ = m;
+    return true;
+}
+
+inline bool pppm_compat::PotentialFieldSolver::computeDphiDn() {
+    // de-interleave normals and gradients with strided 2-D copies, then the
+    // library's element-wise kernel
+    const size_t k = cap_ ? cap_ : 1;
+    double *dst[6] = {split_, split_ + k, split_ + 2 * k, split_ + 3 * k, split_ + 4 * k, split_ + 5 * k};
+    const double *n = reinterpret_cast<const double *>(normals_);
+    const double *g = reinterpret_cast<const double *>(grad_);
+    const double *src[6] = {n, n + 1, n + 2, g, g + 1, g + 2};
+    for (int c = 0; c < 6; c++)
+        if (cudaMemcpy2D(dst[c], sizeof(double), src[c], 3 * sizeof(double), sizeof(double), M_,
+                         cudaMemcpyDeviceToDevice) != cudaSuccess)
+            return false;
+    return pppm_potential_dphidn(p_, M_, dst[0], dst[1], dst[2], dst[3], dst[4], dst[5], mass_, areas_, dphidn_) ==
+           PPPM_OK;
+}
+
+inline bool pppm_compat::PotentialFieldSolver::shutdown() {
+    if (p_) pppm_potential_destroy(p_);
+    p_ = nullptr;
+    cudaFree(grad_);
+    cudaFree(dphidn_);
+    cudaFree(split_);
+    grad_ = nullptr;
+    dphidn_ = nullptr;
+    split_ = nullptr;
+    cap_ = 0;
+    return true;
+}

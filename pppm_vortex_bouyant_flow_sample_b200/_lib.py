@@ -33,7 +33,7 @@ EXPORTED = (
     "pppm_baroclinic", "pppm_get_density", "pppm_write_sgi", "pppm_renderer_create", "pppm_renderer_destroy",
     "pppm_render_shadows", "pppm_render_shadow_map", "pppm_render_smoke", "pppm_potential_create",
     "pppm_potential_destroy", "pppm_potential_set_masses", "pppm_potential_build", "pppm_potential_eval_gradient",
-    "pppm_potential_eval_scalar", "pppm_potential_dphidn", "pppm_potential_grids",
+    "pppm_potential_eval_scalar", "pppm_potential_dphidn", "pppm_potential_grids", "pppm_potential_eval_gradient3",
 )
 REQ_EVAL, REQ_ADVANCE = 0, 1
 NOALLOC_MAX_PARTICLES = 1048576  # PPPM_NOALLOC_MAX_PARTICLES in include/pppm.h
@@ -145,6 +145,7 @@ def load(build_if_missing: bool = True):
         "pppm_potential_build": (st, [vp, C.c_int]),
         "pppm_potential_eval_gradient": (st, [vp, u32, vp, vp, vp, vp]),
         "pppm_potential_eval_scalar": (st, [vp, u32, vp, vp]),
+        "pppm_potential_eval_gradient3": (st, [vp, u32, vp, vp]),
         "pppm_potential_dphidn": (st, [vp, u32, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
         "pppm_potential_grids": (st, [vp, C.POINTER(C.c_double), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
                                       C.POINTER(vp), C.POINTER(C.c_double)]),

@@ -354,7 +354,7 @@ __global__ void pot_eval_kernel(const uint32_t *__restrict__ eidx, uint32_t M, c
                                 const double *__restrict__ smass, int d, int K, double ox, double oy, double oz,
                                 double invh, float bbmin_x, float bbmin_y, float bbmin_z, float bbmax_x,
                                 float bbmax_y, float bbmax_z, double *__restrict__ ox_, double *__restrict__ oy_,
-                                double *__restrict__ oz_) {
+                                double *__restrict__ oz_, uint32_t ostride) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= M) return;
     const uint32_t q = eidx[s];
@@ -456,9 +456,9 @@ __global__ void pot_eval_kernel(const uint32_t *__restrict__ eidx, uint32_t M, c
         const double x = e.x, y = e.y, z = e.z;
         if (x < bbmin_x || x > bbmax_x || y < bbmin_y || y > bbmax_y || z < bbmin_z || z > bbmax_z)
             g[0] = g[1] = g[2] = 0.0;
-        ox_[q] = g[0];
-        oy_[q] = g[1];
-        oz_[q] = g[2];
+        ox_[(size_t)q * ostride] = g[0];
+        oy_[(size_t)q * ostride] = g[1];
+        oz_[(size_t)q * ostride] = g[2];
     } else {
         ox_[q] = g[0];
     }
@@ -691,7 +691,7 @@ extern "C" pppm_status pppm_potential_build(pppm_potential *P, int scalar) {
 }
 
 static pppm_status pot_eval(pppm_potential *P, uint32_t M, const float *eval4, double *a, double *b, double *c,
-                            bool grad) {
+                            bool grad, uint32_t ostride = 1) {
     using namespace pppm;
     if (!P || (M > 0 && (!eval4 || !a || (grad && (!b || !c))))) {
         pppm_set_error("pppm_potential_eval: invalid argument");
@@ -721,11 +721,12 @@ static pppm_status pot_eval(pppm_potential *P, uint32_t M, const float *eval4, d
         if (grad)
             pot_eval_kernel<true><<<(M + 127) / 128, 128, 0, st>>>(
                 sidx, M, ev, P->far, P->start, P->end, P->srec, P->smass, (int)n, P->K, P->origin[0], P->origin[1],
-                P->origin[2], invh, P->of[0], P->of[1], P->of[2], bbmax[0], bbmax[1], bbmax[2], a, b, c);
+                P->origin[2], invh, P->of[0], P->of[1], P->of[2], bbmax[0], bbmax[1], bbmax[2], a, b, c, ostride);
         else
             pot_eval_kernel<false><<<(M + 127) / 128, 128, 0, st>>>(
                 sidx, M, ev, P->far, P->start, P->end, P->srec, P->smass, (int)n, P->K, P->origin[0], P->origin[1],
-                P->origin[2], invh, P->of[0], P->of[1], P->of[2], bbmax[0], bbmax[1], bbmax[2], a, nullptr, nullptr);
+                P->origin[2], invh, P->of[0], P->of[1], P->of[2], bbmax[0], bbmax[1], bbmax[2], a, nullptr, nullptr,
+                1);
         e = cudaGetLastError();
     }
     if (e != cudaSuccess) return pot_fail("pppm_potential_eval", e);
@@ -735,6 +736,11 @@ static pppm_status pot_eval(pppm_potential *P, uint32_t M, const float *eval4, d
 extern "C" pppm_status pppm_potential_eval_gradient(pppm_potential *P, uint32_t M, const float *eval4, double *gx,
                                                     double *gy, double *gz) {
     return pot_eval(P, M, eval4, gx, gy, gz, true);
+}
+
+extern "C" pppm_status pppm_potential_eval_gradient3(pppm_potential *P, uint32_t M, const float *eval4,
+                                                     double *grad3) {
+    return pot_eval(P, M, eval4, grad3, grad3 ? grad3 + 1 : nullptr, grad3 ? grad3 + 2 : nullptr, true, 3);
 }
 
 extern "C" pppm_status pppm_potential_eval_scalar(pppm_potential *P, uint32_t M, const float *eval4, double *phi) {

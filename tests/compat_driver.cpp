@@ -103,6 +103,20 @@ int main(int argc, char **argv) {
     cudaDeviceSynchronize();
     cudaMemcpy(x.data(), dx, 8 * C, cudaMemcpyDeviceToHost);
 
+    // PotentialFieldSolver: masses = the x strengths at the vortex positions,
+    // gradient evaluated at the same positions (HFS/PotentialFieldSolver.h)
+    PotentialFieldSolver pf;
+    CK(pf.initializeSolver(n, n, n, 1, N, N));
+    CK(pf.setMassParameter(N, &cent, &vx));
+    CK(pf.setEvalParameter(N, &cent));
+    pf.computeFarFieldBuffer();
+    CK(pf.lastOk());
+    CK(pf.evaluateGradient(true));
+    std::vector<double> grad(3 * (size_t)N);
+    cudaDeviceSynchronize();
+    cudaMemcpy(grad.data(), pf.getGradPhi()->getDevicePtr(), 24 * (size_t)N, cudaMemcpyDeviceToHost);
+    pf.shutdown();
+
     FILE *g = std::fopen(argv[2], "wb");
     std::fwrite(u.data(), 8, u.size(), g);
     std::fwrite(keys.data(), 4, keys.size(), g);
@@ -111,6 +125,7 @@ int main(int argc, char **argv) {
     const double oo[3] = {o.x, o.y, o.z};
     std::fwrite(oo, 8, 3, g);
     std::fwrite(x.data(), 8, x.size(), g);
+    std::fwrite(grad.data(), 8, grad.size(), g);
     std::fclose(g);
     solver.shutdown();
     std::printf("ok N=%u n=%u\n", N, n);

@@ -1,5 +1,5 @@
 """The C++ classes of include/pppm_compat.hpp (BiotSavartSolver,
-ParticleManager, MultiGridSolver3DPeriod_double) compiled with g++ into a
+ParticleManager, MultiGridSolver3DPeriod_double, PotentialFieldSolver) compiled with g++ into a
 driver that calls them like the reference's own callers, checked against the
 oracle: velocities <= 1e-5, hash keys and sorted indices bit-exact, and the
 multigrid solution against the oracle's FP64 reference schedule."""
@@ -53,7 +53,8 @@ def test_cpp_compat_classes_match_oracle(tmp_path, oracle):
     keys = np.frombuffer(raw, np.uint32, N, off); off += 4 * N
     idx = np.frombuffer(raw, np.uint32, N, off); off += 4 * N
     h, ox, oy, oz = np.frombuffer(raw, np.float64, 4, off); off += 32
-    x = np.frombuffer(raw, np.float64, n ** 3, off)
+    x = np.frombuffer(raw, np.float64, n ** 3, off); off += 8 * n ** 3
+    grad = np.frombuffer(raw, np.float64, 3 * N, off).reshape(N, 3)
 
     ref, d = oracle.pppm(oracle.params(n), pos, al, pos, pos, 1, dump=True)
     assert rel_l2(u, ref) <= 1e-5
@@ -62,3 +63,5 @@ def test_cpp_compat_classes_match_oracle(tmp_path, oracle):
     q = np.arange(n ** 3, dtype=np.float64)
     xr, _, _ = oracle.mg_solve(np.sin(0.001 * q) - 0.5, n, mg_mode=0)
     assert rel_l2(x, xr) <= 1e-6
+    gref = oracle.potential(n, 1, pos, al[:, 0], pos)
+    assert rel_l2(grad, gref) <= 1e-5
