@@ -177,21 +177,34 @@ __device__ __forceinline__ void stage_record(float *__restrict__ pk, int slot, i
 template <bool SEG, bool COUNT>
 __device__ __forceinline__ void cell_pairs_packed(const float4 *__restrict__ vrec, const float4 *__restrict__ valf,
                                                   uint32_t ps, uint32_t pe, float cr_lane, const float3 ra,
-                                                  const float3 rb, float3 o, float2 inv_a3, const float2 *cf,
-                                                  float inv4pia3, bool need_exp, float4 *__restrict__ pk4, int lane,
-                                                  PairAcc2 &acc) {
+                                                  const float3 rb, float3 o, const float3 blo, const float3 bhi,
+                                                  float2 inv_a3, const float2 *cf, float inv4pia3, bool need_exp,
+                                                  float4 *__restrict__ pk4, int lane, PairAcc2 &acc) {
     float *pk = reinterpret_cast<float *>(pk4);
     const float2 tx = make_float2(ra.x, ra.x), ty = make_float2(ra.y, ra.y), tz = make_float2(ra.z, ra.z);
     for (uint32_t base = ps; base < pe; base += 32) {
         const uint32_t cnt = min(32u, pe - base);
+        // records outside the warp's box [blo, bhi] (every lane's box, widened
+        // beyond float rounding) cannot pass any lane's test: the chunk keeps
+        // only the others, packed to the front
+        bool keep = false;
+        float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
         if ((uint32_t)lane < cnt) {
-            stage_record(pk, lane >> 1, lane & 1, vrec[base + lane], valf[base + lane], o);
-        } else if ((uint32_t)lane == cnt && (cnt & 1u)) {
-            stage_record(pk, lane >> 1, 1, make_float4(-1e18f, -1e18f, -1e18f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f),
-                         make_float3(0.f, 0.f, 0.f));
+            r = vrec[base + lane];
+            keep = r.x >= blo.x && r.x <= bhi.x && r.y >= blo.y && r.y <= bhi.y && r.z >= blo.z && r.z <= bhi.z;
         }
+        const unsigned kept = __ballot_sync(0xffffffffu, keep);
+        const uint32_t kc = (uint32_t)__popc(kept);
+        if (kc == 0) continue;
+        if (keep) {
+            const int dst = __popc(kept & ((1u << lane) - 1u));
+            stage_record(pk, dst >> 1, dst & 1, r, valf[base + lane], o);
+        }
+        if (lane == 0 && (kc & 1u))
+            stage_record(pk, (int)(kc >> 1), 1, make_float4(-1e18f, -1e18f, -1e18f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f),
+                         make_float3(0.f, 0.f, 0.f));
         __syncwarp();
-        const uint32_t np = (cnt + 1) >> 1;
+        const uint32_t np = (kc + 1) >> 1;
 #pragma unroll 2
         for (uint32_t p = 0; p < np; p++) {
             const float4 A = pk4[0 * kPackSlots + p], B = pk4[1 * kPackSlots + p], Cc = pk4[2 * kPackSlots + p];
@@ -306,6 +319,26 @@ __global__ void __launch_bounds__(kEvalThreads, 8) eval_kernel(const SmoothSerie
         const float3 o = make_float3(__shfl_sync(0xffffffffu, ra.x, 0), __shfl_sync(0xffffffffu, ra.y, 0),
                                      __shfl_sync(0xffffffffu, ra.z, 0));
         o_w = o;
+        // the warp's box: every active lane's box, widened by far more than
+        // the rounding of these float bounds (2^-18 of the coordinates' size)
+        float3 blo, bhi;
+        {
+            float lx = act ? ra.x : INFINITY, ly = act ? ra.y : INFINITY, lz = act ? ra.z : INFINITY;
+            float hx = act ? ra.x : -INFINITY, hy = act ? ra.y : -INFINITY, hz = act ? ra.z : -INFINITY;
+#pragma unroll
+            for (int s2 = 16; s2 > 0; s2 >>= 1) {
+                lx = fminf(lx, __shfl_xor_sync(0xffffffffu, lx, s2));
+                ly = fminf(ly, __shfl_xor_sync(0xffffffffu, ly, s2));
+                lz = fminf(lz, __shfl_xor_sync(0xffffffffu, lz, s2));
+                hx = fmaxf(hx, __shfl_xor_sync(0xffffffffu, hx, s2));
+                hy = fmaxf(hy, __shfl_xor_sync(0xffffffffu, hy, s2));
+                hz = fmaxf(hz, __shfl_xor_sync(0xffffffffu, hz, s2));
+            }
+            const float mx = ldexpf(fabsf(lx) + fabsf(hx) + cr, -18), my = ldexpf(fabsf(ly) + fabsf(hy) + cr, -18),
+                        mz = ldexpf(fabsf(lz) + fabsf(hz) + cr, -18);
+            blo = make_float3(lx - cr - mx, ly - cr - my, lz - cr - mz);
+            bhi = make_float3(hx + cr + mx, hy + cr + my, hz + cr + mz);
+        }
         const float2 inv_a3_2 = make_float2(inv_a3, inv_a3);
         // The reference walks hash cells [i-K-1, i+K+1]^3.  Only the half-cells
         // (cell, octant runs of the vortex order) that can hold a vortex inside
@@ -356,8 +389,8 @@ __global__ void __launch_bounds__(kEvalThreads, 8) eval_kernel(const SmoothSerie
                         if (ps == kEmpty) continue;
                         const bool lane_ok = act && ci >= rlo[0] && ci <= rhi[0] && cj >= rlo[1] && cj <= rhi[1] &&
                                              ck >= rlo[2] && ck <= rhi[2];
-                        cell_pairs_packed<SEG, COUNT>(vrec, valf, ps, pe, lane_ok ? cr : -1.0f, ra, rb, o,
-                                                      inv_a3_2, cf2, inv4pia3, need_exp, pk, lane, acc2);
+                        cell_pairs_packed<SEG, COUNT>(vrec, valf, ps, pe, lane_ok ? cr : -1.0f, ra, rb, o, blo,
+                                                      bhi, inv_a3_2, cf2, inv4pia3, need_exp, pk, lane, acc2);
                     }
         } else if (act && lo[0] <= hi[0]) {
             // scattered warp (points outside the grid, sparse regions): own walk

@@ -12,7 +12,7 @@ from ._lib import check, load
 
 
 def _f32x4(t: torch.Tensor, name: str) -> torch.Tensor:
-    if not isinstance(t, torch.Tensor) or not t.is_cuda or t.dtype != torch.float32 or t.dim() != 2 \\
+    if not isinstance(t, torch.Tensor) or not t.is_cuda or t.dtype != torch.float32 or t.dim() != 2 \
             or t.shape[1] != 4:
         raise ValueError(f"{name} must be a CUDA float32 (n, 4) tensor")
     return t.contiguous()

@@ -55,3 +55,11 @@ def test_no_cpu_fallback():
 def test_version_string():
     import pppm_vortex_bouyant_flow_sample_b200._lib as L
     assert b"sm_100a" in L.load().pppm_version()
+
+
+def test_every_package_module_imports_without_gpu():
+    """Every module of the package imports on a machine without a GPU (the
+    GPU is needed only when a solver is created)."""
+    import importlib
+    for m in ("potential", "render", "replicas", "server", "frames", "workloads", "_lib"):
+        importlib.import_module("pppm_vortex_bouyant_flow_sample_b200." + m)
