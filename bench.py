@@ -44,6 +44,10 @@ def workload(N: int, n: int) -> str:
     return (f"vortex ring, {N:,} particles, {n}^3 grid, K=1, a=0.08, domain 3x bbox, "
             "reference multigrid schedule (FMG + 1 V(4,4), FP32 with FP64 defect correction); "
             "step = far-field build + velocity at every particle")
+PLUME_N = 4_194_304
+PLUME_GRID = 256
+PLUME_RADIUS = 0.5
+PLUME_DT = 0.002
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1965e6 / 1e12  # nominal: SMs x FP32 lanes x FMA x max clock
 L2_FLUSH_BYTES = 512 << 20
 
@@ -57,9 +61,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--particles", type=int, default=N_PART)
     ap.add_argument("--grid", type=int, default=GRID)
-    ap.add_argument("--workload", default="ring", choices=["ring", "mix", "serve", "render"],
+    ap.add_argument("--workload", default="ring", choices=["ring", "mix", "serve", "render", "plume"],
                     help="ring: the at-scale single scene (default); mix: 64 independent scenes, "
-                         "one after another vs in one batch")
+                         "one after another vs in one batch; plume: buoyant time steps")
+    ap.add_argument("--plume-radius", type=float, default=PLUME_RADIUS,
+                    help="plume: radius of the heated sphere")
     ap.add_argument("--scenes", type=int, default=64)
     ap.add_argument("--rate", type=float, default=200.0, help="serve: mean arrivals per second")
     ap.add_argument("--duration", type=float, default=4.0, help="serve: seconds of arrivals")
@@ -612,6 +618,129 @@ def run_render(args, world, rank, local):
     rnd.close()
 
 
+def plume_cpu_rate(N: int, n: int, radius: float):
+    """The oracle's plume step (orc_baroclinic, then orc_vortex_step with the
+    converged multigrid) on the host cores for a sample with the particles
+    and the grid edge cut by 8 and 2: the same particles per cell."""
+    from oracle import pyoracle as O
+    from pppm_vortex_bouyant_flow_sample_b200 import workloads as W
+    O.build()
+    Ns, ns = max(N // 8, 1000), max(n // 2, 8)
+    pos, al, temp = W.plume_sphere(Ns, seed=3, radius=radius)
+    prm = O.params(ns, mg_mode=1, mg_tol=1e-10)
+    heat = temp.astype(np.float32)
+    t0 = time.perf_counter()
+    al = O.baroclinic(pos, heat, pos, al, PLUME_DT, cap=201 ** 3)[0]
+    O.vortex_step(prm, pos, al, PLUME_DT, h_seg=0.1, nu=0.1)
+    sec = time.perf_counter() - t0
+    return {"value": Ns / sec, "unit": "particle-steps/s", "cores": O.num_threads(), "kind": "port",
+            "sample": f"oracle plume step (baroclinic + vortex-segment step, converged multigrid) for "
+                      f"{Ns:,} particles on {ns}^3 ({sec:.1f} s): the same particles per cell"}
+
+
+def run_plume(args, world, rank, local):
+    """Buoyant plume time steps: N particles uniform in a sphere at
+    (0.5, 0.15, 0.5) carrying a temperature N(1, 0.05^2) and no vorticity
+    (seed 3), n^3 grid, dt = 0.002, the multigrid iterated to a relative
+    residual of 1e-10.  A step is Scene.solve_time_step: the baroclinic source
+    from the particles' own temperatures, then the vortex-segment step
+    (segments, velocity at 2N ends, move, stretching, Gaussian smoothing).
+    The timed steps are steps 1..K of the plume from its initial state (the
+    warm-up runs from the same state, which is then restored); the state
+    evolves from step to step, as in a simulation.  e2e repeats steps 1..3
+    with the frame output of every step (positions to pinned host memory).
+    Radius 0.5 is the heat emitter radius of the reference's demo; with
+    radius 0.1 the reference's 0.2-spaced density grid has two cells per
+    axis, no density gradient, and the plume never moves.  The reference adds
+    the baroclinic increment per particle, with no particle volume, so the
+    circulation grows with N: at millions of particles the sphere disperses
+    within a few steps and the later steps cost more (a dense core in a
+    stretched domain)."""
+    import torch
+    import pppm_vortex_bouyant_flow_sample_b200 as pb
+    from pppm_vortex_bouyant_flow_sample_b200 import workloads as W
+    torch.cuda.set_device(local)
+    N = args.particles if args.particles != N_PART else PLUME_N
+    n = args.grid if args.grid != GRID else PLUME_GRID
+    pos, al, temp = W.plume_sphere(N, seed=3, radius=args.plume_radius)
+    scene = pb.Scene(n, cap_vort=N, cap_eval=2 * N, mg="converged", mg_tol=1e-10, mg_max_cycles=50)
+    pos0 = torch.from_numpy(pos).cuda()
+    al0 = torch.from_numpy(np.ascontiguousarray(al.T)).cuda()
+    dpos, dal = pos0.clone(), al0.clone()
+    dtemp = torch.from_numpy(temp.astype(np.float32)).cuda()
+    stream = torch.cuda.current_stream()
+    warm = max(args.warmup, 3)
+    for _ in range(warm):
+        scene.solve_time_step(dpos, dal, PLUME_DT, dtemp)
+    dpos.copy_(pos0)
+    dal.copy_(al0)
+    torch.cuda.synchronize()
+    scene.set_profiling(True)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms, ms_baro, stages = [], [], []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(stream)
+        scene.baroclinic(dpos, dtemp, dpos, dal, PLUME_DT)
+        e1.record(stream)
+        scene.vortex_step(dpos, dal, PLUME_DT, h_seg=0.1, nu=0.1)
+        e2.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e2))
+        ms_baro.append(e0.elapsed_time(e1))
+        stages.append(scene.stage_times())
+    clk = clocks.stop()
+    scene.set_profiling(False)
+    step_ms = sum(ms) / len(ms)  # mean over steps 1..K: the simulation's throughput
+    mg = scene.stats()
+    p = dpos.cpu().numpy()
+    a = dal.cpu().numpy()
+    host = torch.empty((N, 4), dtype=torch.float32, pin_memory=True)
+    dpos.copy_(pos0)
+    dal.copy_(al0)
+    e2e = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        scene.solve_time_step(dpos, dal, PLUME_DT, dtemp)
+        host.copy_(dpos, non_blocking=True)
+        torch.cuda.synchronize()
+        e2e.append(time.perf_counter() - t0)
+    e2e_s = statistics.median(e2e)
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            cpu = plume_cpu_rate(N, n, args.plume_radius)
+        except Exception as exc:  # reported, not fatal
+            cpu = {"value": None, "unit": "particle-steps/s", "cores": None, "kind": "port", "sample": f"failed: {exc}"}
+    keys = stages[0].keys()
+    st = {k: statistics.median(s[k] for s in stages) for k in keys if stages[0][k] >= 0}
+    if rank == 0:
+        print(json.dumps({
+            "metric": "buoyant plume particle-steps/s", "value": N / (step_ms / 1000.0),
+            "unit": "particle-steps/s", "n_gpus": 1, "steps": args.steps, "warmup": warm, "ms_per_step": step_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (multigrid residual/accumulation f64)", "data": "synthetic",
+            "config": {"workload": f"buoyant plume, {N:,} particles in a radius-{args.plume_radius} sphere, "
+                                   f"{n}^3 grid, dt={PLUME_DT}, multigrid to 1e-10, steps 1..{args.steps} "
+                                   "from the initial state",
+                       "l2": "flushed between timed steps (512 MB write)"},
+            "e2e": {"value": N / e2e_s, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": N * 16},
+            "clocks": clk, "cpu_baseline": cpu,
+            "step_ms": [round(x, 2) for x in ms],
+            "baroclinic_ms": statistics.median(ms_baro), "vortex_step_stages_ms": st,
+            "mg_cycles_last": mg["mg_cycles"], "mg_relres_last": mg["mg_relres"],
+            "state_after": {"steps": args.steps, "mean_y": float(p[:, 1].astype(np.float64).mean()),
+                            "alpha_rms": float(np.sqrt((a * a).sum(axis=0).mean())),
+                            "finite": bool(np.isfinite(p).all() and np.isfinite(a).all())}}), flush=True)
+    scene.close()
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
@@ -626,6 +755,9 @@ def main():
         return
     if args.workload == "render":
         run_render(args, world, rank, local)
+        return
+    if args.workload == "plume":
+        run_plume(args, world, rank, local)
         return
     run_b200(args, world, rank, local)
 

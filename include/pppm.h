@@ -189,7 +189,10 @@ pppm_status pppm_get_density(pppm_scene *s, uint32_t *dim, double origin[3], dou
                              const float **rho_dev, const float **grad_dev);
 
 /* Accessors matching BiotSavartSolver::getOrigin / getCellh
- * (HFS/BiotSavartSolver.h:34-35); synchronises the stream. */
+ * (HFS/BiotSavartSolver.h:34-35); synchronises the stream.  PPPM_ERR_DOMAIN
+ * (origin and length still filled) when the last far field had a zero or
+ * non-finite domain edge (one vortex, or all coincident); pppm_eval then
+ * returned zero velocities. */
 pppm_status pppm_get_domain(pppm_scene *s, double origin[3], double *length, double *cell_h);
 /* getVortStartTable / getVortEndTable (HFS/BiotSavartSolver.h:28-29): device
  * pointers to n^3 uint32 tables (empty cells hold 0xFFFFFFFF in both). */

@@ -267,6 +267,23 @@ class Scene:
                 alpha.copy_(torch.stack([ax, ay, az], dim=0))
         return alpha
 
+    def solve_time_step(self, pos4: torch.Tensor, alpha: torch.Tensor, dt: float, heat: torch.Tensor,
+                        heat4: torch.Tensor | None = None, h_seg: float = 0.1, nu: float = 0.1):
+        """One buoyant time step of VortexSimulationSystem::solveTimeStep without
+        emitters or boundary (HFS/VortexSimulationSystemImp.cpp:90-125):
+        addBaroclinicForce (:369-465), then the vortex-segment step
+        (convertVortToSeg, computeURotation, applyFlow, convertSegToVort,
+        computeStretching).
+
+        heat (H,) float32 is the temperature of the heat particles heat4 (H, 4),
+        which move with the flow in place; with heat4 None the vortex particles
+        themselves carry it (H = N) and move as vortices.  pos4 and alpha are
+        updated in place.  Returns (pos4, alpha)."""
+        carried = heat4 is None
+        self.baroclinic(pos4 if carried else heat4, heat, pos4, alpha, dt)
+        self.vortex_step(pos4, alpha, dt, h_seg=h_seg, nu=nu, passive=None if carried else heat4)
+        return pos4, alpha
+
     def density(self):
         """(dim, origin, h, rho (dim^3,) float32, grad (3, dim^3) float32) of the last pppm_baroclinic."""
         dim = C.c_uint32()

@@ -412,6 +412,14 @@ __global__ void __launch_bounds__(kEvalThreads, 8) eval_kernel(const SmoothSerie
         ux += acc.x + (fmaf(Ay, sz, -(Az * sy)) - Bx);
         uy += acc.y + (fmaf(Az, sx, -(Ax * sz)) - By);
         uz += acc.z + (fmaf(Ax, sy, -(Ay * sx)) - Bz);
+        if (P->status != 0) {
+            // zero or non-finite domain edge (one vortex, or all coincident):
+            // the cell size is 0 and the sums above are meaningless; the
+            // velocity is defined as 0 and pppm_get_domain reports the domain
+            ux = 0.f;
+            uy = 0.f;
+            uz = 0.f;
+        }
         if (u) {
             u[q] = (double)ux;
             v[q] = (double)uy;

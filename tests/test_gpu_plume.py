@@ -1,0 +1,114 @@
+"""Buoyant plume time steps (Scene.solve_time_step) against the oracle.
+
+A sphere of particles that carry a temperature N(1, 0.05^2) and no vorticity,
+as in the plume workload: each step is addBaroclinicForce on the particles'
+own temperatures, then the vortex-segment step, with the multigrid iterated
+to a relative residual of 1e-10 (FP32 cycles inside an FP64 defect
+correction).  The oracle chains orc_baroclinic and orc_vortex_step the same
+way (HFS/VortexSimulationSystemImp.cpp:90-125).
+
+The reference's density grid has a fixed spacing of 0.2 (edge
+floor(1.2 extent / 0.2) + 1), so a sphere of radius 0.1 gets a 2^3 grid whose
+periodic gradient is zero: no baroclinic vorticity arises and nothing moves.
+That case is checked as such; the parity runs use radius 0.5, the heat
+emitter radius of the reference's demo (HFS/newTest.cpp:45), a 7^3 grid.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+DT = 0.002
+
+
+@pytest.fixture(scope="module")
+def pb():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import pppm_vortex_bouyant_flow_sample_b200 as pb
+    pb.load()
+    return pb
+
+
+def _gpu_steps(pb, n, pos, al, temp, steps, **kw):
+    import torch
+    scene = pb.Scene(n, cap_vort=len(pos), cap_eval=2 * len(pos), mg="converged", mg_tol=1e-10, **kw)
+    dpos = torch.from_numpy(pos.copy()).cuda()
+    dal = torch.from_numpy(np.ascontiguousarray(al, dtype=np.float64)).cuda()
+    dtemp = torch.from_numpy(temp.astype(np.float32)).cuda()
+    out = []
+    for _ in range(steps):
+        scene.solve_time_step(dpos, dal, DT, dtemp)
+        out.append((dpos.cpu().numpy().copy(), dal.cpu().numpy().copy()))
+    scene.close()
+    return out
+
+
+def _oracle_steps(oracle, n, pos, al, temp, steps):
+    prm = oracle.params(n, mg_mode=1, mg_tol=1e-10)
+    heat = temp.astype(np.float32)
+    out = []
+    for _ in range(steps):
+        al = oracle.baroclinic(pos, heat, pos, al, DT, cap=201 ** 3)[0]
+        pos, al, _, _ = oracle.vortex_step(prm, pos, al, DT, h_seg=0.1, nu=0.1)
+        out.append((pos.copy(), al.copy()))
+    return out
+
+
+def test_plume_steps_match_oracle(pb, oracle):
+    from pppm_vortex_bouyant_flow_sample_b200 import workloads as W
+    pos, al, temp = W.plume_sphere(20000, seed=3, radius=0.5)
+    n, steps = 32, 3
+    got = _gpu_steps(pb, n, pos, al, temp, steps)
+    ref = _oracle_steps(oracle, n, pos, al, temp, steps)
+    gprev = rprev = pos[:, :3].astype(np.float64)
+    for s, ((gp, ga), (rp, ra)) in enumerate(zip(got, ref)):
+        assert np.linalg.norm(ra) > 0
+        # the strengths: baroclinic source plus stretching, smoothed
+        assert rel_l2(ga, ra) <= 1e-4 * (s + 1)
+        # the displacement of this step
+        gcur, rcur = gp[:, :3].astype(np.float64), rp[:, :3].astype(np.float64)
+        assert rel_l2(gcur - gprev, rcur - rprev) <= 1e-4 * (s + 1)
+        gprev, rprev = gcur, rcur
+
+
+def test_plume_of_radius_0_1_stays_at_rest(pb, oracle):
+    from pppm_vortex_bouyant_flow_sample_b200 import workloads as W
+    pos, al, temp = W.plume_sphere(20000, seed=3, radius=0.1)
+    got = _gpu_steps(pb, 32, pos, al, temp, 2)
+    ref = _oracle_steps(oracle, 32, pos, al, temp, 1)
+    assert not ref[0][1].any()
+    for gp, ga in got:
+        assert not ga.any()
+        assert np.array_equal(gp[:, :3], pos[:, :3])
+
+
+def test_plume_with_separate_heat_particles(pb, oracle):
+    """Heat particles apart from the vortices (the reference's demo layout):
+    they source the baroclinic term and move with the flow as passive points."""
+    import torch
+    from pppm_vortex_bouyant_flow_sample_b200 import workloads as W
+    heat4, _, temp = W.plume_sphere(30000, seed=5, radius=0.5)
+    rng = np.random.default_rng(6)
+    pos = np.zeros((12000, 4), np.float32)
+    pos[:, :3] = heat4[rng.integers(0, len(heat4), 12000), :3] + rng.normal(0, 0.01, (12000, 3)).astype(np.float32)
+    al = rng.normal(0, 1e-4, (12000, 3))
+    n = 32
+    scene = pb.Scene(n, cap_vort=len(pos), cap_eval=2 * len(pos), mg="converged", mg_tol=1e-10)
+    dpos = torch.from_numpy(pos.copy()).cuda()
+    dal = torch.from_numpy(al.copy()).cuda()
+    dheat4 = torch.from_numpy(heat4.copy()).cuda()
+    scene.solve_time_step(dpos, dal, DT, torch.from_numpy(temp.astype(np.float32)).cuda(), heat4=dheat4)
+    prm = oracle.params(n, mg_mode=1, mg_tol=1e-10)
+    ra = oracle.baroclinic(heat4, temp.astype(np.float32), pos, al, DT, cap=201 ** 3)[0]
+    rc, ra, _, _, rheat, _ = oracle.vortex_step(prm, pos, ra, DT, h_seg=0.1, nu=0.1, passive4=heat4)
+    assert rel_l2(dal.cpu().numpy(), ra) <= 1e-4
+    gh = dheat4.cpu().numpy()
+    base = heat4[:, :3].astype(np.float64)
+    assert rel_l2(gh[:, :3] - base, rheat[:, :3].astype(np.float64) - base) <= 1e-4
+    gc = dpos.cpu().numpy()
+    assert rel_l2(gc[:, :3] - pos[:, :3], rc[:, :3].astype(np.float64) - pos[:, :3]) <= 1e-4
+    scene.close()
