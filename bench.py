@@ -143,7 +143,7 @@ class ClockSampler:
                 "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3] not in ("", "[N/A]"))}
 
 
-def cpu_sample_rate(pos, al, n, m_small=2000, m_big=12000):
+def cpu_sample_rate(pos, al, n, m_small=20000, m_big=200000):
     """Oracle (FP64 restatement of the reference path) on the host cores:
     the whole far-field build for all particles plus the near field at two
     evaluation subsets; the per-point cost is extrapolated to all particles."""
@@ -182,7 +182,7 @@ def run_reference(args, world, rank):
     vals = []
     t0 = time.perf_counter()
     for _ in range(max(args.steps, 1)):
-        r = cpu_sample_rate(pos, al, args.grid, m_small=1000, m_big=4000)
+        r = cpu_sample_rate(pos, al, args.grid, m_small=4000, m_big=40000)
         vals.append(r["value"])
     el = time.perf_counter() - t0
     value = statistics.median(vals)

@@ -18,7 +18,8 @@
 //     (alpha x d) * phi((r/a)^3) / (4 pi a^3) with phi(t) = (1 - e^-t)/t,
 //     which equals (1 - e^-(r/a)^3) / (4 pi r^3); pairs with r = 0, or (for
 //     segments) a zero distance to the other end, are skipped.
-// Pair arithmetic is FP32 (r from rsqrt, ~1 ulp); phi uses a degree-4
+// Pair arithmetic is FP32 (r^3 = r^2 sqrt.approx(r^2) in the warp-uniform walk,
+// r^2 rsqrt(r^2) in a lane's own walk; ~1 ulp); phi uses a degree-4
 // polynomial below t = 0.25 (Chebyshev interpolant, relative error 5e-9, no
 // cancellation) and (1 - exp(-t)) / t above.
 #include <climits>
@@ -153,6 +154,22 @@ struct PairAcc2 {
 constexpr int kPackSlots = 16;
 constexpr int kPackPlanes = 5;
 
+// max(|a|, |b|, |c|) in one instruction: the three-input max.abs of PTX ISA 8.8
+// (sm_100 and later).
+__device__ __forceinline__ float max3_abs(float a, float b, float c) {
+    float r;
+    asm("max.abs.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
+// sqrt.approx.f32: one special-function op, sqrt(+0) = +0, so r^3 = r^2 sqrt(r^2)
+// needs no guard at r = 0 (where rsqrt would give infinity).
+__device__ __forceinline__ float sqrt_approx(float x) {
+    float r;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 __device__ __forceinline__ void stage_record(float *__restrict__ pk, int slot, int half, float4 r, float4 a,
                                              float3 o) {
     float *A = pk + 4 * (0 * kPackSlots + slot), *B = pk + 4 * (1 * kPackSlots + slot);
@@ -173,13 +190,15 @@ __device__ __forceinline__ void stage_record(float *__restrict__ pk, int slot, i
 // whose hash-cell range excludes this run.  An odd chunk is padded with a
 // record at (-1e18, -1e18, -1e18) and zero strength, outside every box.  The
 // r = 0 exclusion needs no test: the pair's (ra - r_p) is zero.  SEG keeps the
-// other-end test.
-template <bool SEG, bool COUNT>
+// other-end test.  FOLD: the polynomial's coefficients carry the powers of
+// 1/a^3, so it takes r^3 directly; tbig is then 0.25 a^3 instead of 0.25.
+template <bool SEG, bool COUNT, bool FOLD>
 __device__ __forceinline__ void cell_pairs_packed(const float4 *__restrict__ vrec, const float4 *__restrict__ valf,
                                                   uint32_t ps, uint32_t pe, float cr_lane, const float3 ra,
                                                   const float3 rb, float3 o, const float3 blo, const float3 bhi,
-                                                  float2 inv_a3, const float2 *cf, float inv4pia3, bool need_exp,
-                                                  float4 *__restrict__ pk4, int lane, PairAcc2 &acc) {
+                                                  float2 inv_a3, const float2 *cf, float tbig, float inv4pia3,
+                                                  bool need_exp, float4 *__restrict__ pk4, int lane,
+                                                  PairAcc2 &acc) {
     float *pk = reinterpret_cast<float *>(pk4);
     const float2 tx = make_float2(ra.x, ra.x), ty = make_float2(ra.y, ra.y), tz = make_float2(ra.z, ra.z);
     for (uint32_t base = ps; base < pe; base += 32) {
@@ -211,8 +230,8 @@ __device__ __forceinline__ void cell_pairs_packed(const float4 *__restrict__ vre
             const float4 D = pk4[3 * kPackSlots + p], E = pk4[4 * kPackSlots + p];
             const float2 nx = make_float2(A.x, A.y), ny = make_float2(A.z, A.w), nz = make_float2(B.x, B.y);
             const float2 dx = __fadd2_rn(tx, nx), dy = __fadd2_rn(ty, ny), dz = __fadd2_rn(tz, nz);
-            const float m0 = fmaxf(fabsf(dx.x), fmaxf(fabsf(dy.x), fabsf(dz.x)));
-            const float m1 = fmaxf(fabsf(dx.y), fmaxf(fabsf(dy.y), fabsf(dz.y)));
+            const float m0 = max3_abs(dx.x, dy.x, dz.x);
+            const float m1 = max3_abs(dx.y, dy.y, dz.y);
             const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
             bool ok0 = m0 <= cr_lane, ok1 = m1 <= cr_lane;
             if (COUNT) acc.n += (ok0 ? 1ull : 0ull) + (ok1 ? 1ull : 0ull);
@@ -224,20 +243,18 @@ __device__ __forceinline__ void cell_pairs_packed(const float4 *__restrict__ vre
                 ok0 = ok0 && !(e2.x < 1e-24f);
                 ok1 = ok1 && !(e2.y < 1e-24f);
             }
-            // 1e-30 keeps rsqrt finite at r = 0 (that pair's term is zero anyway);
-            // it changes r2 only below 2e-23, i.e. r < 5e-12
-            const float2 r2g = __fadd2_rn(r2, make_float2(1e-30f, 1e-30f));
-            const float2 rs = make_float2(rsqrtf(r2g.x), rsqrtf(r2g.y));
-            const float2 t = __fmul2_rn(__fmul2_rn(r2, __fmul2_rn(r2, rs)), inv_a3);
+            const float2 r3 = __fmul2_rn(r2, make_float2(sqrt_approx(r2.x), sqrt_approx(r2.y)));
+            const float2 t = FOLD ? r3 : __fmul2_rn(r3, inv_a3);
             float2 c = __ffma2_rn(cf[4], t, cf[3]);
             c = __ffma2_rn(c, t, cf[2]);
             c = __ffma2_rn(c, t, cf[1]);
             c = __ffma2_rn(c, t, cf[0]);
             if (need_exp) {
-                const bool big0 = ok0 && t.x >= 0.25f, big1 = ok1 && t.y >= 0.25f;
+                const bool big0 = ok0 && t.x >= tbig, big1 = ok1 && t.y >= tbig;
                 if (__any_sync(0xffffffffu, big0 || big1)) {
-                    const float e0 = __fdividef(1.0f - __expf(-t.x), fmaxf(t.x, 0.25f)) * inv4pia3;
-                    const float e1 = __fdividef(1.0f - __expf(-t.y), fmaxf(t.y, 0.25f)) * inv4pia3;
+                    const float s0 = FOLD ? t.x * inv_a3.x : t.x, s1 = FOLD ? t.y * inv_a3.y : t.y;
+                    const float e0 = __fdividef(1.0f - __expf(-s0), fmaxf(s0, 0.25f)) * inv4pia3;
+                    const float e1 = __fdividef(1.0f - __expf(-s1), fmaxf(s1, 0.25f)) * inv4pia3;
                     c.x = big0 ? e0 : c.x;
                     c.y = big1 ? e1 : c.y;
                 }
@@ -260,11 +277,16 @@ constexpr int kUniformMaxSub = 1000;  // warp-uniform walk up to 10^3 half-cells
 // the other-end test is the r = 0 test itself, so SEG is off).
 // Series coefficients of the smoothing kernel, known on the host from a alone;
 // passed by value so they sit in the constant bank.
+// The packed forms hold each coefficient twice ({c, c}): the f32x2 multiply-add
+// then reads them straight from the kernel's parameter bank.
 struct SmoothSeries {
-    float c[5];
+    float c[5];     // in t = (r/a)^3, scaled by 1/(4 pi a^3)
+    float2 c2[5];   // c, packed
+    float2 cu2[5];  // the same polynomial in r^3 (c[q] / a^(3q)), packed, when it fits float
+    float tbig;     // 0.25 a^3: the exp branch's threshold in r^3
 };
 
-template <bool SEG, bool COUNT>
+template <bool SEG, bool COUNT, bool FOLD>
 __global__ void __launch_bounds__(kEvalThreads, 8) eval_kernel(const SmoothSeries sc, const uint32_t *__restrict__ eidx, uint32_t M, const float4 *__restrict__ eval_a,
             const float4 *__restrict__ eval_b, const float *__restrict__ far,
             const uint32_t *__restrict__ start, const uint32_t *__restrict__ end,
@@ -312,9 +334,8 @@ __global__ void __launch_bounds__(kEvalThreads, 8) eval_kernel(const SmoothSerie
         const float cr = P->cr_f, inv_a3 = P->inv_a3_f, inv4pia3 = P->inv4pia3_f;
         const bool need_exp = P->need_exp != 0;
         const float *cf = sc.c;
-        float2 cf2[5];
-#pragma unroll
-        for (int q = 0; q < 5; q++) cf2[q] = make_float2(cf[q], cf[q]);
+        const float2 *cf2 = FOLD ? sc.cu2 : sc.c2;
+        const float tbig = FOLD ? sc.tbig : 0.25f;
         // warp origin of the packed accumulation: lane 0's position
         const float3 o = make_float3(__shfl_sync(0xffffffffu, ra.x, 0), __shfl_sync(0xffffffffu, ra.y, 0),
                                      __shfl_sync(0xffffffffu, ra.z, 0));
@@ -389,8 +410,9 @@ __global__ void __launch_bounds__(kEvalThreads, 8) eval_kernel(const SmoothSerie
                         if (ps == kEmpty) continue;
                         const bool lane_ok = act && ci >= rlo[0] && ci <= rhi[0] && cj >= rlo[1] && cj <= rhi[1] &&
                                              ck >= rlo[2] && ck <= rhi[2];
-                        cell_pairs_packed<SEG, COUNT>(vrec, valf, ps, pe, lane_ok ? cr : -1.0f, ra, rb, o, blo,
-                                                      bhi, inv_a3_2, cf2, inv4pia3, need_exp, pk, lane, acc2);
+                        cell_pairs_packed<SEG, COUNT, FOLD>(vrec, valf, ps, pe, lane_ok ? cr : -1.0f, ra, rb, o,
+                                                            blo, bhi, inv_a3_2, cf2, tbig, inv4pia3, need_exp, pk,
+                                                            lane, acc2);
                     }
         } else if (act && lo[0] <= hi[0]) {
             // scattered warp (points outside the grid, sparse regions): own walk
@@ -487,23 +509,43 @@ cudaError_t launch_eval(pppm_scene *s, const float4 *eval_a, const float4 *eval_
     const unsigned grid = (M + kEvalThreads - 1) / kEvalThreads;
     unsigned long long *pc = count_pairs ? s->pair_count : nullptr;
     SmoothSeries sc;
+    bool fold = true;
     {
         const double a = s->prm.a;
         const double k = 1.0 / (kFourPi * a * a * a);
         double f[5];
         phi_chebyshev4(f);
-        for (int q = 0; q < 5; q++) sc.c[q] = (float)(k * f[q]);
+        for (int q = 0; q < 5; q++) {
+            sc.c[q] = (float)(k * f[q]);
+            sc.c2[q] = make_float2(sc.c[q], sc.c[q]);
+        }
+        // r^3 form: c_q / a^(3q); kept only while every coefficient is a normal
+        // float far from overflow (a in about [0.01, 100])
+        const double ia3 = 1.0 / (a * a * a);
+        double pw = 1.0;
+        for (int q = 0; q < 5; q++, pw *= ia3) {
+            const double cu = k * f[q] * pw;
+            if (!(std::fabs(cu) <= 1e30 && std::fabs(cu) >= 1e-30)) fold = false;
+            sc.cu2[q] = make_float2((float)cu, (float)cu);
+        }
+        sc.tbig = (float)(0.25 * a * a * a);
     }
 #define PPPM_EVAL_ARGS sc, sidx, M, eval_a, eval_b, s->far, s->cell_start, s->cell_end, s->sub_start, s->sub_end, \
                        s->vrec, s->valf, s->dparams, \
                        (int)s->n, s->prm.K, u, v, w, uf, pc
+#define PPPM_EVAL_LAUNCH(SEG_, COUNT_)                                                              \
+    do {                                                                                              \
+        if (fold) eval_kernel<SEG_, COUNT_, true><<<grid, kEvalThreads, 0, s->stream>>>(PPPM_EVAL_ARGS); \
+        else eval_kernel<SEG_, COUNT_, false><<<grid, kEvalThreads, 0, s->stream>>>(PPPM_EVAL_ARGS);    \
+    } while (0)
     if (seg) {
-        if (count_pairs) eval_kernel<true, true><<<grid, kEvalThreads, 0, s->stream>>>(PPPM_EVAL_ARGS);
-        else eval_kernel<true, false><<<grid, kEvalThreads, 0, s->stream>>>(PPPM_EVAL_ARGS);
+        if (count_pairs) PPPM_EVAL_LAUNCH(true, true);
+        else PPPM_EVAL_LAUNCH(true, false);
     } else {
-        if (count_pairs) eval_kernel<false, true><<<grid, kEvalThreads, 0, s->stream>>>(PPPM_EVAL_ARGS);
-        else eval_kernel<false, false><<<grid, kEvalThreads, 0, s->stream>>>(PPPM_EVAL_ARGS);
+        if (count_pairs) PPPM_EVAL_LAUNCH(false, true);
+        else PPPM_EVAL_LAUNCH(false, false);
     }
+#undef PPPM_EVAL_LAUNCH
 #undef PPPM_EVAL_ARGS
     prof_end(s, kStageEval);
     return cudaGetLastError();
