@@ -19,11 +19,14 @@
 //     which equals (1 - e^-(r/a)^3) / (4 pi r^3); pairs with r = 0, or (for
 //     segments) a zero distance to the other end, are skipped.
 // Pair arithmetic is FP32 (r^3 = r^2 sqrt.approx(r^2) in the warp-uniform walk,
-// r^2 rsqrt(r^2) in a lane's own walk; ~1 ulp); phi uses a degree-4
-// polynomial below t = 0.25 (Chebyshev interpolant, relative error 5e-9, no
-// cancellation) and (1 - exp(-t)) / t above.
+// r^2 rsqrt(r^2) in a lane's own walk; ~1 ulp).  phi: when no pair of the
+// scene can reach t = 0.25, a degree-4 polynomial (Chebyshev interpolant on
+// [0, 0.25], relative error 5e-9); otherwise a degree-7 one on [0, 2] (relative
+// error 2e-7, below that of the exp form near t = 0.25) and (1 - exp(-t)) / t
+// above t = 2.  No cancellation in either polynomial.
 #include <climits>
 #include <cmath>
+#include <type_traits>
 #include <utility>
 
 #include "pppm_internal.cuh"
@@ -162,11 +165,12 @@ __device__ __forceinline__ float max3_abs(float a, float b, float c) {
     return r;
 }
 
-// sqrt.approx.f32: one special-function op, sqrt(+0) = +0, so r^3 = r^2 sqrt(r^2)
-// needs no guard at r = 0 (where rsqrt would give infinity).
+// sqrt.approx.ftz.f32: one special-function op, sqrt(+0) = +0, so
+// r^3 = r^2 sqrt(r^2) needs no guard at r = 0 (where rsqrt would give infinity);
+// a subnormal r^2 (r < 1e-19) flushes to 0, where phi is its value at 0.
 __device__ __forceinline__ float sqrt_approx(float x) {
     float r;
-    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
     return r;
 }
 
@@ -190,9 +194,11 @@ __device__ __forceinline__ void stage_record(float *__restrict__ pk, int slot, i
 // whose hash-cell range excludes this run.  An odd chunk is padded with a
 // record at (-1e18, -1e18, -1e18) and zero strength, outside every box.  The
 // r = 0 exclusion needs no test: the pair's (ra - r_p) is zero.  SEG keeps the
-// other-end test.  FOLD: the polynomial's coefficients carry the powers of
-// 1/a^3, so it takes r^3 directly; tbig is then 0.25 a^3 instead of 0.25.
-template <bool SEG, bool COUNT, bool FOLD>
+// other-end test.  phi is the degree-DEG polynomial cf (DEG 4: the scene never
+// leaves [0, 0.25]; DEG 7: valid on [0, 2], the exp form above tbig when
+// need_exp).  FOLD: the coefficients carry the powers of 1/a^3, so the
+// polynomial takes r^3 directly and tbig is in r^3 too.
+template <bool SEG, bool COUNT, bool FOLD, int DEG>
 __device__ __forceinline__ void cell_pairs_packed(const float4 *__restrict__ vrec, const float4 *__restrict__ valf,
                                                   uint32_t ps, uint32_t pe, float cr_lane, const float3 ra,
                                                   const float3 rb, float3 o, const float3 blo, const float3 bhi,
@@ -245,16 +251,15 @@ __device__ __forceinline__ void cell_pairs_packed(const float4 *__restrict__ vre
             }
             const float2 r3 = __fmul2_rn(r2, make_float2(sqrt_approx(r2.x), sqrt_approx(r2.y)));
             const float2 t = FOLD ? r3 : __fmul2_rn(r3, inv_a3);
-            float2 c = __ffma2_rn(cf[4], t, cf[3]);
-            c = __ffma2_rn(c, t, cf[2]);
-            c = __ffma2_rn(c, t, cf[1]);
-            c = __ffma2_rn(c, t, cf[0]);
-            if (need_exp) {
+            float2 c = __ffma2_rn(cf[DEG], t, cf[DEG - 1]);
+#pragma unroll
+            for (int q = DEG - 2; q >= 0; q--) c = __ffma2_rn(c, t, cf[q]);
+            if (DEG > 4 && need_exp) {
                 const bool big0 = ok0 && t.x >= tbig, big1 = ok1 && t.y >= tbig;
                 if (__any_sync(0xffffffffu, big0 || big1)) {
                     const float s0 = FOLD ? t.x * inv_a3.x : t.x, s1 = FOLD ? t.y * inv_a3.y : t.y;
-                    const float e0 = __fdividef(1.0f - __expf(-s0), fmaxf(s0, 0.25f)) * inv4pia3;
-                    const float e1 = __fdividef(1.0f - __expf(-s1), fmaxf(s1, 0.25f)) * inv4pia3;
+                    const float e0 = __fdividef(1.0f - __expf(-s0), fmaxf(s0, 1.0f)) * inv4pia3;
+                    const float e1 = __fdividef(1.0f - __expf(-s1), fmaxf(s1, 1.0f)) * inv4pia3;
                     c.x = big0 ? e0 : c.x;
                     c.y = big1 ? e1 : c.y;
                 }
@@ -277,13 +282,15 @@ constexpr int kUniformMaxSub = 1000;  // warp-uniform walk up to 10^3 half-cells
 // the other-end test is the r = 0 test itself, so SEG is off).
 // Series coefficients of the smoothing kernel, known on the host from a alone;
 // passed by value so they sit in the constant bank.
-// The packed forms hold each coefficient twice ({c, c}): the f32x2 multiply-add
-// then reads them straight from the kernel's parameter bank.
+// Polynomials of phi, scaled by 1/(4 pi a^3).  The packed forms hold each
+// coefficient twice ({c, c}): the f32x2 multiply-add then reads them straight
+// from the kernel's parameter bank.  With fold they are in r^3 (c_q / a^(3q)),
+// otherwise in t = (r/a)^3.
 struct SmoothSeries {
-    float c[5];     // in t = (r/a)^3, scaled by 1/(4 pi a^3)
-    float2 c2[5];   // c, packed
-    float2 cu2[5];  // the same polynomial in r^3 (c[q] / a^(3q)), packed, when it fits float
-    float tbig;     // 0.25 a^3: the exp branch's threshold in r^3
+    float c[5];    // degree 4 on [0, 0.25], in t (a lane's own walk)
+    float2 p4[5];  // degree 4 on [0, 0.25], packed
+    float2 p7[8];  // degree 7 on [0, 2], packed
+    float t7;      // 2 in the packed polynomials' variable: where the exp form takes over
 };
 
 template <bool SEG, bool COUNT, bool FOLD>
@@ -334,8 +341,9 @@ __global__ void __launch_bounds__(kEvalThreads, 8) eval_kernel(const SmoothSerie
         const float cr = P->cr_f, inv_a3 = P->inv_a3_f, inv4pia3 = P->inv4pia3_f;
         const bool need_exp = P->need_exp != 0;
         const float *cf = sc.c;
-        const float2 *cf2 = FOLD ? sc.cu2 : sc.c2;
-        const float tbig = FOLD ? sc.tbig : 0.25f;
+        // some pair can reach t = 0.25: the degree-7 polynomial, exp above t = 2
+        const bool tier7 = need_exp;
+        const bool need_exp2 = P->need_exp2 != 0;
         // warp origin of the packed accumulation: lane 0's position
         const float3 o = make_float3(__shfl_sync(0xffffffffu, ra.x, 0), __shfl_sync(0xffffffffu, ra.y, 0),
                                      __shfl_sync(0xffffffffu, ra.z, 0));
@@ -387,8 +395,11 @@ __global__ void __launch_bounds__(kEvalThreads, 8) eval_kernel(const SmoothSerie
         long long vol = 1;
 #pragma unroll
         for (int a = 0; a < 3; a++) vol *= (uhi[a] >= ulo[a]) ? (long long)(uhi[a] - ulo[a] + 1) : 0ll;
-        if (vol > 0 && vol <= kUniformMaxSub) {
-            // warp-uniform walk over half-cells: every lane sees the same vortex at once
+        // warp-uniform walk over half-cells: every lane sees the same vortex at
+        // once; DEG picks phi's polynomial (one walk per polynomial, so that
+        // only one pair loop is live at a time)
+        auto uniform_walk = [&](auto deg) {
+            constexpr int D = decltype(deg)::value;
             for (int k2 = ulo[2]; k2 <= uhi[2]; k2++)
                 for (int j2 = ulo[1]; j2 <= uhi[1]; j2++)
                     for (int i2 = ulo[0]; i2 <= uhi[0];) {
@@ -410,10 +421,15 @@ __global__ void __launch_bounds__(kEvalThreads, 8) eval_kernel(const SmoothSerie
                         if (ps == kEmpty) continue;
                         const bool lane_ok = act && ci >= rlo[0] && ci <= rhi[0] && cj >= rlo[1] && cj <= rhi[1] &&
                                              ck >= rlo[2] && ck <= rhi[2];
-                        cell_pairs_packed<SEG, COUNT, FOLD>(vrec, valf, ps, pe, lane_ok ? cr : -1.0f, ra, rb, o,
-                                                            blo, bhi, inv_a3_2, cf2, tbig, inv4pia3, need_exp, pk,
-                                                            lane, acc2);
+                        cell_pairs_packed<SEG, COUNT, FOLD, D>(vrec, valf, ps, pe, lane_ok ? cr : -1.0f, ra, rb, o,
+                                                               blo, bhi, inv_a3_2, D == 7 ? sc.p7 : sc.p4,
+                                                               sc.t7, inv4pia3, D == 7 && need_exp2, pk, lane,
+                                                               acc2);
                     }
+        };
+        if (vol > 0 && vol <= kUniformMaxSub) {
+            if (tier7) uniform_walk(std::integral_constant<int, 7>{});
+            else uniform_walk(std::integral_constant<int, 4>{});
         } else if (act && lo[0] <= hi[0]) {
             // scattered warp (points outside the grid, sparse regions): own walk
             for (int kk = lo[2] >> 1; kk <= (hi[2] >> 1); kk++)
@@ -461,31 +477,32 @@ __global__ void __launch_bounds__(kEvalThreads, 8) eval_kernel(const SmoothSerie
     }
 }
 
-// Monomial coefficients of the degree-4 polynomial that interpolates
-// phi(t) = (1 - e^-t) / t at the 5 Chebyshev nodes of [0, 0.25] (a near-best
-// uniform approximation: relative error 2.6e-9 on the interval), by solving
-// the 5 x 5 Vandermonde system in FP64.
-void phi_chebyshev4(double c[5]) {
+// Monomial coefficients of the degree-deg polynomial that interpolates
+// phi(t) = (1 - e^-t) / t at the deg + 1 Chebyshev nodes of [0, T] (a near-best
+// uniform approximation: relative error 2.6e-9 for degree 4 on [0, 0.25],
+// 2e-8 for degree 7 on [0, 2]), by solving the Vandermonde system in FP64.
+void phi_chebyshev(int deg, double T, double *c) {
     const double pi = 3.14159265358979323846;
-    double V[5][6];
-    for (int k = 0; k < 5; k++) {
-        const double t = 0.125 + 0.125 * std::cos((2 * k + 1) * pi / 10.0);
+    const int m = deg + 1;
+    double V[8][9];
+    for (int k = 0; k < m; k++) {
+        const double t = 0.5 * T + 0.5 * T * std::cos((2 * k + 1) * pi / (2.0 * m));
         double pw = 1.0;
-        for (int q = 0; q < 5; q++) { V[k][q] = pw; pw *= t; }
-        V[k][5] = -std::expm1(-t) / t;
+        for (int q = 0; q < m; q++) { V[k][q] = pw; pw *= t; }
+        V[k][m] = -std::expm1(-t) / t;
     }
-    for (int col = 0; col < 5; col++) {  // Gaussian elimination, partial pivoting
+    for (int col = 0; col < m; col++) {  // Gauss-Jordan elimination, partial pivoting
         int piv = col;
-        for (int r = col + 1; r < 5; r++)
+        for (int r = col + 1; r < m; r++)
             if (std::fabs(V[r][col]) > std::fabs(V[piv][col])) piv = r;
-        for (int q = 0; q < 6; q++) std::swap(V[col][q], V[piv][q]);
-        for (int r = 0; r < 5; r++) {
+        for (int q = 0; q <= m; q++) std::swap(V[col][q], V[piv][q]);
+        for (int r = 0; r < m; r++) {
             if (r == col) continue;
             const double f = V[r][col] / V[col][col];
-            for (int q = col; q < 6; q++) V[r][q] -= f * V[col][q];
+            for (int q = col; q <= m; q++) V[r][q] -= f * V[col][q];
         }
     }
-    for (int q = 0; q < 5; q++) c[q] = V[q][5] / V[q][q];
+    for (int q = 0; q < m; q++) c[q] = V[q][m] / V[q][q];
 }
 
 }  // namespace
@@ -511,24 +528,32 @@ cudaError_t launch_eval(pppm_scene *s, const float4 *eval_a, const float4 *eval_
     SmoothSeries sc;
     bool fold = true;
     {
+        // the packed polynomials in r^3 (c_q / a^(3q)) while every coefficient
+        // stays a normal float far from overflow, else in t = (r/a)^3
         const double a = s->prm.a;
         const double k = 1.0 / (kFourPi * a * a * a);
-        double f[5];
-        phi_chebyshev4(f);
-        for (int q = 0; q < 5; q++) {
-            sc.c[q] = (float)(k * f[q]);
-            sc.c2[q] = make_float2(sc.c[q], sc.c[q]);
-        }
-        // r^3 form: c_q / a^(3q); kept only while every coefficient is a normal
-        // float far from overflow (a in about [0.01, 100])
         const double ia3 = 1.0 / (a * a * a);
-        double pw = 1.0;
-        for (int q = 0; q < 5; q++, pw *= ia3) {
-            const double cu = k * f[q] * pw;
-            if (!(std::fabs(cu) <= 1e30 && std::fabs(cu) >= 1e-30)) fold = false;
-            sc.cu2[q] = make_float2((float)cu, (float)cu);
+        double f4[5], f7[8];
+        phi_chebyshev(4, 0.25, f4);
+        phi_chebyshev(7, 2.0, f7);
+        double u4[5], u7[8], pw = 1.0;
+        for (int q = 0; q < 8; q++, pw *= ia3) {
+            if (q < 5) u4[q] = k * f4[q] * pw;
+            u7[q] = k * f7[q] * pw;
+            for (double x : {q < 5 ? u4[q] : 1.0, u7[q]})
+                if (!(std::fabs(x) <= 1e30 && std::fabs(x) >= 1e-30)) fold = false;
         }
-        sc.tbig = (float)(0.25 * a * a * a);
+        pw = 1.0;
+        for (int q = 0; q < 8; q++) {
+            if (q < 5) {
+                sc.c[q] = (float)(k * f4[q]);
+                const float v4 = fold ? (float)u4[q] : sc.c[q];
+                sc.p4[q] = make_float2(v4, v4);
+            }
+            const float v7 = fold ? (float)u7[q] : (float)(k * f7[q]);
+            sc.p7[q] = make_float2(v7, v7);
+        }
+        sc.t7 = fold ? (float)(2.0 * a * a * a) : 2.0f;
     }
 #define PPPM_EVAL_ARGS sc, sidx, M, eval_a, eval_b, s->far, s->cell_start, s->cell_end, s->sub_start, s->sub_end, \
                        s->vrec, s->valf, s->dparams, \

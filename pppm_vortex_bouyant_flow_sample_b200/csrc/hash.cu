@@ -121,6 +121,7 @@ __global__ void params_kernel(const float *__restrict__ partial, int nblocks, pp
         const double rmax = ((double)prm.K + 0.5) * h * 1.7320508075688772 * 1.001;
         const double tmax = (rmax / a) * (rmax / a) * (rmax / a);
         P->need_exp = !(tmax < 0.25);
+        P->need_exp2 = !(tmax < 2.0);
     }
     // The FP32 hash coordinate fl(fl(p - o_f) / h_f) and the FP64 NGP coordinate
     // fl32(p - o) / h differ by at most a few float roundings of |p| + |o| over h;

@@ -48,6 +48,7 @@ struct DevParams {
     float inv_a3_f;     // 1/a^3
     float inv4pia3_f;   // 1/(4 pi a^3)
     int32_t need_exp;   // some pair inside the box can reach (r/a)^3 >= 0.25
+    int32_t need_exp2;  // ... and (r/a)^3 >= 2
     double prune_cells; // bound, in cells, on |hash cell coordinate - FP64 NGP coordinate|
                         // plus the float rounding of the box test (near-field cell pruning)
     uint32_t n;
