@@ -733,6 +733,8 @@ def run_plume(args, world, rank, local):
                     "d2h_bytes_per_step": N * 16},
             "clocks": clk, "cpu_baseline": cpu,
             "step_ms": [round(x, 2) for x in ms],
+            "step1_stages_ms": {k: round(v, 3) for k, v in stages[0].items() if v >= 0},
+            "step1_baroclinic_ms": ms_baro[0],
             "baroclinic_ms": statistics.median(ms_baro), "vortex_step_stages_ms": st,
             "mg_cycles_last": mg["mg_cycles"], "mg_relres_last": mg["mg_relres"],
             "state_after": {"steps": args.steps, "mean_y": float(p[:, 1].astype(np.float64).mean()),
