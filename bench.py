@@ -61,9 +61,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--particles", type=int, default=N_PART)
     ap.add_argument("--grid", type=int, default=GRID)
-    ap.add_argument("--workload", default="ring", choices=["ring", "mix", "serve", "render", "plume"],
+    ap.add_argument("--workload", default="ring", choices=["ring", "mix", "serve", "render", "plume", "potential"],
                     help="ring: the at-scale single scene (default); mix: 64 independent scenes, "
-                         "one after another vs in one batch; plume: buoyant time steps")
+                         "one after another vs in one batch; plume: buoyant time steps; potential: "
+                         "the scalar PPPM (PotentialFieldSolver)")
     ap.add_argument("--plume-radius", type=float, default=PLUME_RADIUS,
                     help="plume: radius of the heated sphere")
     ap.add_argument("--scenes", type=int, default=64)
@@ -743,6 +744,98 @@ def run_plume(args, world, rank, local):
     scene.close()
 
 
+def run_potential(args, world, rank, local):
+    """Scalar PPPM (PotentialFieldSolver): 262,144 boundary sources on a sphere
+    of radius 0.15 at (0.5, 0.5, 0.5), mass = panel area x cos(polar angle),
+    128^3 grid, K = 1; gradient at 1,048,576 points uniform in the shell
+    0.16 <= r <= 0.29 around it.  A step is computeFarFieldBuffer (density,
+    monopole Dirichlet data, three full-multigrid calls, gradient buffer)
+    followed by evaluateGradient at every point, device-timed with the inputs
+    resident; e2e adds the upload of sources, masses and points and the
+    download of the gradients.  The oracle (FP64 restatement) runs the whole
+    step on the host cores (a second or two): its time is the CPU baseline and
+    its gradients give the GPU's error against it at full scale."""
+    import torch
+    import pppm_vortex_bouyant_flow_sample_b200 as pb
+    from pppm_vortex_bouyant_flow_sample_b200 import workloads as W
+    from pppm_vortex_bouyant_flow_sample_b200.potential import PotentialFieldSolver
+    torch.cuda.set_device(local)
+    pb.load()
+    Ns = 262_144
+    M = args.particles
+    n = args.grid
+    src, mass = W.sphere_panels(Ns)
+    ev = W.shell_points(M)
+    dsrc, dmass, dev = (torch.from_numpy(a).cuda() for a in (src, mass, ev))
+    solver = PotentialFieldSolver()
+    solver.initializeSolver(n, n, n, K_NEAR, M, Ns)
+    stream = torch.cuda.current_stream()
+
+    def step(sp, mp, ep):
+        solver.setMassParameter(Ns, sp, mp)
+        solver.setEvalParameter(M, ep)
+        solver.computeFarFieldBuffer()
+        solver.evaluateGradient(True)
+        return solver.getGradPhi()
+
+    warm = max(args.warmup, 3)
+    for _ in range(warm):
+        step(dsrc, dmass, dev)
+    torch.cuda.synchronize()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step(dsrc, dmass, dev)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    clk = clocks.stop()
+    step_ms = statistics.median(ms)
+    g = step(dsrc, dmass, dev).cpu().numpy()
+    hs, hm, he = (torch.from_numpy(a).pin_memory() for a in (src, mass, ev))
+    gh = torch.empty((M, 3), dtype=torch.float64, pin_memory=True)
+    e2e = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = step(hs.cuda(non_blocking=True), hm.cuda(non_blocking=True), he.cuda(non_blocking=True))
+        gh.copy_(out, non_blocking=True)
+        torch.cuda.synchronize()
+        e2e.append(time.perf_counter() - t0)
+    e2e_s = statistics.median(e2e)
+    cpu, err = None, None
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import pyoracle as O
+        O.build()
+        t0 = time.perf_counter()
+        ref = O.potential(n, K_NEAR, src, mass, ev)
+        sec = time.perf_counter() - t0
+        cpu = {"value": M / sec, "unit": "gradient evals/s", "cores": O.num_threads(), "kind": "port",
+               "sample": f"the whole step (build for {Ns:,} sources + gradient at all {M:,} points) by the "
+                         f"oracle's FP64 restatement ({sec:.1f} s)"}
+        err = float(np.linalg.norm(g - ref) / np.linalg.norm(ref))
+    solver.shutdown()
+    if rank == 0:
+        print(json.dumps({
+            "metric": "scalar PPPM gradient evals/s (PotentialFieldSolver)", "value": M / (step_ms / 1000.0),
+            "unit": "gradient evals/s", "n_gpus": 1, "steps": args.steps, "warmup": warm, "ms_per_step": step_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 (multigrid f32 with f64 defect correction)", "data": "synthetic",
+            "config": {"workload": f"{Ns:,} sphere sources (radius 0.15), {n}^3 grid, K=1, gradient at {M:,} "
+                                   "shell points; step = computeFarFieldBuffer + evaluateGradient",
+                       "l2": "flushed between timed steps (512 MB write)"},
+            "e2e": {"value": M / e2e_s, "unit": "gradient evals/s", "h2d_bytes_per_step": Ns * 24 + M * 16,
+                    "d2h_bytes_per_step": M * 24},
+            "clocks": clk, "cpu_baseline": cpu, "rel_l2_vs_oracle": err}), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
@@ -760,6 +853,9 @@ def main():
         return
     if args.workload == "plume":
         run_plume(args, world, rank, local)
+        return
+    if args.workload == "potential":
+        run_potential(args, world, rank, local)
         return
     run_b200(args, world, rank, local)
 

@@ -52,9 +52,32 @@ __device__ __forceinline__ double nb_sum64(const double *__restrict__ x, int i, 
     return ((lv + rv) + (uv + dv)) + (fv + bv);
 }
 
+// log2(d) for a power-of-two edge, else -1: index arithmetic then uses shifts
+// instead of integer division (every level of the 32..512 grids).
+inline int edge_log2(int d) {
+    if (d <= 0 || (d & (d - 1))) return -1;
+    int l = 0;
+    while ((1 << l) < d) l++;
+    return l;
+}
+
+// t -> (i, j, k) on an a x d x d index box (x fastest); la = log2(a) or -1,
+// ld = log2(d) or -1.
+__device__ __forceinline__ void split3(uint32_t t, int a, int d, int la, int ld, int &i, int &j, int &k) {
+    if (la >= 0 && ld >= 0) {
+        i = (int)(t & (uint32_t)(a - 1));
+        j = (int)((t >> la) & (uint32_t)(d - 1));
+        k = (int)(t >> (la + ld));
+    } else {
+        i = (int)(t % (uint32_t)a);
+        j = (int)((t / (uint32_t)a) % (uint32_t)d);
+        k = (int)(t / ((uint32_t)a * (uint32_t)d));
+    }
+}
+
 // One half sweep over the cells with (i+j+k) % 2 == color.
 __global__ void __launch_bounds__(kMGThreads)
-rbsor_kernel(float *__restrict__ x, const float *__restrict__ b, int d, int color) {
+rbsor_kernel(float *__restrict__ x, const float *__restrict__ b, int d, int color, int ld) {
     const int half = d >> 1;
     const uint32_t per = (uint32_t)half * d * d;
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -63,9 +86,8 @@ rbsor_kernel(float *__restrict__ x, const float *__restrict__ b, int d, int colo
     const size_t cells = (size_t)d * d * d;
     float *xc = x + comp * cells;
     const float *bc = b + comp * cells;
-    const int ih = (int)(t % half);
-    const int j = (int)((t / half) % d);
-    const int k = (int)(t / ((uint32_t)half * d));
+    int ih, j, k;
+    split3(t, half, d, ld > 0 ? ld - 1 : -1, ld, ih, j, k);
     const int i = 2 * ih + ((j + k + color) & 1);
     const size_t c = ((size_t)k * d + j) * d + i;
     const float r = nb_sum(xc, i, j, k, d, c) - bc[c];
@@ -76,7 +98,7 @@ rbsor_kernel(float *__restrict__ x, const float *__restrict__ b, int d, int colo
 // bc = 0.5 * sum over the 8 children of (bf - (sum_nbr(xf) - 6 xf)).
 __global__ void __launch_bounds__(kMGThreads)
 resid_restrict_kernel(const float *__restrict__ xf, const float *__restrict__ bf, float *__restrict__ bc,
-                      int dc, int x_zero) {
+                      int dc, int x_zero, int ldc) {
     const uint32_t per = (uint32_t)dc * dc * dc;
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= per) return;
@@ -85,7 +107,8 @@ resid_restrict_kernel(const float *__restrict__ xf, const float *__restrict__ bf
     const size_t fcells = (size_t)df * df * df;
     const float *x = xf + comp * fcells;
     const float *b = bf + comp * fcells;
-    const int ic = (int)(t % dc), jc = (int)((t / dc) % dc), kc = (int)(t / ((uint32_t)dc * dc));
+    int ic, jc, kc;
+    split3(t, dc, dc, ldc, ldc, ic, jc, kc);
     float sum = 0.f;
 #pragma unroll
     for (int q = 0; q < 8; q++) {
@@ -99,13 +122,14 @@ resid_restrict_kernel(const float *__restrict__ xf, const float *__restrict__ bf
 }
 
 __global__ void __launch_bounds__(kMGThreads)
-prolong_kernel(float *__restrict__ xf, const float *__restrict__ xc, int df) {
+prolong_kernel(float *__restrict__ xf, const float *__restrict__ xc, int df, int ldf) {
     const uint32_t per = (uint32_t)df * df * df;
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= per) return;
     const size_t comp = blockIdx.y;
     const int dc = df >> 1;
-    const int i = (int)(t % df), j = (int)((t / df) % df), k = (int)(t / ((uint32_t)df * df));
+    int i, j, k;
+    split3(t, df, df, ldf, ldf, i, j, k);
     xf[comp * per + t] += xc[comp * (size_t)dc * dc * dc + ((size_t)(k >> 1) * dc + (j >> 1)) * dc + (i >> 1)];
 }
 
@@ -182,14 +206,16 @@ coarse_apply_kernel(const double *__restrict__ op, float *__restrict__ x, const 
 // -(vort * h2f) from the FP32 P2M grid.  Optional squared norms of r and b.
 __global__ void __launch_bounds__(kMGThreads)
 dc_residual_kernel(const double *__restrict__ psi, const double *__restrict__ b64, const float *__restrict__ vort,
-                   const DevParams *__restrict__ P, float *__restrict__ rout, int d, double *__restrict__ norms) {
+                   const DevParams *__restrict__ P, float *__restrict__ rout, int d, int ld,
+                   double *__restrict__ norms) {
     const uint32_t per = (uint32_t)d * d * d;
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     const size_t comp = blockIdx.y;
     double r2 = 0.0, b2 = 0.0;
     if (t < per) {
         const double *x = psi + comp * per;
-        const int i = (int)(t % d), j = (int)((t / d) % d), k = (int)(t / ((uint32_t)d * d));
+        int i, j, k;
+        split3(t, d, d, ld, ld, i, j, k);
         double bv;
         if (b64)
             bv = b64[comp * per + t];
@@ -282,25 +308,26 @@ static cudaError_t vcycle32(const MGPlan &m, int level) {
         const dim3 g = grid_for((uint32_t)(d / 2) * d * d, m.comps);
         for (int it = 0; it < 4; it++) {
             ::pppm::note_launch();
-            rbsor_kernel<<<g, kMGThreads, 0, m.st>>>(m.lv[j].x, m.lv[j].b, d, 1);
+            rbsor_kernel<<<g, kMGThreads, 0, m.st>>>(m.lv[j].x, m.lv[j].b, d, 1, edge_log2(d));
             ::pppm::note_launch();
-            rbsor_kernel<<<g, kMGThreads, 0, m.st>>>(m.lv[j].x, m.lv[j].b, d, 0);
+            rbsor_kernel<<<g, kMGThreads, 0, m.st>>>(m.lv[j].x, m.lv[j].b, d, 0, edge_log2(d));
         }
         ::pppm::note_launch();
         resid_restrict_kernel<<<grid_for(m.lv[j + 1].cells, m.comps), kMGThreads, 0, m.st>>>(
-            m.lv[j].x, m.lv[j].b, m.lv[j + 1].b, (int)m.lv[j + 1].d, 0);
+            m.lv[j].x, m.lv[j].b, m.lv[j + 1].b, (int)m.lv[j + 1].d, 0, edge_log2((int)m.lv[j + 1].d));
     }
     coarse_solve(m);
     for (int j = L - 2; j >= level; j--) {
         const int d = (int)m.lv[j].d;
         ::pppm::note_launch();
-        prolong_kernel<<<grid_for(m.lv[j].cells, m.comps), kMGThreads, 0, m.st>>>(m.lv[j].x, m.lv[j + 1].x, d);
+        prolong_kernel<<<grid_for(m.lv[j].cells, m.comps), kMGThreads, 0, m.st>>>(m.lv[j].x, m.lv[j + 1].x, d,
+                                                                                  edge_log2(d));
         const dim3 g = grid_for((uint32_t)(d / 2) * d * d, m.comps);
         for (int it = 0; it < 4; it++) {
             ::pppm::note_launch();
-            rbsor_kernel<<<g, kMGThreads, 0, m.st>>>(m.lv[j].x, m.lv[j].b, d, 1);
+            rbsor_kernel<<<g, kMGThreads, 0, m.st>>>(m.lv[j].x, m.lv[j].b, d, 1, edge_log2(d));
             ::pppm::note_launch();
-            rbsor_kernel<<<g, kMGThreads, 0, m.st>>>(m.lv[j].x, m.lv[j].b, d, 0);
+            rbsor_kernel<<<g, kMGThreads, 0, m.st>>>(m.lv[j].x, m.lv[j].b, d, 0, edge_log2(d));
         }
     }
     return cudaGetLastError();
@@ -316,14 +343,14 @@ static cudaError_t fmg32(const MGPlan &m) {
     for (int j = 0; j < L - 1; j++) {
         ::pppm::note_launch();
         resid_restrict_kernel<<<grid_for(m.lv[j + 1].cells, m.comps), kMGThreads, 0, m.st>>>(
-            m.lv[j].x, m.lv[j].b, m.lv[j + 1].b, (int)m.lv[j + 1].d, 1);
+            m.lv[j].x, m.lv[j].b, m.lv[j + 1].b, (int)m.lv[j + 1].d, 1, edge_log2((int)m.lv[j + 1].d));
     }
     coarse_solve(m);
     PPPM_CUDA_TRY(cudaGetLastError());
     for (int j = L - 2; j >= 0; j--) {
         ::pppm::note_launch();
-        prolong_kernel<<<grid_for(m.lv[j].cells, m.comps), kMGThreads, 0, m.st>>>(m.lv[j].x, m.lv[j + 1].x,
-                                                                                (int)m.lv[j].d);
+        prolong_kernel<<<grid_for(m.lv[j].cells, m.comps), kMGThreads, 0, m.st>>>(
+            m.lv[j].x, m.lv[j + 1].x, (int)m.lv[j].d, edge_log2((int)m.lv[j].d));
         PPPM_CUDA_TRY(vcycle32(m, j));
     }
     return cudaGetLastError();
@@ -336,7 +363,8 @@ static cudaError_t dc_residual(const MGPlan &m, bool want_norms) {
     if (want_norms) PPPM_CUDA_TRY(cudaMemsetAsync(m.norms, 0, 2 * sizeof(double), m.st));
     ::pppm::note_launch();
     dc_residual_kernel<<<grid_for(C0, m.comps), kMGThreads, 0, m.st>>>(m.psi, m.b64, m.vort, m.P, m.lv[0].b,
-                                                                       (int)m.lv[0].d, want_norms ? m.norms : nullptr);
+                                                                       (int)m.lv[0].d, edge_log2((int)m.lv[0].d),
+                                                                       want_norms ? m.norms : nullptr);
     return cudaGetLastError();
 }
 

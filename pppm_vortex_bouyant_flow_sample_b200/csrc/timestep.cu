@@ -35,7 +35,7 @@ namespace {
 
 constexpr int kSmoothThreads = 128;
 // A warp walks the union of its lanes' 5^3 boxes when that union holds at most
-// this many cells; otherwise it walks each distinct box in turn.
+// this many cells; otherwise (sparse vortices) each lane walks its own box.
 constexpr int kSmoothUnionMax = 250;
 
 // ComputePosb: endb = c + s/2, enda = c - s/2 with s = alpha capped to length
@@ -248,20 +248,33 @@ __global__ void __launch_bounds__(kSmoothThreads) gaussian_smooth_kernel(
         const int vol = (xhi - xlo + 1) * (yhi - ylo + 1) * (zhi - zlo + 1);
         if (vol <= kSmoothUnionMax) {
             walk(xlo, xhi, ylo, yhi, zlo, zhi, live);
-        } else {
-            const uint32_t key = (uint32_t)(ci + 4) | ((uint32_t)(cj + 4) << 10) | ((uint32_t)(ck + 4) << 20);
-            const unsigned group = __match_any_sync(0xffffffffu, key);
-            unsigned todo = 0xffffffffu;
-            while (todo) {
-                const int leader = __ffs(todo) - 1;
-                const unsigned gm = __shfl_sync(0xffffffffu, group, leader);
-                const int li = __shfl_sync(0xffffffffu, ci, leader);
-                const int lj = __shfl_sync(0xffffffffu, cj, leader);
-                const int lk = __shfl_sync(0xffffffffu, ck, leader);
-                walk(max(li - 2, 0), min(li + 2, n - 1), max(lj - 2, 0), min(lj + 2, n - 1), max(lk - 2, 0),
-                     min(lk + 2, n - 1), live && ((gm >> lane) & 1u));
-                todo &= ~gm;
-            }
+        } else if (live) {
+            // sparse warp (its lanes' boxes far apart): each lane walks its own
+            // 5^3 box with the same arithmetic, one record at a time
+            for (int z = max(ck - 2, 0); z <= min(ck + 2, n - 1); z++)
+                for (int y = max(cj - 2, 0); y <= min(cj + 2, n - 1); y++)
+                    for (int x = max(ci - 2, 0); x <= min(ci + 2, n - 1); x++) {
+                        const uint32_t c = ((uint32_t)z * (uint32_t)n + (uint32_t)y) * (uint32_t)n + (uint32_t)x;
+                        const uint32_t s0 = cstart[c];
+                        if (s0 == kEmpty) continue;
+                        const uint32_t s1 = cend[c];
+                        float pw = 0.f, px = 0.f, py = 0.f, pz = 0.f;
+                        for (uint32_t p = s0; p < s1; p++) {
+                            const float4 b = vrec[p];
+                            const float4 al = valf[p];
+                            const float dx = ra.x + (-b.x), dy = ra.y + (-b.y), dz = ra.z + (-b.z);
+                            const float dsq = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                            const float w = ex2_approx(dsq * wscale);
+                            pw += w;
+                            px = fmaf(w, al.x, px);
+                            py = fmaf(w, al.y, py);
+                            pz = fmaf(w, al.z, pz);
+                        }
+                        tw += (double)pw;
+                        wx += (double)px;
+                        wy += (double)py;
+                        wz += (double)pz;
+                    }
         }
     }
     if (!live) return;

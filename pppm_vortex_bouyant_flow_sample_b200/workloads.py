@@ -13,6 +13,9 @@ these scenes follow the workload descriptions instead:
   component (the ring's circulation stays Gamma).
 * ``plume_sphere``: positions uniform in a sphere (radius 0.1 at
   (0.5, 0.15, 0.5)), zero strength, temperature N(1, 0.05^2).
+* ``sphere_panels`` / ``shell_points``: sources of the scalar PPPM on a sphere
+  (mass = area x cos of the polar angle) and evaluation points in a shell
+  around it.
 * ``scene_mix``: the batched mix (grid edge from {32,48,64,96,128}, particle
   count log-uniform in [1e4, 1e6], even scenes clouds, odd scenes rings).
 """
@@ -101,6 +104,30 @@ def plume_sphere(N: int, seed: int = 3, radius: float = 0.1, centre=(0.5, 0.15, 
     alpha = np.zeros((N, 3))
     temp = 1.0 + 0.05 * g.normal(N)
     return pos, alpha, temp
+
+
+def sphere_panels(N: int, radius: float = 0.15, centre=(0.5, 0.5, 0.5)):
+    """Boundary-element sources: N points of a Fibonacci lattice on a sphere,
+    mass = panel area x cos(polar angle) (the source layer of a sphere in a
+    uniform stream along +y), as float4 positions and float64 masses."""
+    k = np.arange(N, dtype=np.float64) + 0.5
+    y = 1.0 - 2.0 * k / N
+    r = np.sqrt(np.maximum(0.0, 1.0 - y * y))
+    phi = np.pi * (3.0 - np.sqrt(5.0)) * k
+    p = np.stack([r * np.cos(phi), y, r * np.sin(phi)], axis=1)
+    pos = _pack_pos(*(centre[c] + radius * p[:, c] for c in range(3)))
+    mass = (4.0 * np.pi * radius * radius / N) * y
+    return pos, mass
+
+
+def shell_points(N: int, seed: int = 4, r0: float = 0.16, r1: float = 0.29, centre=(0.5, 0.5, 0.5)):
+    """N points uniform in the spherical shell r0 <= |x - centre| <= r1."""
+    g = SplitMix64(seed)
+    d = g.normal(3 * N).reshape(N, 3)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    r = np.cbrt(r0 ** 3 + (r1 ** 3 - r0 ** 3) * g.uniform(N))
+    p = np.asarray(centre)[None, :] + d * r[:, None]
+    return _pack_pos(p[:, 0], p[:, 1], p[:, 2])
 
 
 def scene_mix(count: int = 64, seed: int = 2, grids=(32, 48, 64, 96, 128),

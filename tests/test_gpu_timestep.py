@@ -96,7 +96,7 @@ def test_cloud_step_k2(pb, oracle):
 
 
 def test_sparse_step_wide_warps(pb, oracle):
-    """Few vortices per cell: warps span many cells and take the per-box walk."""
+    """Few vortices per cell: warps span many cells and each lane walks its own box."""
     from pppm_vortex_bouyant_flow_sample_b200 import workloads as W
     pos, al = W.uniform_cloud(3000, seed=43)
     _check(pb, oracle, 64, pos, al, 0.005, 0.1)
