@@ -8,15 +8,21 @@
  * Nothing in the product links it: only tests/, __graft_entry__.smoke() and the
  * cpu_baseline / reference legs of bench.py load it.
  *
- * Parity status: UNPINNED against reference outputs.  The reference ships no
- * golden vectors and cannot be built or run here (it needs GL headers, the CUDA
- * samples' helper_cuda.h / helper_math.h, and the texture-reference API that
- * CUDA 12 removed).  The restatement is anchored instead by known-answer tests
- * (tests/golden/, tests/test_oracle_*.py): FP32 cell assignment on crafted
- * face / +-1 ulp particles, the discrete zero-ghost Laplacian's sine
- * eigenmodes, the closed-form smoothed Biot-Savart kernel for one and two
- * blobs, the finite-difference Green's-gradient table, and an independent
- * numpy restatement of every stage at small sizes.
+ * Parity status: PINNED against the reference's own GPU kernels for every
+ * stage but the multigrid.  The reference ships no golden vectors and its
+ * whole solver cannot be built (the multigrid's host wrappers include GL
+ * headers, its kernels use the texture-reference API that CUDA 12 removed).
+ * Its hash kernels (particle_hash_kernel.cu) and its P2M, curl, far-field,
+ * interpolation and near-field kernels (GPU_kernel.cu) do build from their
+ * sources for sm_100a (`make -C oracle refgpu`, ref_gpu/); the GPU tests run
+ * them beside this restatement, stage by stage (tests/test_gpu_ref_kernels.py:
+ * keys, order and cell tables bit-exact; grids and velocities to FP64
+ * round-off).  The multigrid is anchored by known-answer tests instead
+ * (tests/golden/, tests/test_oracle_*.py): the discrete zero-ghost
+ * Laplacian's sine eigenmodes, the level rule, and an independent numpy
+ * restatement at small sizes; so are the FP32 cell assignment on crafted
+ * face / +-1 ulp particles, the closed-form smoothed Biot-Savart kernel for
+ * one and two blobs, and the finite-difference Green's-gradient table.
  *
  * Every function cites the reference file:line it restates.  Paths are
  * relative to the reference project root; HFS = hybridFastSummation/

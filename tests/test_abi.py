@@ -63,3 +63,15 @@ def test_every_package_module_imports_without_gpu():
     import importlib
     for m in ("potential", "render", "replicas", "server", "frames", "workloads", "_lib"):
         importlib.import_module("pppm_vortex_bouyant_flow_sample_b200." + m)
+
+
+def test_reference_gpu_checker_exports():
+    """The reference's own kernels, built as a checker (oracle/_ref), load on
+    the host and export the two shim entry points the GPU tests call."""
+    import ctypes
+    from oracle import pyref_gpu
+    if not pyref_gpu.available():
+        import pytest
+        pytest.skip("oracle/_ref/librefgpu.so not built (the reference's sources were absent)")
+    lib = ctypes.CDLL(pyref_gpu._LIB_PATH)
+    assert hasattr(lib, "refgpu_farfield_eval") and hasattr(lib, "refgpu_hash")

@@ -1,0 +1,143 @@
+"""Pin of the oracle and of the product against the reference's own GPU kernels.
+
+oracle/_ref/librefgpu.so is hybridFastSummation/GPU_kernel.cu and
+particle_hash/particle_hash_kernel.cu compiled from the reference's sources
+for sm_100a (`make -C oracle refgpu`).  The hash shim runs calcHashD, the
+stable key sort and FindCellStartD; the velocity shim runs ParticleToMesh,
+getCurl, BiotSavartComputeFarField, BiotSavartInterpolateFarField and
+BiotSavartPPCorrScaleMN in the order of
+BiotSavartSolver::computeFarFieldBuffer + evaluateVelocity.  Its multigrid
+cannot be built (texture references, removed in CUDA 12), so psi is the
+oracle's; the sorted vortices and cell tables are the oracle's too (pinned by
+the hash known-answer tests).  Every stage of the reference is compared with
+the oracle's FP64 restatement, and the final velocities with this build's
+CUDA path (north-star tolerance 1e-5).
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+VEL_TOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def refgpu():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from oracle import pyref_gpu
+    if not pyref_gpu.available():
+        pytest.skip("oracle/_ref/librefgpu.so not built (the reference's sources were absent)")
+    return pyref_gpu
+
+
+@pytest.fixture(scope="module")
+def pb():
+    import pppm_vortex_bouyant_flow_sample_b200 as pb
+    pb.load()
+    return pb
+
+
+def _points(kind, N, seed):
+    from pppm_vortex_bouyant_flow_sample_b200 import workloads as W
+    return W.make_scene(kind, N, seed)
+
+
+@pytest.mark.parametrize("kind,n,N,K,mode", [
+    ("cloud", 32, 16384, 1, "self"),     # the CPU-runnable configuration's shape
+    ("ring", 64, 40000, 1, "self"),
+    ("cloud", 32, 8000, 0, "points"),
+    ("cloud", 32, 8000, 2, "segments"),
+    ("ring", 32, 12000, -1, "self"),
+])
+def test_reference_kernels(refgpu, pb, oracle, kind, n, N, K, mode):
+    import torch
+    pos, al = _points(kind, N, seed=50 + n + K)
+    rng = np.random.default_rng(60 + N)
+    if mode == "self":
+        ea, eb, seg = pos, pos, 1
+    elif mode == "points":
+        ea = np.zeros((6000, 4), np.float32)
+        ea[:, :3] = pos[rng.integers(0, N, 6000), :3] + rng.normal(0, 0.02, (6000, 3)).astype(np.float32)
+        eb, seg = None, 0
+    else:
+        ea = pos.copy()
+        eb = pos.copy()
+        eb[:, :3] += rng.normal(0, 0.01, (N, 3)).astype(np.float32)
+        seg = 1
+    prm = oracle.params(n, K=K)
+    ref_o, d = oracle.pppm(prm, pos, al, ea, eb, seg, dump=True)
+    idx = d["vort_idx"]
+    R = refgpu.farfield_eval(n, K, pos[idx], al[idx], d["cell_start"], d["cell_end"], d["psi"], d["origin"],
+                             float(d["h_f"][0]), ea, eb, seg)
+    # the reference's stages against the oracle's restatement (FP64 both)
+    assert rel_l2(R["vort"], d["grid_vort"]) <= 1e-14
+    assert rel_l2(R["curl"], d["grid_u"]) <= 1e-14
+    assert rel_l2(R["far"], d["far_u"]) <= 1e-13
+    assert rel_l2(R["far_at"], d["u_far_only"]) <= 1e-13
+    assert rel_l2(R["uvw"].T, ref_o) <= 1e-12
+    # this build's CUDA path against the reference's kernels
+    scene = pb.Scene(n, K=K, cap_vort=N, cap_eval=len(ea))
+    dpos = torch.from_numpy(pos).cuda()
+    scene.set_vortices(dpos, torch.from_numpy(np.ascontiguousarray(al)).cuda())
+    scene.build_far_field()
+    dea = torch.from_numpy(np.ascontiguousarray(ea)).cuda()
+    deb = torch.from_numpy(np.ascontiguousarray(eb)).cuda() if eb is not None else None
+    u = scene.eval(dea, deb if seg == 1 else None, seg).cpu().numpy()
+    scene.close()
+    assert rel_l2(u, R["uvw"].T) <= VEL_TOL
+
+
+def _hash_case(kind, N, seed):
+    import os
+    if kind == "kat":
+        d = np.load(os.path.join(os.path.dirname(__file__), "golden", "hash_kat.npz"))
+        return d["pos"], int(d["n"]), float(d["h"]), d["origin"], d["keys"]
+    pos, _ = _points(kind, N, seed)
+    return pos, None, None, None, None
+
+
+@pytest.mark.parametrize("kind,n,N", [("kat", 16, 0), ("cloud", 32, 20000), ("ring", 64, 50000),
+                                      ("cloud", 48, 30000)])
+def test_reference_hash(refgpu, pb, oracle, kind, n, N):
+    """The reference's hash, sort and cell tables against the oracle's (and the
+    golden keys of particles on cell faces and 1 ulp either side) and against
+    this build's hash: both the scene's own (3 x bbox domain) and the
+    ParticleManager mirror with an explicit cell size and origin."""
+    import torch
+    pos, n_kat, h_kat, o_kat, keys_kat = _hash_case(kind, N, seed=70 + n)
+    if kind == "kat":
+        n, h, origin = n_kat, h_kat, o_kat
+    else:
+        _, d = oracle.pppm(oracle.params(n), pos, np.zeros((len(pos), 3)), pos[:1], None, 0, dump=True)
+        h, origin = float(d["h_f"][0]), d["origin"].astype(np.float32)
+    rk, ri, rs, re = refgpu.hash_particles(n, h, origin, pos)
+    occupied = rs != 0xFFFFFFFF
+    if kind == "kat":
+        assert np.array_equal(np.sort(keys_kat), rk)
+    else:
+        assert np.array_equal(rk, d["vort_key"]) and np.array_equal(ri, d["vort_idx"])
+        assert np.array_equal(rs, d["cell_start"])
+        assert np.array_equal(re[occupied], d["cell_end"][occupied])
+        scene = pb.Scene(n, cap_vort=len(pos), cap_eval=1)
+        scene.set_vortices(torch.from_numpy(pos).cuda(), torch.zeros((len(pos), 3), dtype=torch.float64).cuda())
+        scene.build_far_field()
+        k, i = scene.sorted_index()
+        s, e = scene.cell_tables()
+        scene.close()
+        assert np.array_equal(k.numpy(), rk.astype(np.int64)) and np.array_equal(i.numpy(), ri.astype(np.int64))
+        assert np.array_equal(s.numpy(), rs.astype(np.int64))
+        assert np.array_equal(e.numpy()[occupied], re[occupied].astype(np.int64))
+    pm = pb.ParticleManager()
+    pm.initSpatialHash(len(pos), n, n, n)
+    pm.setSpatialHashGrid(n, h, tuple(float(v) for v in origin), len(pos))
+    pm.setHashParam()
+    pm.doSpatialHash(torch.from_numpy(np.ascontiguousarray(pos)).cuda(), len(pos))
+    assert np.array_equal(pm.getHashTable().numpy(), rk.astype(np.int64))
+    assert np.array_equal(pm.getIndexTable().numpy(), ri.astype(np.int64))
+    assert np.array_equal(pm.getStartTable().numpy(), rs.astype(np.int64))
+    assert np.array_equal(pm.getEndTable().numpy()[occupied], re[occupied].astype(np.int64))
+    pm.endSpatialHash()
