@@ -28,9 +28,10 @@ struct Buf {
 // pos4: N float4 positions; n: grid edge; h, origin: the float cell size and
 // origin.  Outputs (host): keys and indices after the sort (N each), cellStart
 // and cellEnd (n^3 each; cellEnd is written for occupied cells only, as in the
-// reference: the caller pre-fills it).  Returns 0 or a CUDA error code.
+// reference: the caller pre-fills it); ms (may be NULL): device time of the
+// three steps by CUDA events.  Returns 0 or a CUDA error code.
 extern "C" int refgpu_hash(uint32_t n, float h, const float origin[3], uint32_t N, const float *pos4,
-                           uint32_t *keys, uint32_t *index, uint32_t *cell_start, uint32_t *cell_end) {
+                           uint32_t *keys, uint32_t *index, uint32_t *cell_start, uint32_t *cell_end, float *ms) {
     const size_t C = (size_t)n * n * n;
     HashParams hp = {};
     hp.gridSize = make_uint3(n, n, n);
@@ -49,6 +50,10 @@ extern "C" int refgpu_hash(uint32_t n, float h, const float origin[3], uint32_t 
     if (e != cudaSuccess) return (int)e;
     uint *hash = static_cast<uint *>(d_hash.p), *idx = static_cast<uint *>(d_idx.p);
     const uint threads = 256, blocks = (N + threads - 1) / threads;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0);
     if (N) calcHashD<<<blocks, threads>>>(hash, idx, static_cast<float4 *>(d_pos.p), N);
     e = cudaGetLastError();
     if (e == cudaSuccess && N) {
@@ -60,7 +65,13 @@ extern "C" int refgpu_hash(uint32_t n, float h, const float origin[3], uint32_t 
     if (e == cudaSuccess && N)
         FindCellStartD<<<blocks, threads, (threads + 1) * sizeof(uint)>>>(static_cast<uint *>(d_start.p),
                                                                           static_cast<uint *>(d_end.p), hash, idx, N);
+    cudaEventRecord(e1);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    float t = 0.f;
+    cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (ms) *ms = t;
     if (e == cudaSuccess) e = cudaMemcpy(keys, hash, sizeof(uint) * N, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(index, idx, sizeof(uint) * N, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(cell_start, d_start.p, sizeof(uint) * C, cudaMemcpyDeviceToHost);

@@ -114,7 +114,7 @@ def test_reference_hash(refgpu, pb, oracle, kind, n, N):
     else:
         _, d = oracle.pppm(oracle.params(n), pos, np.zeros((len(pos), 3)), pos[:1], None, 0, dump=True)
         h, origin = float(d["h_f"][0]), d["origin"].astype(np.float32)
-    rk, ri, rs, re = refgpu.hash_particles(n, h, origin, pos)
+    rk, ri, rs, re, _ = refgpu.hash_particles(n, h, origin, pos)
     occupied = rs != 0xFFFFFFFF
     if kind == "kat":
         assert np.array_equal(np.sort(keys_kat), rk)

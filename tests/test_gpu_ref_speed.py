@@ -1,0 +1,88 @@
+"""This build's path against the reference's own CUDA kernels on the same B200.
+
+The reference's hash, P2M, curl, far-field, interpolation and near-field
+kernels (oracle/_ref/librefgpu.so, compiled from its sources for sm_100a) run
+on the at-scale workload, a 1,048,576-particle vortex ring on 128^3 with the
+velocity at every particle, fed with this build's sorted vortices, cell tables
+and potential (the stage-by-stage equality of those inputs is
+tests/test_gpu_ref_kernels.py).  Device times by CUDA events, after a warm-up
+pass, against this build's stage times on the same scene.  The multigrid is
+left out of both sides: the reference's cannot be built (texture references).
+With PPPM_TIMING_OUT set, the table is also written there as JSON.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def refgpu():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from oracle import pyref_gpu
+    if not pyref_gpu.available():
+        pytest.skip("oracle/_ref/librefgpu.so not built (the reference's sources were absent)")
+    return pyref_gpu
+
+
+def test_path_outruns_reference_kernels(refgpu):
+    import torch
+    import pppm_vortex_bouyant_flow_sample_b200 as pb
+    from pppm_vortex_bouyant_flow_sample_b200 import workloads as W
+    pb.load()
+    N, n, K = 1 << 20, 128, 1
+    pos, al = W.vortex_ring(N, seed=1)
+    scene = pb.Scene(n, K=K, cap_vort=N, cap_eval=N)
+    dpos = torch.from_numpy(pos).cuda()
+    dal = torch.from_numpy(np.ascontiguousarray(al)).cuda()
+    out = torch.empty((3, N), dtype=torch.float64, device="cuda")
+    for _ in range(3):
+        scene.set_vortices(dpos, dal)
+        scene.build_far_field()
+        scene.eval(dpos, dpos, 1, out=out)
+    torch.cuda.synchronize()
+    scene.set_profiling(True)
+    ours = []
+    for _ in range(5):
+        scene.set_vortices(dpos, dal)
+        scene.build_far_field()
+        scene.eval(dpos, dpos, 1, out=out)
+        torch.cuda.synchronize()
+        ours.append(scene.stage_times())
+    scene.set_profiling(False)
+    mine = {k: float(np.median([t[k] for t in ours])) for k in ours[0] if ours[0][k] >= 0}
+    origin, L, h = scene.domain()
+    spos, sal = scene.sorted_vortices()
+    start, end = scene.cell_tables()
+    psi = scene.grid(pb.GRID_PSI).numpy()
+    u_ours = out.t().cpu().numpy()
+    scene.close()
+    spos = spos.cpu().numpy()
+    sal = sal.cpu().numpy().T
+    start = start.numpy().astype(np.uint32)
+    end = end.numpy().astype(np.uint32)
+    ref = None
+    for _ in range(2):  # the first pass warms the reference's kernels up
+        ref = refgpu.farfield_eval(n, K, spos, sal, start, end, psi, np.asarray(origin), h, pos, pos, 1)
+    hash_ms = min(refgpu.hash_particles(n, np.float32(h), np.asarray(origin, np.float32), pos)[4]
+                  for _ in range(2))
+    theirs = dict(ref["stage_ms"], hash=hash_ms)
+    t_ref = sum(theirs.values())
+    t_ours = sum(v for k, v in mine.items() if k != "multigrid")
+    rel = float(np.linalg.norm(u_ours - ref["uvw"].T) / np.linalg.norm(ref["uvw"]))
+    table = {"workload": f"vortex ring, {N:,} particles, {n}^3, K={K}, velocity at every particle",
+             "reference_kernels_ms": theirs, "reference_total_ms": t_ref,
+             "this_build_ms": mine, "this_build_total_without_multigrid_ms": t_ours,
+             "speedup_without_multigrid": t_ref / t_ours, "rel_l2_velocity_vs_reference_kernels": rel}
+    print(json.dumps(table, indent=1))
+    dest = os.environ.get("PPPM_TIMING_OUT")
+    if dest:
+        with open(dest, "w") as f:
+            json.dump(table, f, indent=1)
+    assert rel <= 1e-5
+    assert t_ours < t_ref
