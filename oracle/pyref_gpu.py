@@ -45,6 +45,14 @@ def lib():
         L.refgpu_farfield_eval.restype = C.c_int
         L.refgpu_hash.argtypes = [C.c_uint32, C.c_float, f32p, C.c_uint32, f32p, u32p, u32p, u32p, u32p, f32p]
         L.refgpu_hash.restype = C.c_int
+        L.refgpu_segments.argtypes = [C.c_uint32, f32p, f64p, C.c_double, f32p, f32p, f64p]
+        L.refgpu_segment_update.argtypes = [C.c_uint32, f32p, f32p, f64p, f64p, f64p, f64p, C.c_double, f32p, f64p]
+        L.refgpu_gaussian_smooth.argtypes = [C.c_uint32, C.c_double, f64p, C.c_uint32, f32p, f32p, u32p, u32p, f64p,
+                                             C.c_double, C.c_double, f64p]
+        L.refgpu_baroclinic.argtypes = [C.c_uint32, C.c_double, C.c_float, f64p, C.c_uint32, f32p, f32p, u32p, u32p,
+                                        C.c_uint32, f32p, f64p, C.c_double, f32p, f32p]
+        for name in ("refgpu_segments", "refgpu_segment_update", "refgpu_gaussian_smooth", "refgpu_baroclinic"):
+            getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
 
@@ -79,10 +87,10 @@ def farfield_eval(n, K, sorted_pos4, sorted_alpha, start, end, psi, origin, cell
     return res
 
 
-def hash_particles(n, h, origin, pos4):
+def hash_particles(n, h, origin, pos4, end_fill=0xFFFFFFFF):
     """The reference's calcHashD, stable key sort and FindCellStartD for float
     cell size h and float origin.  Returns (sorted keys, sorted indices,
-    cellStart, cellEnd, milliseconds); cellEnd holds 0xFFFFFFFF where the
+    cellStart, cellEnd, milliseconds); cellEnd holds end_fill where the
     reference leaves it unwritten (empty cells)."""
     pos = np.ascontiguousarray(pos4, dtype=np.float32)
     N = len(pos)
@@ -90,10 +98,74 @@ def hash_particles(n, h, origin, pos4):
     keys = np.zeros(N, np.uint32)
     idx = np.zeros(N, np.uint32)
     start = np.zeros(Cn, np.uint32)
-    end = np.full(Cn, 0xFFFFFFFF, np.uint32)
+    end = np.full(Cn, end_fill, np.uint32)
     ms = np.zeros(1, np.float32)
     rc = lib().refgpu_hash(n, C.c_float(h), np.ascontiguousarray(origin, dtype=np.float32), N, pos, keys, idx,
                            start, end, ms)
     if rc != 0:
         raise RuntimeError(f"refgpu_hash: CUDA error {rc}")
     return keys, idx, start, end, float(ms[0])
+
+
+def _check(rc, name):
+    if rc != 0:
+        raise RuntimeError(f"{name}: error {rc}")
+
+
+def _soa(a, N):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(N, 3).T)
+
+
+def segments(cent4, alpha3, h_seg):
+    """ComputePosb: (enda4, endb4, kappa)."""
+    cent = np.ascontiguousarray(cent4, dtype=np.float32)
+    N = len(cent)
+    ea = np.zeros((N, 4), np.float32)
+    eb = np.zeros((N, 4), np.float32)
+    k = np.zeros(N)
+    _check(lib().refgpu_segments(N, cent, _soa(alpha3, N), float(h_seg), ea, eb, k), "refgpu_segments")
+    return ea, eb, k
+
+
+def segment_update(enda4, endb4, alpha3, kappa, ua3, ub3, dt):
+    """move_particle on both ends, ComputePosa, ComputeVortex, VectorAdd:
+    (moved enda4, moved endb4, centres4, strengths to smooth (N, 3))."""
+    ea = np.array(enda4, dtype=np.float32, order="C", copy=True)
+    eb = np.array(endb4, dtype=np.float32, order="C", copy=True)
+    N = len(ea)
+    cent = np.zeros((N, 4), np.float32)
+    dv = np.zeros(3 * N)
+    _check(lib().refgpu_segment_update(N, ea, eb, _soa(alpha3, N), np.ascontiguousarray(kappa, dtype=np.float64),
+                                       _soa(ua3, N), _soa(ub3, N), float(dt), cent, dv), "refgpu_segment_update")
+    return ea, eb, cent, dv.reshape(3, N).T.copy()
+
+
+def gaussian_smooth(n, cell_h, origin, cent4, sorted_cent4, start, end, sorted_d3, nu, dt):
+    """ParticleGaussianSmooth: smoothed strengths (N, 3) in caller order."""
+    cent = np.ascontiguousarray(cent4, dtype=np.float32)
+    N = len(cent)
+    out = np.zeros(3 * N)
+    _check(lib().refgpu_gaussian_smooth(n, float(cell_h), np.ascontiguousarray(origin, dtype=np.float64), N, cent,
+                                        np.ascontiguousarray(sorted_cent4, dtype=np.float32),
+                                        np.ascontiguousarray(start, dtype=np.uint32),
+                                        np.ascontiguousarray(end, dtype=np.uint32), _soa(sorted_d3, N), float(nu),
+                                        float(dt), out), "refgpu_gaussian_smooth")
+    return out.reshape(3, N).T.copy()
+
+
+def baroclinic(dim, h, h_f, origin, sorted_heat4, sorted_heat, start, end, cent4, alpha3, dt):
+    """AssignDensity, GradDensity, ParticleGetBaroclinic: (alpha (N, 3),
+    rho (dim^3,), grad (dim^3, 3))."""
+    cent = np.ascontiguousarray(cent4, dtype=np.float32)
+    N = len(cent)
+    al = _soa(alpha3, N)
+    c = dim ** 3
+    rho = np.zeros(c, np.float32)
+    grad = np.zeros(3 * c, np.float32)
+    hp = np.ascontiguousarray(sorted_heat4, dtype=np.float32)
+    _check(lib().refgpu_baroclinic(dim, float(h), C.c_float(h_f), np.ascontiguousarray(origin, dtype=np.float64),
+                                   len(hp), hp, np.ascontiguousarray(sorted_heat, dtype=np.float32),
+                                   np.ascontiguousarray(start, dtype=np.uint32),
+                                   np.ascontiguousarray(end, dtype=np.uint32), N, cent, al, float(dt), rho, grad),
+           "refgpu_baroclinic")
+    return al.T.copy(), rho, grad.reshape(3, c).T.copy()

@@ -147,3 +147,136 @@ extern "C" int refgpu_farfield_eval(uint32_t n, int K, uint32_t N, const float *
     if (e == cudaSuccess) e = cudaMemcpy(uvw, u, sizeof(double) * 3 * M, cudaMemcpyDeviceToHost);
     return (int)e;
 }
+
+// convertVortToSeg (HFS/VortexSimulationSystemImp.cpp:126-137): ComputePosb on
+// the centres.  Outputs the two ends (enda = c - s/2, endb = c + s/2) and kappa.
+extern "C" int refgpu_segments(uint32_t N, const float *cent4, const double *alpha, double h_seg, float *enda4,
+                               float *endb4, double *kappa) {
+    DevBuf d_c, d_a, d_b, d_al, d_k;
+    cudaError_t e = upload(d_c, cent4, 4 * (size_t)N);
+    if (e == cudaSuccess) e = upload(d_al, alpha, 3 * (size_t)N);
+    if (e == cudaSuccess) e = upload<float>(d_a, nullptr, 4 * (size_t)N);
+    if (e == cudaSuccess) e = upload<float>(d_b, nullptr, 4 * (size_t)N);
+    if (e == cudaSuccess) e = upload<double>(d_k, nullptr, N);
+    if (e != cudaSuccess) return (int)e;
+    double *al = ptr<double>(d_al);
+    ComputePosb(ptr<float4>(d_c), ptr<float4>(d_a), ptr<float4>(d_b), al, al + N, al + 2 * (size_t)N,
+                ptr<double>(d_k), h_seg, N);
+    e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(enda4, d_a.p, sizeof(float4) * N, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(endb4, d_b.p, sizeof(float4) * N, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(kappa, d_k.p, sizeof(double) * N, cudaMemcpyDeviceToHost);
+    return (int)e;
+}
+
+// applyFlow + convertSegToVort + the first VectorAdd of computeStretching
+// (HFS/VortexSimulationSystemImp.cpp:277-297, 315-330, 470-478): move both
+// ends by their velocities ua / ub (3 x N; packed as the double4 of
+// AddURotation), centres as the ends' midpoints (ComputePosa), then
+// dv = kappa (endb - enda) - alpha (ComputeVortex) and dv = alpha + dv.
+// enda4 / endb4 are moved in place.
+extern "C" int refgpu_segment_update(uint32_t N, float *enda4, float *endb4, const double *alpha, const double *kappa,
+                                     const double *ua, const double *ub, double dt, float *cent4, double *dv) {
+    double4 *hua = new double4[N ? N : 1], *hub = new double4[N ? N : 1];
+    for (uint32_t t = 0; t < N; t++) {
+        hua[t] = make_double4(ua[t], ua[N + t], ua[2 * (size_t)N + t], 0.0);
+        hub[t] = make_double4(ub[t], ub[N + t], ub[2 * (size_t)N + t], 0.0);
+    }
+    DevBuf d_a, d_b, d_c, d_al, d_k, d_ua, d_ub, d_dv;
+    cudaError_t e = upload(d_a, enda4, 4 * (size_t)N);
+    if (e == cudaSuccess) e = upload(d_b, endb4, 4 * (size_t)N);
+    if (e == cudaSuccess) e = upload<float>(d_c, nullptr, 4 * (size_t)N);
+    if (e == cudaSuccess) e = upload(d_al, alpha, 3 * (size_t)N);
+    if (e == cudaSuccess) e = upload(d_k, kappa, N);
+    if (e == cudaSuccess) e = upload(d_ua, hua, N);
+    if (e == cudaSuccess) e = upload(d_ub, hub, N);
+    if (e == cudaSuccess) e = upload<double>(d_dv, nullptr, 3 * (size_t)N);
+    delete[] hua;
+    delete[] hub;
+    if (e != cudaSuccess) return (int)e;
+    float4 *a = ptr<float4>(d_a), *b = ptr<float4>(d_b), *c = ptr<float4>(d_c);
+    double *al = ptr<double>(d_al), *v = ptr<double>(d_dv);
+    move_particle(a, dt, ptr<double4>(d_ua), N);
+    move_particle(b, dt, ptr<double4>(d_ub), N);
+    ComputePosa(a, b, c, N);
+    ComputeVortex(a, b, al, al + N, al + 2 * (size_t)N, v, v + N, v + 2 * (size_t)N, ptr<double>(d_k), N);
+    for (int q = 0; q < 3; q++) VectorAdd(al + q * (size_t)N, v + q * (size_t)N, v + q * (size_t)N, 1, 1, N);
+    e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(enda4, a, sizeof(float4) * N, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(endb4, b, sizeof(float4) * N, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(cent4, c, sizeof(float4) * N, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(dv, v, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost);
+    return (int)e;
+}
+
+// computeStretching's smoothing (HFS/VortexSimulationSystemImp.cpp:492-509):
+// ParticleGaussianSmooth with the centres in caller order, the centres and the
+// strengths sorted by cell, the cell tables, the solver's cell size and origin.
+// out (3 x N) receives the smoothed strengths in caller order.
+extern "C" int refgpu_gaussian_smooth(uint32_t n, double cell_h, const double origin3[3], uint32_t N,
+                                      const float *cent4, const float *scent4, const uint32_t *start,
+                                      const uint32_t *end, const double *sdv, double nu, double dt, double *out) {
+    const size_t C = (size_t)n * n * n;
+    DevBuf d_c, d_sc, d_s, d_e, d_in, d_out;
+    cudaError_t e = upload(d_c, cent4, 4 * (size_t)N);
+    if (e == cudaSuccess) e = upload(d_sc, scent4, 4 * (size_t)N);
+    if (e == cudaSuccess) e = upload(d_s, start, C);
+    if (e == cudaSuccess) e = upload(d_e, end, C);
+    if (e == cudaSuccess) e = upload(d_in, sdv, 3 * (size_t)N);
+    if (e == cudaSuccess) e = upload<double>(d_out, nullptr, 3 * (size_t)N);
+    if (e != cudaSuccess) return (int)e;
+    double *in = ptr<double>(d_in), *o = ptr<double>(d_out);
+    ParticleGaussianSmooth(ptr<uint32_t>(d_s), ptr<uint32_t>(d_e), ptr<float4>(d_c), ptr<float4>(d_sc), nu, dt, o,
+                           o + N, o + 2 * (size_t)N, in, in + N, in + 2 * (size_t)N, cell_h, make_uint3(n, n, n), N,
+                           make_double4(origin3[0], origin3[1], origin3[2], 0.0));
+    e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(out, o, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost);
+    return (int)e;
+}
+
+// addBaroclinicForce's device part (HFS/VortexSimulationSystemImp.cpp:412-446):
+// AssignDensity on the heat particles sorted by density cell (sheat4, sheat,
+// start, end), GradDensity, ParticleGetBaroclinic with dt_beta = 5 dt.  dim,
+// h (double, L / dim), hf (the hash's float cell size) and origin3 describe
+// the density grid.  alpha (3 x N) is updated in place; rho (dim^3) and grad
+// (3 x dim^3, component planes) receive the grids.  ParticleGetBaroclinic
+// launches 256 blocks of N/256 + 1 threads (its block and grid sizes swapped),
+// which covers every vortex while N/256 + 1 <= 1024.
+extern "C" int refgpu_baroclinic(uint32_t dim, double h, float hf, const double origin3[3], uint32_t H,
+                                 const float *sheat4, const float *sheat, const uint32_t *start, const uint32_t *end,
+                                 uint32_t N, const float *cent4, double *alpha, double dt, float *rho, float *grad) {
+    if (N / 256 + 1 > 1024) return -1;
+    const size_t C = (size_t)dim * dim * dim;
+    DevBuf d_hp, d_h, d_s, d_e, d_rho, d_grad, d_c, d_al;
+    cudaError_t e = upload(d_hp, sheat4, 4 * (size_t)H);
+    if (e == cudaSuccess) e = upload(d_h, sheat, H);
+    if (e == cudaSuccess) e = upload(d_s, start, C);
+    if (e == cudaSuccess) e = upload(d_e, end, C);
+    if (e == cudaSuccess) e = upload<float>(d_rho, nullptr, C);
+    if (e == cudaSuccess) e = upload<float>(d_grad, nullptr, 3 * C);
+    if (e == cudaSuccess) e = upload(d_c, cent4, 4 * (size_t)N);
+    if (e == cudaSuccess) e = upload(d_al, alpha, 3 * (size_t)N);
+    if (e != cudaSuccess) return (int)e;
+    const double4 origin = make_double4(origin3[0], origin3[1], origin3[2], 0.0);
+    const uint3 gd = make_uint3(dim, dim, dim);
+    float *heat = ptr<float>(d_h);
+    AssignDensity(ptr<uint32_t>(d_s), ptr<uint32_t>(d_e), ptr<float4>(d_hp), heat, heat, h, ptr<float>(d_rho), gd, gd,
+                  H, origin);
+    float3 *g3 = ptr<float3>(d_grad);
+    GradDensity(ptr<float>(d_rho), g3, h, dim, dim, dim);
+    double *al = ptr<double>(d_al);
+    ParticleGetBaroclinic(ptr<float4>(d_c), al, al + N, al + 2 * (size_t)N, g3, dt * 5.0, N, dim, dim, dim,
+                          1.0 / (double)hf, origin);
+    e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(rho, d_rho.p, sizeof(float) * C, cudaMemcpyDeviceToHost);
+    float3 *hg = new float3[C ? C : 1];
+    if (e == cudaSuccess) e = cudaMemcpy(hg, g3, sizeof(float3) * C, cudaMemcpyDeviceToHost);
+    for (size_t c = 0; e == cudaSuccess && c < C; c++) {
+        grad[c] = hg[c].x;
+        grad[C + c] = hg[c].y;
+        grad[2 * C + c] = hg[c].z;
+    }
+    delete[] hg;
+    if (e == cudaSuccess) e = cudaMemcpy(alpha, al, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost);
+    return (int)e;
+}

@@ -141,3 +141,82 @@ def test_reference_hash(refgpu, pb, oracle, kind, n, N):
     assert np.array_equal(pm.getStartTable().numpy(), rs.astype(np.int64))
     assert np.array_equal(pm.getEndTable().numpy()[occupied], re[occupied].astype(np.int64))
     pm.endSpatialHash()
+
+
+@pytest.mark.parametrize("kind,n,N,h_seg", [("ring", 32, 8000, 0.1), ("cloud", 64, 3000, 0.1),
+                                            ("ring", 32, 6000, 7.852e-5)])
+def test_reference_vortex_step(refgpu, pb, oracle, kind, n, N, h_seg):
+    """The reference's segment step chained from its own kernels: ComputePosb,
+    velocities at both ends (P2M ... near field, with the oracle's psi),
+    move_particle, ComputePosa, ComputeVortex + VectorAdd, its hash of the new
+    centres and ParticleGaussianSmooth; against the oracle's orc_vortex_step
+    and this build's pppm_vortex_step."""
+    import torch
+    pos, al = _points(kind, N, seed=80 + n)
+    if kind == "cloud":
+        al = al * 1e-3
+    dt, nu = 0.01, 0.1
+    prm = oracle.params(n)
+    rc, ra, rea, reb = oracle.vortex_step(prm, pos, al, dt, h_seg=h_seg, nu=nu)
+    ea0, eb0, kappa = refgpu.segments(pos, al, h_seg)
+    _, _, oea0, oeb0 = oracle.vortex_step(prm, pos, al, 0.0, h_seg=h_seg, nu=nu)
+    assert np.array_equal(ea0[:, :3], oea0[:, :3]) and np.array_equal(eb0[:, :3], oeb0[:, :3])
+    _, d = oracle.pppm(prm, pos, al, pos[:1], None, 0, dump=True)
+    idx = d["vort_idx"]
+    args = (n, 1, pos[idx], al[idx], d["cell_start"], d["cell_end"], d["psi"], d["origin"], float(d["h_f"][0]))
+    ub = refgpu.farfield_eval(*args, eb0, pos, 1)["uvw"].T
+    ua = refgpu.farfield_eval(*args, ea0, pos, 1)["uvw"].T
+    ea1, eb1, cent1, dv = refgpu.segment_update(ea0, eb0, al, kappa, ua, ub, dt)
+    # FP64 velocities agree to round-off, so the float ends and centres agree to an ulp
+    for got, ref in ((ea1, rea), (eb1, reb), (cent1, rc)):
+        assert np.max(np.abs(got[:, :3] - ref[:, :3])) <= 4 * np.finfo(np.float32).eps * np.abs(ref[:, :3]).max()
+    o1, L1 = oracle.set_domain(cent1)
+    h1, of1 = oracle.hash_params(o1, L1, n)
+    _, sidx, s1, e1, _ = refgpu.hash_particles(n, h1, of1, cent1)
+    smooth = refgpu.gaussian_smooth(n, float(h1), o1, cent1, cent1[sidx], s1, e1, dv[sidx], nu, dt)
+    assert rel_l2(smooth, ra) <= 1e-9
+    scene = pb.Scene(n, cap_vort=N, cap_eval=2 * N)
+    dpos = torch.from_numpy(pos.copy()).cuda()
+    dal = torch.from_numpy(np.ascontiguousarray(al)).cuda()
+    scene.vortex_step(dpos, dal, dt, h_seg=h_seg, nu=nu)
+    scene.close()
+    assert rel_l2(dal.cpu().numpy(), smooth) <= 1e-4
+    disp_g = dpos.cpu().numpy()[:, :3].astype(np.float64) - pos[:, :3]
+    disp_r = cent1[:, :3].astype(np.float64) - pos[:, :3]
+    assert rel_l2(disp_g, disp_r) <= 1e-4
+
+
+@pytest.mark.parametrize("H,radius,N", [(200000, 0.35, 20000), (60000, 1.0, 20000), (30000, 0.5, 5000)])
+def test_reference_baroclinic(refgpu, pb, oracle, H, radius, N):
+    """The reference's AssignDensity, GradDensity and ParticleGetBaroclinic on
+    its own hash of the heat particles (empty cells' cellEnd as a fresh
+    allocation leaves it: zero); against orc_baroclinic and pppm_baroclinic."""
+    import torch
+    rng = np.random.default_rng(90 + N)
+    v = rng.normal(0, 1, (H, 3))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    heat4 = np.zeros((H, 4), np.float32)
+    heat4[:, :3] = np.array([0.5, 0.15, 0.5]) + v * (radius * rng.uniform(0, 1, H) ** (1 / 3))[:, None]
+    heat = rng.normal(1.0, 0.05, H).astype(np.float32)
+    cent = np.zeros((N, 4), np.float32)
+    cent[:, :3] = heat4[rng.integers(0, H, N), :3] + rng.normal(0, 0.02 * radius, (N, 3)).astype(np.float32)
+    al = rng.normal(0, 1e-4, (N, 3))
+    dt = 0.002
+    ra, dim, origin, h, rrho, rgrad = oracle.baroclinic(heat4, heat, cent, al, dt, cap=201 ** 3)
+    h_f = np.float32(h)
+    _, hidx, hs, he, _ = refgpu.hash_particles(dim, h_f, origin.astype(np.float32), heat4, end_fill=0)
+    R_al, R_rho, R_grad = refgpu.baroclinic(dim, h, h_f, origin, heat4[hidx], heat[hidx], hs, he, cent, al, dt)
+    scale = np.abs(rrho).max()
+    assert np.max(np.abs(R_rho - rrho)) <= 4 * np.finfo(np.float32).eps * scale
+    assert np.max(np.abs(R_grad - rgrad)) <= 4 * np.finfo(np.float32).eps * scale / h
+    assert np.linalg.norm(ra - al) > 0
+    assert rel_l2(R_al - al, ra - al) <= 1e-6
+    scene = pb.Scene(32, cap_vort=N, cap_eval=N)
+    dal = torch.from_numpy(al.copy()).cuda()
+    scene.baroclinic(torch.from_numpy(heat4).cuda(), torch.from_numpy(heat).cuda(), torch.from_numpy(cent).cuda(),
+                     dal, dt)
+    gdim, _, _, grho, _ = scene.density()
+    scene.close()
+    assert gdim == dim
+    assert np.max(np.abs(grho.numpy() - R_rho)) <= 4 * np.finfo(np.float32).eps * scale
+    assert rel_l2(dal.cpu().numpy() - al, R_al - al) <= 1e-5
