@@ -13,8 +13,8 @@
  * whole solver cannot be built (the multigrid's host wrappers include GL
  * headers, its kernels use the texture-reference API that CUDA 12 removed).
  * Its hash kernels (particle_hash_kernel.cu) and its P2M, curl, far-field,
- * interpolation, near-field, segment, move, smoothing, density and baroclinic
- * kernels (GPU_kernel.cu) do build from their sources for sm_100a
+ * interpolation, near-field, segment, move, smoothing, density, baroclinic and
+ * PotentialFieldSolver kernels (GPU_kernel.cu) do build from their sources for sm_100a
  * (`make -C oracle refgpu`, ref_gpu/); the GPU tests run them beside this
  * restatement, stage by stage (tests/test_gpu_ref_kernels.py: keys, order and
  * cell tables bit-exact; grids, velocities and strengths to FP64 round-off).  The multigrid is anchored by known-answer tests instead

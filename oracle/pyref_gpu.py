@@ -51,7 +51,11 @@ def lib():
                                              C.c_double, C.c_double, f64p]
         L.refgpu_baroclinic.argtypes = [C.c_uint32, C.c_double, C.c_float, f64p, C.c_uint32, f32p, f32p, u32p, u32p,
                                         C.c_uint32, f32p, f64p, C.c_double, f32p, f32p]
-        for name in ("refgpu_segments", "refgpu_segment_update", "refgpu_gaussian_smooth", "refgpu_baroclinic"):
+        L.refgpu_potential.argtypes = [C.c_uint32, C.c_int, C.c_uint32, f32p, f64p, f64p, u32p, u32p, f64p, f64p,
+                                       C.c_float, C.c_double, C.c_uint32, f32p, C.c_int, C.c_void_p, C.c_void_p,
+                                       f64p, f64p, f64p, f64p, C.c_void_p]
+        for name in ("refgpu_segments", "refgpu_segment_update", "refgpu_gaussian_smooth", "refgpu_baroclinic",
+                     "refgpu_potential"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -169,3 +173,37 @@ def baroclinic(dim, h, h_f, origin, sorted_heat4, sorted_heat, start, end, cent4
                                    np.ascontiguousarray(end, dtype=np.uint32), N, cent, al, float(dt), rho, grad),
            "refgpu_baroclinic")
     return al.T.copy(), rho, grad.reshape(3, c).T.copy()
+
+
+def potential(n, K, sorted_pos4, sorted_mass, mass, start, end, phi, origin, h_f, L, eval4, scalar=False,
+              normals=None, areas=None):
+    """PotentialFieldSolver's stages with the reference's kernels and the
+    given phi: dict of density, rhs (n^3), far (n^3 or (n^3, 3)), out (M or
+    (M, 3)) and, with normals and areas, dphidn (M)."""
+    pos = np.ascontiguousarray(sorted_pos4, dtype=np.float32)
+    ev = np.ascontiguousarray(eval4, dtype=np.float32)
+    N, M, Cn = len(pos), len(ev), n ** 3
+    out = {"density": np.zeros(Cn), "rhs": np.zeros(Cn), "far": np.zeros(3 * Cn), "out": np.zeros(3 * M)}
+    nrm = ar = dp = None
+    if normals is not None:
+        nrm = np.ascontiguousarray(np.asarray(normals, dtype=np.float64).reshape(M, 3))
+        ar = np.ascontiguousarray(areas, dtype=np.float64)
+        dp = np.zeros(M)
+    ptr = lambda a: None if a is None else a.ctypes.data
+    _check(lib().refgpu_potential(n, K, N, pos, np.ascontiguousarray(sorted_mass, dtype=np.float64),
+                                  np.ascontiguousarray(mass, dtype=np.float64),
+                                  np.ascontiguousarray(start, dtype=np.uint32),
+                                  np.ascontiguousarray(end, dtype=np.uint32),
+                                  np.ascontiguousarray(phi, dtype=np.float64),
+                                  np.ascontiguousarray(origin, dtype=np.float64), C.c_float(h_f), float(L), M, ev,
+                                  int(bool(scalar)), ptr(nrm), ptr(ar), out["density"], out["rhs"], out["far"],
+                                  out["out"], ptr(dp)), "refgpu_potential")
+    if scalar:
+        out["far"] = out["far"][:Cn]
+        out["out"] = out["out"][:M]
+    else:
+        out["far"] = out["far"].reshape(3, Cn).T.copy()
+        out["out"] = out["out"].reshape(3, M).T.copy()
+    if dp is not None:
+        out["dphidn"] = dp
+    return out

@@ -280,3 +280,121 @@ extern "C" int refgpu_baroclinic(uint32_t dim, double h, float hf, const double 
     if (e == cudaSuccess) e = cudaMemcpy(alpha, al, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost);
     return (int)e;
 }
+
+// The scalar wrappers GPU_kernel.cu defines without a declaration in
+// ParticleMesh.h (signatures as defined there).
+void PotentialComputeScalarFarField(double *mass, double *gridval, double *phi, double cell_h, double G,
+                                    double direction, uint3 gdim, uint3 hdim, int K);
+void PotentialInterpolateFarFieldScalar(float4 *pos, double *far_force, double *p_force, double cell_h, uint dimx,
+                                        uint dimy, uint dimz, uint num_particles, double4 origin);
+void Potential_PPCorrMNScalar(uint *start, uint *end, float4 *pos_eval, float4 *pos_mass, double *mass,
+                              double *p_phi, double invh, double h, double G, double direction, uint3 gdim,
+                              uint3 hdim, uint2 gstride, uint2 hstride, int K, uint M, uint N, double4 origin);
+
+// PotentialFieldSolver (HFS/PotentialFieldSolver.cpp:527-608 m_ParticleToMesh,
+// 622-630 m_ComputeGradient, 645-672 computeFarFieldBuffer, 441-525
+// evaluateGradient on unsorted points, 674-679 computeDphiDn, 695-739 the scalar
+// path) with the reference's wrappers; the multigrid's phi comes in.  The
+// masses come sorted by cell (spos4, smass, start, end) as m_ParticleToMesh
+// leaves them, umass in caller order for computeDphiDn.  cell_h is the hash's
+// float cell size, L the domain edge, origin3 the double origin.  Outputs:
+// density, rhs (n^3), far (scalar: n^3; gradient: 3 x n^3 planes), out (M or
+// 3 x M) and, for the gradient with normals, dphidn (M).
+extern "C" int refgpu_potential(uint32_t n, int K, uint32_t N, const float *spos4, const double *smass,
+                                const double *umass, const uint32_t *start, const uint32_t *end, const double *phi,
+                                const double origin3[3], float cell_hf, double L, uint32_t M, const float *eval4,
+                                int scalar, const double *normals, const double *areas, double *density, double *rhs,
+                                double *far, double *out, double *dphidn) {
+    const size_t C = (size_t)n * n * n;
+    const uint3 dim = make_uint3(n, n, n);
+    const double cell_h = (double)cell_hf;
+    const double4 origin = make_double4(origin3[0], origin3[1], origin3[2], 0.0);
+    // monopole of m_ParticleToMesh, summed on the host in the sorted order
+    double tw = 0.0, tm = 0.0, cx = 0.0, cy = 0.0, cz = 0.0;
+    for (uint32_t i = 0; i < N; i++) {
+        tw += fabs(smass[i]);
+        tm += smass[i];
+    }
+    for (uint32_t i = 0; i < N; i++) {
+        cx += spos4[4 * i] * fabs(smass[i]);
+        cy += spos4[4 * i + 1] * fabs(smass[i]);
+        cz += spos4[4 * i + 2] * fabs(smass[i]);
+    }
+    cx /= tw;
+    cy /= tw;
+    cz /= tw;
+    DevBuf d_pos, d_m, d_um, d_s, d_e, d_rho, d_rhs, d_phi, d_g, d_far, d_ev, d_out, d_nrm, d_area, d_dp;
+    cudaError_t e = upload(d_pos, spos4, 4 * (size_t)N);
+    if (e == cudaSuccess) e = upload(d_m, smass, N);
+    if (e == cudaSuccess) e = upload(d_um, umass, N);
+    if (e == cudaSuccess) e = upload(d_s, start, C);
+    if (e == cudaSuccess) e = upload(d_e, end, C);
+    if (e == cudaSuccess) e = upload<double>(d_rho, nullptr, C);
+    if (e == cudaSuccess) e = upload<double>(d_rhs, nullptr, C);
+    if (e == cudaSuccess) e = upload(d_phi, phi, C);
+    if (e == cudaSuccess) e = upload<double>(d_g, nullptr, 3 * C);
+    if (e == cudaSuccess) e = upload<double>(d_far, nullptr, 3 * C);
+    if (e == cudaSuccess) e = upload(d_ev, eval4, 4 * (size_t)M);
+    if (e == cudaSuccess) e = upload<double>(d_out, nullptr, 3 * (size_t)M);
+    if (e != cudaSuccess) return (int)e;
+    uint32_t *st = ptr<uint32_t>(d_s), *en = ptr<uint32_t>(d_e);
+    float4 *pos = ptr<float4>(d_pos), *ev = ptr<float4>(d_ev);
+    double *rho = ptr<double>(d_rho), *rh = ptr<double>(d_rhs), *ph = ptr<double>(d_phi);
+    ParticleToMesh(st, en, pos, ptr<double>(d_m), cell_h, rho, dim, dim, N, origin);
+    e = cudaMemcpy(rh, rho, sizeof(double) * C, cudaMemcpyDeviceToDevice);
+    if (e != cudaSuccess) return (int)e;
+    ComputeRHS(rh, (double)(cell_hf * cell_hf), -1.0, (uint)C);
+    applyDirichlet(rh, make_double4(cx, cy, cz, 0.0), tm, origin, cell_h, n, n, n);
+    e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(density, rho, sizeof(double) * C, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(rhs, rh, sizeof(double) * C, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return (int)e;
+    const uint2 stride = make_uint2(n * n, n);
+    if (scalar) {
+        double *o = ptr<double>(d_out);
+        PotentialComputeScalarFarField(ptr<double>(d_um), rho, ph, cell_h, 1.0, 1.0, dim, dim, K);
+        PotentialInterpolateFarFieldScalar(ev, ph, o, cell_h, n, n, n, M, origin);
+        Potential_PPCorrMNScalar(st, en, ev, pos, ptr<double>(d_m), o, 1.0 / cell_h, cell_h, 1.0, 1.0, dim, dim,
+                                 stride, stride, K, M, N, origin);
+        e = cudaDeviceSynchronize();
+        if (e == cudaSuccess) e = cudaMemcpy(far, ph, sizeof(double) * C, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(out, o, sizeof(double) * M, cudaMemcpyDeviceToHost);
+        return (int)e;
+    }
+    double3 *g3 = ptr<double3>(d_g), *f3 = ptr<double3>(d_far), *o3 = ptr<double3>(d_out);
+    ComputeGradient(ph, g3, cell_h, 1.0, n, n, n);
+    PotentialComputeFarField(st, en, pos, ptr<double>(d_m), rho, ph, g3, f3, cell_h, 1.0, 1.0, dim, dim, K, M, origin);
+    PotentialInterpolateFarField(ev, f3, o3, cell_h, n, n, n, M, origin);
+    Potential_PPCorrMN(st, en, ev, pos, ptr<double>(d_m), o3, 1.0 / cell_h, cell_h, 1.0, 1.0, dim, dim, stride,
+                       stride, K, M, N, origin);
+    const float3 bbmin = make_float3((float)origin3[0], (float)origin3[1], (float)origin3[2]);
+    const float3 bbmax = make_float3((float)((double)bbmin.x + L), (float)((double)bbmin.y + L),
+                                     (float)((double)bbmin.z + L));
+    PotentialComputeGradForOutParticle(ev, tm, make_double3(cx, cy, cz), bbmin, bbmax, 1.0, 1.0, o3, M);
+    if (normals && areas) {
+        e = upload(d_nrm, normals, 3 * (size_t)M);
+        if (e == cudaSuccess) e = upload(d_area, areas, M);
+        if (e == cudaSuccess) e = upload<double>(d_dp, nullptr, M);
+        if (e != cudaSuccess) return (int)e;
+        ComputeDphidn(ptr<double3>(d_nrm), o3, ptr<double>(d_um), ptr<double>(d_dp), ptr<double>(d_area), M);
+    }
+    e = cudaDeviceSynchronize();
+    double3 *hf = new double3[C ? C : 1];
+    if (e == cudaSuccess) e = cudaMemcpy(hf, f3, sizeof(double3) * C, cudaMemcpyDeviceToHost);
+    for (size_t c = 0; e == cudaSuccess && c < C; c++) {
+        far[c] = hf[c].x;
+        far[C + c] = hf[c].y;
+        far[2 * C + c] = hf[c].z;
+    }
+    delete[] hf;
+    double3 *ho = new double3[M ? M : 1];
+    if (e == cudaSuccess) e = cudaMemcpy(ho, o3, sizeof(double3) * M, cudaMemcpyDeviceToHost);
+    for (uint32_t t = 0; e == cudaSuccess && t < M; t++) {
+        out[t] = ho[t].x;
+        out[M + t] = ho[t].y;
+        out[2 * (size_t)M + t] = ho[t].z;
+    }
+    delete[] ho;
+    if (e == cudaSuccess && normals && areas) e = cudaMemcpy(dphidn, d_dp.p, sizeof(double) * M, cudaMemcpyDeviceToHost);
+    return (int)e;
+}

@@ -220,3 +220,85 @@ def test_reference_baroclinic(refgpu, pb, oracle, H, radius, N):
     assert gdim == dim
     assert np.max(np.abs(grho.numpy() - R_rho)) <= 4 * np.finfo(np.float32).eps * scale
     assert rel_l2(dal.cpu().numpy() - al, R_al - al) <= 1e-5
+
+
+def _pot_case(N, M, seed, spread=0.2):
+    rng = np.random.default_rng(seed)
+    pos = np.zeros((N, 4), np.float32)
+    pos[:, :3] = rng.normal(0.3, spread, (N, 3))
+    mass = rng.normal(0.5, 1.0, N)
+    ev = np.zeros((M, 4), np.float32)
+    ev[:, :3] = rng.normal(0.3, 2.5 * spread, (M, 3))      # some outside the 2x box
+    ev[: M // 4] = pos[rng.integers(0, N, M // 4)]          # some on the masses themselves
+    return pos, mass, ev
+
+
+@pytest.mark.parametrize("n,K,scalar", [(32, 1, False), (64, 1, False), (32, 2, False), (32, 1, True),
+                                        (48, 2, True)])
+def test_reference_potential(refgpu, oracle, n, K, scalar):
+    """PotentialFieldSolver's P2M, Dirichlet data, gradient / scalar far field,
+    interpolation and particle corrections from the reference's own kernels
+    (with the oracle's phi and the reference's hash of the masses), against
+    orc_potential and this build's PotentialFieldSolver."""
+    import torch
+    from pppm_vortex_bouyant_flow_sample_b200.potential import PotentialFieldSolver
+    pos, mass, ev = _pot_case(20000, 8000, seed=100 + n + K)
+    ref, d = oracle.potential(n, K, pos, mass, ev, scalar=scalar, dump=True)
+    origin, L = d["origin"][:3], float(d["origin"][3])
+    h_f = np.float32(L / n)
+    _, idx, s, e, _ = refgpu.hash_particles(n, h_f, origin.astype(np.float32), pos)
+    R = refgpu.potential(n, K, pos[idx], mass[idx], mass, s, e, d["phi"], origin, h_f, L, ev, scalar=scalar)
+    assert rel_l2(R["density"], d["density"]) <= 1e-14
+    assert rel_l2(R["rhs"], d["rhs"]) <= 1e-13
+    far_o = d["far"] if scalar else d["far"].reshape(3, -1).T
+    assert rel_l2(R["far"], far_o) <= 1e-12
+    assert rel_l2(R["out"], ref) <= 1e-12
+    solver = PotentialFieldSolver()
+    solver.initializeSolver(n, n, n, K, len(ev), len(pos))
+    solver.setMassParameter(len(pos), torch.from_numpy(pos).cuda(), torch.from_numpy(mass).cuda())
+    solver.setEvalParameter(len(ev), torch.from_numpy(ev).cuda())
+    if scalar:
+        solver.computeFarFieldPotentialBuffer()
+        solver.evaluateScalarPotential()
+        got = solver.getScalarPhi().cpu().numpy()
+    else:
+        solver.computeFarFieldBuffer()
+        solver.evaluateGradient(True)
+        got = solver.getGradPhi().cpu().numpy()
+    solver.shutdown()
+    assert rel_l2(got, R["out"]) <= 1e-5
+
+
+def test_reference_dphidn(refgpu, oracle):
+    """computeDphiDn on the sources themselves (the boundary-element layout,
+    M = N): the reference's ComputeDphidn against this build's."""
+    import torch
+    from pppm_vortex_bouyant_flow_sample_b200.potential import PotentialFieldSolver
+    n, K = 32, 1
+    rng = np.random.default_rng(110)
+    pos, mass, _ = _pot_case(12000, 10, seed=111)
+    normals = rng.normal(0, 1, (len(pos), 3))
+    normals /= np.linalg.norm(normals, axis=1, keepdims=True)
+    areas = rng.uniform(0.5, 1.5, len(pos)) * 1e-4
+    ref, d = oracle.potential(n, K, pos, mass, pos, dump=True)
+    origin, L = d["origin"][:3], float(d["origin"][3])
+    h_f = np.float32(L / n)
+    _, idx, s, e, _ = refgpu.hash_particles(n, h_f, origin.astype(np.float32), pos)
+    R = refgpu.potential(n, K, pos[idx], mass[idx], mass, s, e, d["phi"], origin, h_f, L, pos, normals=normals,
+                         areas=areas)
+    assert rel_l2(R["out"], ref) <= 1e-12
+    expect = -0.5 * mass / areas + (normals * R["out"]).sum(axis=1)
+    assert rel_l2(R["dphidn"], expect) <= 1e-14
+    solver = PotentialFieldSolver()
+    solver.initializeSolver(n, n, n, K, len(pos), len(pos))
+    dpos = torch.from_numpy(pos).cuda()
+    solver.setMassParameter(len(pos), dpos, torch.from_numpy(mass).cuda())
+    solver.setEvalParameter(len(pos), dpos)
+    solver.setEvalNormals(len(pos), torch.from_numpy(normals).cuda())
+    solver.setEvalAreas(len(pos), torch.from_numpy(areas).cuda())
+    solver.computeFarFieldBuffer()
+    solver.evaluateGradient(True)
+    solver.computeDphiDn()
+    got = solver.getDpDn().cpu().numpy()
+    solver.shutdown()
+    assert rel_l2(got, R["dphidn"]) <= 1e-5
