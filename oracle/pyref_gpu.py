@@ -48,7 +48,7 @@ def lib():
         L.refgpu_segments.argtypes = [C.c_uint32, f32p, f64p, C.c_double, f32p, f32p, f64p]
         L.refgpu_segment_update.argtypes = [C.c_uint32, f32p, f32p, f64p, f64p, f64p, f64p, C.c_double, f32p, f64p]
         L.refgpu_gaussian_smooth.argtypes = [C.c_uint32, C.c_double, f64p, C.c_uint32, f32p, f32p, u32p, u32p, f64p,
-                                             C.c_double, C.c_double, f64p]
+                                             C.c_double, C.c_double, f64p, f32p]
         L.refgpu_baroclinic.argtypes = [C.c_uint32, C.c_double, C.c_float, f64p, C.c_uint32, f32p, f32p, u32p, u32p,
                                         C.c_uint32, f32p, f64p, C.c_double, f32p, f32p]
         L.refgpu_potential.argtypes = [C.c_uint32, C.c_int, C.c_uint32, f32p, f64p, f64p, u32p, u32p, f64p, f64p,
@@ -144,16 +144,20 @@ def segment_update(enda4, endb4, alpha3, kappa, ua3, ub3, dt):
     return ea, eb, cent, dv.reshape(3, N).T.copy()
 
 
-def gaussian_smooth(n, cell_h, origin, cent4, sorted_cent4, start, end, sorted_d3, nu, dt):
-    """ParticleGaussianSmooth: smoothed strengths (N, 3) in caller order."""
+def gaussian_smooth(n, cell_h, origin, cent4, sorted_cent4, start, end, sorted_d3, nu, dt, timing=None):
+    """ParticleGaussianSmooth: smoothed strengths (N, 3) in caller order (the
+    kernel's milliseconds appended to the list timing when given)."""
     cent = np.ascontiguousarray(cent4, dtype=np.float32)
     N = len(cent)
     out = np.zeros(3 * N)
+    ms = np.zeros(1, np.float32)
     _check(lib().refgpu_gaussian_smooth(n, float(cell_h), np.ascontiguousarray(origin, dtype=np.float64), N, cent,
                                         np.ascontiguousarray(sorted_cent4, dtype=np.float32),
                                         np.ascontiguousarray(start, dtype=np.uint32),
                                         np.ascontiguousarray(end, dtype=np.uint32), _soa(sorted_d3, N), float(nu),
-                                        float(dt), out), "refgpu_gaussian_smooth")
+                                        float(dt), out, ms), "refgpu_gaussian_smooth")
+    if timing is not None:
+        timing.append(float(ms[0]))
     return out.reshape(3, N).T.copy()
 
 

@@ -212,10 +212,12 @@ extern "C" int refgpu_segment_update(uint32_t N, float *enda4, float *endb4, con
 // computeStretching's smoothing (HFS/VortexSimulationSystemImp.cpp:492-509):
 // ParticleGaussianSmooth with the centres in caller order, the centres and the
 // strengths sorted by cell, the cell tables, the solver's cell size and origin.
-// out (3 x N) receives the smoothed strengths in caller order.
+// out (3 x N) receives the smoothed strengths in caller order; ms (may be
+// NULL) the kernel's device time.
 extern "C" int refgpu_gaussian_smooth(uint32_t n, double cell_h, const double origin3[3], uint32_t N,
                                       const float *cent4, const float *scent4, const uint32_t *start,
-                                      const uint32_t *end, const double *sdv, double nu, double dt, double *out) {
+                                      const uint32_t *end, const double *sdv, double nu, double dt, double *out,
+                                      float *ms) {
     const size_t C = (size_t)n * n * n;
     DevBuf d_c, d_sc, d_s, d_e, d_in, d_out;
     cudaError_t e = upload(d_c, cent4, 4 * (size_t)N);
@@ -226,10 +228,14 @@ extern "C" int refgpu_gaussian_smooth(uint32_t n, double cell_h, const double or
     if (e == cudaSuccess) e = upload<double>(d_out, nullptr, 3 * (size_t)N);
     if (e != cudaSuccess) return (int)e;
     double *in = ptr<double>(d_in), *o = ptr<double>(d_out);
+    Events ev;
+    cudaEventRecord(ev[0]);
     ParticleGaussianSmooth(ptr<uint32_t>(d_s), ptr<uint32_t>(d_e), ptr<float4>(d_c), ptr<float4>(d_sc), nu, dt, o,
                            o + N, o + 2 * (size_t)N, in, in + N, in + 2 * (size_t)N, cell_h, make_uint3(n, n, n), N,
                            make_double4(origin3[0], origin3[1], origin3[2], 0.0));
+    cudaEventRecord(ev[1]);
     e = cudaDeviceSynchronize();
+    if (ms) cudaEventElapsedTime(ms, ev[0], ev[1]);
     if (e == cudaSuccess) e = cudaMemcpy(out, o, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost);
     return (int)e;
 }

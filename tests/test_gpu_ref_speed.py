@@ -86,3 +86,66 @@ def test_path_outruns_reference_kernels(refgpu):
             json.dump(table, f, indent=1)
     assert rel <= 1e-5
     assert t_ours < t_ref
+
+
+def test_vortex_step_outruns_reference_kernels(refgpu, oracle):
+    """One vortex-segment time step of the same ring, the reference's kernels
+    chained as solveTimeStep does (segments, far field, velocity at both ends,
+    move + strength update, hash of the new centres, Gaussian smoothing)
+    against this build's pppm_vortex_step; the multigrid left out of both."""
+    import torch
+    import pppm_vortex_bouyant_flow_sample_b200 as pb
+    from pppm_vortex_bouyant_flow_sample_b200 import workloads as W
+    pb.load()
+    N, n, K, dt, h_seg, nu = 1 << 20, 128, 1, 0.01, 0.1, 0.1
+    pos, al = W.vortex_ring(N, seed=1)
+    scene = pb.Scene(n, K=K, cap_vort=N, cap_eval=2 * N)
+    for _ in range(2):
+        p, a = torch.from_numpy(pos.copy()).cuda(), torch.from_numpy(np.ascontiguousarray(al)).cuda()
+        scene.vortex_step(p, a, dt, h_seg=h_seg, nu=nu)
+    torch.cuda.synchronize()
+    scene.set_profiling(True)
+    steps = []
+    for _ in range(3):
+        p, a = torch.from_numpy(pos.copy()).cuda(), torch.from_numpy(np.ascontiguousarray(al)).cuda()
+        scene.vortex_step(p, a, dt, h_seg=h_seg, nu=nu)
+        torch.cuda.synchronize()
+        steps.append(scene.stage_times())
+    scene.set_profiling(False)
+    mine = {k: float(np.median([t[k] for t in steps])) for k in steps[0] if steps[0][k] >= 0}
+    # the centre scene's far field, for the reference's evaluation kernels
+    scene.set_vortices(torch.from_numpy(pos).cuda(), torch.from_numpy(np.ascontiguousarray(al)).cuda())
+    scene.build_far_field()
+    origin, L, h = scene.domain()
+    spos, sal = scene.sorted_vortices()
+    start, end = scene.cell_tables()
+    psi = scene.grid(pb.GRID_PSI).numpy()
+    scene.close()
+    args = (n, K, spos.cpu().numpy(), sal.cpu().numpy().T, start.numpy().astype(np.uint32),
+            end.numpy().astype(np.uint32), psi, np.asarray(origin), h)
+    ea, eb, kappa = refgpu.segments(pos, al, h_seg)
+    rb = refgpu.farfield_eval(*args, eb, pos, 1)
+    ra = refgpu.farfield_eval(*args, ea, pos, 1)
+    _, _, cent1, dv = refgpu.segment_update(ea, eb, al, kappa, ra["uvw"].T, rb["uvw"].T, dt)
+    o1, L1 = oracle.set_domain(cent1)
+    h1, of1 = oracle.hash_params(o1, L1, n)
+    _, sidx, s1, e1, hash_ms = refgpu.hash_particles(n, h1, of1, cent1)
+    smooth_ms = []
+    refgpu.gaussian_smooth(n, float(h1), o1, cent1, cent1[sidx], s1, e1, dv[sidx], nu, dt, timing=smooth_ms)
+    st = rb["stage_ms"]
+    theirs = {"p2m": st["p2m"], "curl + far field": st["curl"] + st["farfield"],
+              "velocity at the ends (interpolation + near field, 2N points)":
+                  st["interp"] + st["near_field"] + ra["stage_ms"]["interp"] + ra["stage_ms"]["near_field"],
+              "hash of the new centres": hash_ms, "gaussian smoothing": smooth_ms[0]}
+    t_ref = sum(theirs.values())
+    t_ours = sum(v for k, v in mine.items() if k != "multigrid")
+    table = {"workload": f"vortex-segment time step, vortex ring, {N:,} particles, {n}^3, dt={dt}",
+             "reference_kernels_ms": theirs, "reference_total_ms": t_ref,
+             "this_build_ms": mine, "this_build_total_without_multigrid_ms": t_ours,
+             "speedup_without_multigrid": t_ref / t_ours}
+    print(json.dumps(table, indent=1))
+    dest = os.environ.get("PPPM_TIMING_OUT")
+    if dest:
+        with open(dest.replace(".json", "_step.json"), "w") as f:
+            json.dump(table, f, indent=1)
+    assert t_ours < t_ref
