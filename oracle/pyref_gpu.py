@@ -50,10 +50,10 @@ def lib():
         L.refgpu_gaussian_smooth.argtypes = [C.c_uint32, C.c_double, f64p, C.c_uint32, f32p, f32p, u32p, u32p, f64p,
                                              C.c_double, C.c_double, f64p, f32p]
         L.refgpu_baroclinic.argtypes = [C.c_uint32, C.c_double, C.c_float, f64p, C.c_uint32, f32p, f32p, u32p, u32p,
-                                        C.c_uint32, f32p, f64p, C.c_double, f32p, f32p]
+                                        C.c_uint32, f32p, f64p, C.c_double, f32p, f32p, f32p]
         L.refgpu_potential.argtypes = [C.c_uint32, C.c_int, C.c_uint32, f32p, f64p, f64p, u32p, u32p, f64p, f64p,
                                        C.c_float, C.c_double, C.c_uint32, f32p, C.c_int, C.c_void_p, C.c_void_p,
-                                       f64p, f64p, f64p, f64p, C.c_void_p]
+                                       f64p, f64p, f64p, f64p, C.c_void_p, f32p]
         for name in ("refgpu_segments", "refgpu_segment_update", "refgpu_gaussian_smooth", "refgpu_baroclinic",
                      "refgpu_potential"):
             getattr(L, name).restype = C.c_int
@@ -161,9 +161,10 @@ def gaussian_smooth(n, cell_h, origin, cent4, sorted_cent4, start, end, sorted_d
     return out.reshape(3, N).T.copy()
 
 
-def baroclinic(dim, h, h_f, origin, sorted_heat4, sorted_heat, start, end, cent4, alpha3, dt):
+def baroclinic(dim, h, h_f, origin, sorted_heat4, sorted_heat, start, end, cent4, alpha3, dt, timing=None):
     """AssignDensity, GradDensity, ParticleGetBaroclinic: (alpha (N, 3),
-    rho (dim^3,), grad (dim^3, 3))."""
+    rho (dim^3,), grad (dim^3, 3)); the kernels' milliseconds appended to the
+    list timing when given."""
     cent = np.ascontiguousarray(cent4, dtype=np.float32)
     N = len(cent)
     al = _soa(alpha3, N)
@@ -171,11 +172,14 @@ def baroclinic(dim, h, h_f, origin, sorted_heat4, sorted_heat, start, end, cent4
     rho = np.zeros(c, np.float32)
     grad = np.zeros(3 * c, np.float32)
     hp = np.ascontiguousarray(sorted_heat4, dtype=np.float32)
+    ms = np.zeros(1, np.float32)
     _check(lib().refgpu_baroclinic(dim, float(h), C.c_float(h_f), np.ascontiguousarray(origin, dtype=np.float64),
                                    len(hp), hp, np.ascontiguousarray(sorted_heat, dtype=np.float32),
                                    np.ascontiguousarray(start, dtype=np.uint32),
-                                   np.ascontiguousarray(end, dtype=np.uint32), N, cent, al, float(dt), rho, grad),
+                                   np.ascontiguousarray(end, dtype=np.uint32), N, cent, al, float(dt), rho, grad, ms),
            "refgpu_baroclinic")
+    if timing is not None:
+        timing.append(float(ms[0]))
     return al.T.copy(), rho, grad.reshape(3, c).T.copy()
 
 
@@ -183,7 +187,8 @@ def potential(n, K, sorted_pos4, sorted_mass, mass, start, end, phi, origin, h_f
               normals=None, areas=None):
     """PotentialFieldSolver's stages with the reference's kernels and the
     given phi: dict of density, rhs (n^3), far (n^3 or (n^3, 3)), out (M or
-    (M, 3)) and, with normals and areas, dphidn (M)."""
+    (M, 3)), stage_ms (density + RHS, far-field buffer, evaluation) and, with
+    normals and areas, dphidn (M)."""
     pos = np.ascontiguousarray(sorted_pos4, dtype=np.float32)
     ev = np.ascontiguousarray(eval4, dtype=np.float32)
     N, M, Cn = len(pos), len(ev), n ** 3
@@ -194,6 +199,7 @@ def potential(n, K, sorted_pos4, sorted_mass, mass, start, end, phi, origin, h_f
         ar = np.ascontiguousarray(areas, dtype=np.float64)
         dp = np.zeros(M)
     ptr = lambda a: None if a is None else a.ctypes.data
+    ms = np.zeros(3, np.float32)
     _check(lib().refgpu_potential(n, K, N, pos, np.ascontiguousarray(sorted_mass, dtype=np.float64),
                                   np.ascontiguousarray(mass, dtype=np.float64),
                                   np.ascontiguousarray(start, dtype=np.uint32),
@@ -201,7 +207,8 @@ def potential(n, K, sorted_pos4, sorted_mass, mass, start, end, phi, origin, h_f
                                   np.ascontiguousarray(phi, dtype=np.float64),
                                   np.ascontiguousarray(origin, dtype=np.float64), C.c_float(h_f), float(L), M, ev,
                                   int(bool(scalar)), ptr(nrm), ptr(ar), out["density"], out["rhs"], out["far"],
-                                  out["out"], ptr(dp)), "refgpu_potential")
+                                  out["out"], ptr(dp), ms), "refgpu_potential")
+    out["stage_ms"] = dict(zip(("density", "far_field", "evaluation"), ms.tolist()))
     if scalar:
         out["far"] = out["far"][:Cn]
         out["out"] = out["out"][:M]

@@ -245,12 +245,14 @@ extern "C" int refgpu_gaussian_smooth(uint32_t n, double cell_h, const double or
 // start, end), GradDensity, ParticleGetBaroclinic with dt_beta = 5 dt.  dim,
 // h (double, L / dim), hf (the hash's float cell size) and origin3 describe
 // the density grid.  alpha (3 x N) is updated in place; rho (dim^3) and grad
-// (3 x dim^3, component planes) receive the grids.  ParticleGetBaroclinic
+// (3 x dim^3, component planes) receive the grids, ms (may be NULL) the device
+// time of the three kernels.  ParticleGetBaroclinic
 // launches 256 blocks of N/256 + 1 threads (its block and grid sizes swapped),
 // which covers every vortex while N/256 + 1 <= 1024.
 extern "C" int refgpu_baroclinic(uint32_t dim, double h, float hf, const double origin3[3], uint32_t H,
                                  const float *sheat4, const float *sheat, const uint32_t *start, const uint32_t *end,
-                                 uint32_t N, const float *cent4, double *alpha, double dt, float *rho, float *grad) {
+                                 uint32_t N, const float *cent4, double *alpha, double dt, float *rho, float *grad,
+                                 float *ms) {
     if (N / 256 + 1 > 1024) return -1;
     const size_t C = (size_t)dim * dim * dim;
     DevBuf d_hp, d_h, d_s, d_e, d_rho, d_grad, d_c, d_al;
@@ -266,6 +268,8 @@ extern "C" int refgpu_baroclinic(uint32_t dim, double h, float hf, const double 
     const double4 origin = make_double4(origin3[0], origin3[1], origin3[2], 0.0);
     const uint3 gd = make_uint3(dim, dim, dim);
     float *heat = ptr<float>(d_h);
+    Events ev;
+    cudaEventRecord(ev[0]);
     AssignDensity(ptr<uint32_t>(d_s), ptr<uint32_t>(d_e), ptr<float4>(d_hp), heat, heat, h, ptr<float>(d_rho), gd, gd,
                   H, origin);
     float3 *g3 = ptr<float3>(d_grad);
@@ -273,7 +277,9 @@ extern "C" int refgpu_baroclinic(uint32_t dim, double h, float hf, const double 
     double *al = ptr<double>(d_al);
     ParticleGetBaroclinic(ptr<float4>(d_c), al, al + N, al + 2 * (size_t)N, g3, dt * 5.0, N, dim, dim, dim,
                           1.0 / (double)hf, origin);
+    cudaEventRecord(ev[1]);
     e = cudaDeviceSynchronize();
+    if (ms) cudaEventElapsedTime(ms, ev[0], ev[1]);
     if (e == cudaSuccess) e = cudaMemcpy(rho, d_rho.p, sizeof(float) * C, cudaMemcpyDeviceToHost);
     float3 *hg = new float3[C ? C : 1];
     if (e == cudaSuccess) e = cudaMemcpy(hg, g3, sizeof(float3) * C, cudaMemcpyDeviceToHost);
@@ -305,12 +311,14 @@ void Potential_PPCorrMNScalar(uint *start, uint *end, float4 *pos_eval, float4 *
 // leaves them, umass in caller order for computeDphiDn.  cell_h is the hash's
 // float cell size, L the domain edge, origin3 the double origin.  Outputs:
 // density, rhs (n^3), far (scalar: n^3; gradient: 3 x n^3 planes), out (M or
-// 3 x M) and, for the gradient with normals, dphidn (M).
+// 3 x M) and, for the gradient with normals, dphidn (M); ms (may be NULL,
+// 3 entries): device time of density + RHS, of the far-field buffer, and of
+// the evaluation at the points.
 extern "C" int refgpu_potential(uint32_t n, int K, uint32_t N, const float *spos4, const double *smass,
                                 const double *umass, const uint32_t *start, const uint32_t *end, const double *phi,
                                 const double origin3[3], float cell_hf, double L, uint32_t M, const float *eval4,
                                 int scalar, const double *normals, const double *areas, double *density, double *rhs,
-                                double *far, double *out, double *dphidn) {
+                                double *far, double *out, double *dphidn, float *ms) {
     const size_t C = (size_t)n * n * n;
     const uint3 dim = make_uint3(n, n, n);
     const double cell_h = (double)cell_hf;
@@ -344,13 +352,16 @@ extern "C" int refgpu_potential(uint32_t n, int K, uint32_t N, const float *spos
     if (e == cudaSuccess) e = upload<double>(d_out, nullptr, 3 * (size_t)M);
     if (e != cudaSuccess) return (int)e;
     uint32_t *st = ptr<uint32_t>(d_s), *en = ptr<uint32_t>(d_e);
-    float4 *pos = ptr<float4>(d_pos), *ev = ptr<float4>(d_ev);
+    float4 *pos = ptr<float4>(d_pos), *pts = ptr<float4>(d_ev);
     double *rho = ptr<double>(d_rho), *rh = ptr<double>(d_rhs), *ph = ptr<double>(d_phi);
+    Events ev;
+    cudaEventRecord(ev[0]);
     ParticleToMesh(st, en, pos, ptr<double>(d_m), cell_h, rho, dim, dim, N, origin);
     e = cudaMemcpy(rh, rho, sizeof(double) * C, cudaMemcpyDeviceToDevice);
     if (e != cudaSuccess) return (int)e;
     ComputeRHS(rh, (double)(cell_hf * cell_hf), -1.0, (uint)C);
     applyDirichlet(rh, make_double4(cx, cy, cz, 0.0), tm, origin, cell_h, n, n, n);
+    cudaEventRecord(ev[1]);
     e = cudaDeviceSynchronize();
     if (e == cudaSuccess) e = cudaMemcpy(density, rho, sizeof(double) * C, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(rhs, rh, sizeof(double) * C, cudaMemcpyDeviceToHost);
@@ -358,25 +369,36 @@ extern "C" int refgpu_potential(uint32_t n, int K, uint32_t N, const float *spos
     const uint2 stride = make_uint2(n * n, n);
     if (scalar) {
         double *o = ptr<double>(d_out);
+        cudaEventRecord(ev[2]);
         PotentialComputeScalarFarField(ptr<double>(d_um), rho, ph, cell_h, 1.0, 1.0, dim, dim, K);
-        PotentialInterpolateFarFieldScalar(ev, ph, o, cell_h, n, n, n, M, origin);
-        Potential_PPCorrMNScalar(st, en, ev, pos, ptr<double>(d_m), o, 1.0 / cell_h, cell_h, 1.0, 1.0, dim, dim,
+        cudaEventRecord(ev[3]);
+        PotentialInterpolateFarFieldScalar(pts, ph, o, cell_h, n, n, n, M, origin);
+        Potential_PPCorrMNScalar(st, en, pts, pos, ptr<double>(d_m), o, 1.0 / cell_h, cell_h, 1.0, 1.0, dim, dim,
                                  stride, stride, K, M, N, origin);
+        cudaEventRecord(ev[4]);
         e = cudaDeviceSynchronize();
+        if (ms) {
+            cudaEventElapsedTime(ms, ev[0], ev[1]);
+            cudaEventElapsedTime(ms + 1, ev[2], ev[3]);
+            cudaEventElapsedTime(ms + 2, ev[3], ev[4]);
+        }
         if (e == cudaSuccess) e = cudaMemcpy(far, ph, sizeof(double) * C, cudaMemcpyDeviceToHost);
         if (e == cudaSuccess) e = cudaMemcpy(out, o, sizeof(double) * M, cudaMemcpyDeviceToHost);
         return (int)e;
     }
     double3 *g3 = ptr<double3>(d_g), *f3 = ptr<double3>(d_far), *o3 = ptr<double3>(d_out);
+    cudaEventRecord(ev[2]);
     ComputeGradient(ph, g3, cell_h, 1.0, n, n, n);
     PotentialComputeFarField(st, en, pos, ptr<double>(d_m), rho, ph, g3, f3, cell_h, 1.0, 1.0, dim, dim, K, M, origin);
-    PotentialInterpolateFarField(ev, f3, o3, cell_h, n, n, n, M, origin);
-    Potential_PPCorrMN(st, en, ev, pos, ptr<double>(d_m), o3, 1.0 / cell_h, cell_h, 1.0, 1.0, dim, dim, stride,
+    cudaEventRecord(ev[3]);
+    PotentialInterpolateFarField(pts, f3, o3, cell_h, n, n, n, M, origin);
+    Potential_PPCorrMN(st, en, pts, pos, ptr<double>(d_m), o3, 1.0 / cell_h, cell_h, 1.0, 1.0, dim, dim, stride,
                        stride, K, M, N, origin);
     const float3 bbmin = make_float3((float)origin3[0], (float)origin3[1], (float)origin3[2]);
     const float3 bbmax = make_float3((float)((double)bbmin.x + L), (float)((double)bbmin.y + L),
                                      (float)((double)bbmin.z + L));
-    PotentialComputeGradForOutParticle(ev, tm, make_double3(cx, cy, cz), bbmin, bbmax, 1.0, 1.0, o3, M);
+    PotentialComputeGradForOutParticle(pts, tm, make_double3(cx, cy, cz), bbmin, bbmax, 1.0, 1.0, o3, M);
+    cudaEventRecord(ev[4]);
     if (normals && areas) {
         e = upload(d_nrm, normals, 3 * (size_t)M);
         if (e == cudaSuccess) e = upload(d_area, areas, M);
@@ -385,6 +407,11 @@ extern "C" int refgpu_potential(uint32_t n, int K, uint32_t N, const float *spos
         ComputeDphidn(ptr<double3>(d_nrm), o3, ptr<double>(d_um), ptr<double>(d_dp), ptr<double>(d_area), M);
     }
     e = cudaDeviceSynchronize();
+    if (ms) {
+        cudaEventElapsedTime(ms, ev[0], ev[1]);
+        cudaEventElapsedTime(ms + 1, ev[2], ev[3]);
+        cudaEventElapsedTime(ms + 2, ev[3], ev[4]);
+    }
     double3 *hf = new double3[C ? C : 1];
     if (e == cudaSuccess) e = cudaMemcpy(hf, f3, sizeof(double3) * C, cudaMemcpyDeviceToHost);
     for (size_t c = 0; e == cudaSuccess && c < C; c++) {

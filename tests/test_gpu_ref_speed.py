@@ -149,3 +149,118 @@ def test_vortex_step_outruns_reference_kernels(refgpu, oracle):
         with open(dest.replace(".json", "_step.json"), "w") as f:
             json.dump(table, f, indent=1)
     assert t_ours < t_ref
+
+
+def _events():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def test_potential_outruns_reference_kernels(refgpu):
+    """The scalar PPPM workload of the bench (262,144 sphere sources, 128^3,
+    gradient at 1,048,576 shell points): the reference's P2M + Dirichlet data,
+    gradient far field and evaluation kernels (its multigrid left out) against
+    this build's whole computeFarFieldBuffer + evaluateGradient, multigrid
+    included."""
+    import torch
+    import pppm_vortex_bouyant_flow_sample_b200 as pb
+    from pppm_vortex_bouyant_flow_sample_b200 import workloads as W
+    from pppm_vortex_bouyant_flow_sample_b200.potential import PotentialFieldSolver
+    pb.load()
+    Ns, M, n, K = 262_144, 1 << 20, 128, 1
+    src, mass = W.sphere_panels(Ns)
+    ev = W.shell_points(M)
+    dsrc, dmass, dev = (torch.from_numpy(a).cuda() for a in (src, mass, ev))
+    solver = PotentialFieldSolver()
+    solver.initializeSolver(n, n, n, K, M, Ns)
+    ms = []
+    for it in range(5):
+        e0, e1 = _events()
+        e0.record()
+        solver.setMassParameter(Ns, dsrc, dmass)
+        solver.setEvalParameter(M, dev)
+        solver.computeFarFieldBuffer()
+        solver.evaluateGradient(True)
+        e1.record()
+        torch.cuda.synchronize()
+        if it >= 2:
+            ms.append(e0.elapsed_time(e1))
+    g = solver.getGradPhi().cpu().numpy()
+    grids = solver.grids()
+    solver.shutdown()
+    origin, L = np.asarray(grids["origin"]), grids["length"]
+    h_f = np.float32(L / n)
+    _, idx, s, e, hash_ms = refgpu.hash_particles(n, h_f, origin.astype(np.float32), src)
+    R = None
+    for _ in range(2):
+        R = refgpu.potential(n, K, src[idx], mass[idx], mass, s, e, grids["phi"].numpy(), origin, h_f, L, ev)
+    theirs = dict(R["stage_ms"], hash=hash_ms)
+    t_ref = sum(theirs.values())
+    t_ours = float(np.median(ms))
+    rel = float(np.linalg.norm(g - R["out"]) / np.linalg.norm(R["out"]))
+    table = {"workload": f"scalar PPPM gradient, {Ns:,} sphere sources, {n}^3, {M:,} points",
+             "reference_kernels_ms_without_multigrid": theirs, "reference_total_ms": t_ref,
+             "this_build_total_ms_with_multigrid": t_ours, "speedup": t_ref / t_ours,
+             "rel_l2_gradient_vs_reference_kernels": rel}
+    print(json.dumps(table, indent=1))
+    dest = os.environ.get("PPPM_TIMING_OUT")
+    if dest:
+        with open(dest.replace(".json", "_potential.json"), "w") as f:
+            json.dump(table, f, indent=1)
+    assert rel <= 1e-5
+    assert t_ours < t_ref
+
+
+def test_baroclinic_outruns_reference_kernels(refgpu, oracle):
+    """The buoyancy source on 1,048,576 heat particles in a radius-0.5 sphere
+    and 200,000 vortices (the reference's launch covers at most 261,888): the
+    reference's hash of the heat particles, AssignDensity, GradDensity and
+    ParticleGetBaroclinic against this build's pppm_baroclinic (its host
+    round trip for the bounding box included)."""
+    import torch
+    import pppm_vortex_bouyant_flow_sample_b200 as pb
+    from pppm_vortex_bouyant_flow_sample_b200 import workloads as W
+    pb.load()
+    heat4, _, temp = W.plume_sphere(1 << 20, seed=3, radius=0.5)
+    heat = temp.astype(np.float32)
+    rng = np.random.default_rng(7)
+    N = 200_000
+    cent = np.zeros((N, 4), np.float32)
+    cent[:, :3] = heat4[rng.integers(0, len(heat4), N), :3]
+    al = rng.normal(0, 1e-4, (N, 3))
+    dt = 0.002
+    scene = pb.Scene(32, cap_vort=N, cap_eval=N)
+    dheat4, dheat, dcent = (torch.from_numpy(a).cuda() for a in (heat4, heat, cent))
+    ms = []
+    for it in range(5):
+        dal = torch.from_numpy(al.copy()).cuda()
+        e0, e1 = _events()
+        e0.record()
+        scene.baroclinic(dheat4, dheat, dcent, dal, dt)
+        e1.record()
+        torch.cuda.synchronize()
+        if it >= 2:
+            ms.append(e0.elapsed_time(e1))
+    got = dal.cpu().numpy()
+    scene.close()
+    ra, dim, origin, h, _, _ = oracle.baroclinic(heat4, heat, cent, al, dt)
+    h_f = np.float32(h)
+    t_ref = []
+    for _ in range(2):
+        _, hidx, hs, he, hash_ms = refgpu.hash_particles(dim, h_f, origin.astype(np.float32), heat4, end_fill=0)
+        kern = []
+        R_al, _, _ = refgpu.baroclinic(dim, h, h_f, origin, heat4[hidx], heat[hidx], hs, he, cent, al, dt, timing=kern)
+        t_ref.append((hash_ms, kern[0]))
+    theirs = {"hash": t_ref[-1][0], "density + gradient + force": t_ref[-1][1]}
+    rel = float(np.linalg.norm((got - al) - (R_al - al)) / np.linalg.norm(R_al - al))
+    table = {"workload": f"baroclinic source, {len(heat4):,} heat particles (radius 0.5), {N:,} vortices, "
+                         f"density grid {dim}^3",
+             "reference_kernels_ms": theirs, "reference_total_ms": sum(theirs.values()),
+             "this_build_ms": float(np.median(ms)), "speedup": sum(theirs.values()) / float(np.median(ms)),
+             "rel_l2_strength_change_vs_reference_kernels": rel}
+    print(json.dumps(table, indent=1))
+    dest = os.environ.get("PPPM_TIMING_OUT")
+    if dest:
+        with open(dest.replace(".json", "_baroclinic.json"), "w") as f:
+            json.dump(table, f, indent=1)
+    assert rel <= 1e-5
