@@ -43,6 +43,54 @@ def test_params_default_and_validation_without_gpu():
     assert lib.pppm_scene_create(ctypes.byref(bad), 10, 10, None, ctypes.byref(h)) == 1
 
 
+@pytest.mark.parametrize("kw,why", [
+    (dict(n=3), b"outside [4, 512]"),
+    (dict(n=513), b"outside [4, 512]"),
+    (dict(n=100), b"odd edge"),              # 100 -> 50 -> 25: odd level above the coarsest
+    (dict(n=32, K=-2), b"K=-2"),
+    (dict(n=32, K=5), b"K=5"),
+    (dict(n=32, a=0.0), b"smoothing radius"),
+    (dict(n=32, a=float("nan")), b"smoothing radius"),
+    (dict(n=32, domain_mode=7), b"domain_mode"),
+    (dict(n=32, domain_mode=1, fixed_length=0.0), b"fixed_length"),
+    (dict(n=32, domain_mode=1, fixed_length=float("inf")), b"fixed_length"),
+    (dict(n=32, mg_mode=9), b"mg_mode"),
+    (dict(n=32, mg_mode=1, mg_max_cycles=0), b"CONVERGED"),
+    (dict(n=32, mg_mode=1, mg_tol=0.0), b"CONVERGED"),
+])
+def test_scene_parameters_refused_before_any_allocation(kw, why):
+    """Every invalid parameter set is refused with PPPM_ERR_INVALID and a
+    message, before the library touches a device (so it runs on CPU)."""
+    import pppm_vortex_bouyant_flow_sample_b200._lib as L
+    lib = L.load()
+    n = kw.pop("n")
+    p = L.default_params(n, **kw)
+    h = ctypes.c_void_p()
+    assert lib.pppm_scene_create(ctypes.byref(p), 10, 10, None, ctypes.byref(h)) == 1
+    assert h.value is None
+    assert why in lib.pppm_last_error()
+
+
+def test_null_handles_and_arguments_refused():
+    """NULL scenes and output pointers give PPPM_ERR_INVALID, not a crash."""
+    import pppm_vortex_bouyant_flow_sample_b200._lib as L
+    lib = L.load()
+    vp = ctypes.c_void_p
+    assert lib.pppm_scene_create(ctypes.byref(L.default_params(32)), 10, 10, None, None) == 1
+    assert lib.pppm_set_vortices(None, 1, vp(8), vp(8), vp(8), vp(8)) == 1
+    assert lib.pppm_build_far_field(None) == 1
+    assert lib.pppm_eval(None, 1, vp(8), None, 0, vp(8), vp(8), vp(8)) == 1
+    assert lib.pppm_get_domain(None, None, None, None) == 1
+    h = ctypes.c_void_p()
+    assert lib.pppm_potential_create(3, 1, 10, 10, None, ctypes.byref(h)) == 1
+    assert lib.pppm_potential_create(32, 9, 10, 10, None, ctypes.byref(h)) == 1
+    assert lib.pppm_hasher_create(0, 32, None, ctypes.byref(h)) == 1
+    assert lib.pppm_hasher_create(16, 1, None, ctypes.byref(h)) == 1
+    assert lib.pppm_mg_create(100, None, ctypes.byref(h)) == 1
+    assert lib.pppm_renderer_create(None, None) == 1
+    assert lib.pppm_scene_destroy(None) == 0
+
+
 def test_no_cpu_fallback():
     import torch
     if torch.cuda.is_available():
