@@ -437,6 +437,14 @@ pppm_status pppm_direct_sum_fp64(uint32_t N, const float *vort_pos4_dev, const d
                                  double a, double *u_dev, double *v_dev, double *w_dev,
                                  void *stream);
 
+/* Test hook, no counterpart in the reference: after `after` more device or
+ * pinned-host allocations by the library succeed, the next one fails as if
+ * the device were out of memory (the call that made it returns PPPM_ERR_OOM);
+ * later allocations succeed again.  after < 0 disarms it.  Lets a test walk
+ * every allocation of a call sequence and check that each failure is reported
+ * and leaves nothing allocated, with no real memory pressure. */
+pppm_status pppm_debug_fail_allocation(int64_t after);
+
 #ifdef __cplusplus
 }
 #endif

@@ -34,6 +34,7 @@ EXPORTED = (
     "pppm_render_shadows", "pppm_render_shadow_map", "pppm_render_smoke", "pppm_potential_create",
     "pppm_potential_destroy", "pppm_potential_set_masses", "pppm_potential_build", "pppm_potential_eval_gradient",
     "pppm_potential_eval_scalar", "pppm_potential_dphidn", "pppm_potential_grids", "pppm_potential_eval_gradient3",
+    "pppm_debug_fail_allocation",
 )
 REQ_EVAL, REQ_ADVANCE = 0, 1
 NOALLOC_MAX_PARTICLES = 1048576  # PPPM_NOALLOC_MAX_PARTICLES in include/pppm.h
@@ -132,6 +133,7 @@ def load(build_if_missing: bool = True):
         "pppm_stage_name": (C.c_char_p, [C.c_int]),
         "pppm_get_stage_times": (st, [vp, C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_int)]),
         "pppm_kernel_launches": (C.c_uint64, []),
+        "pppm_debug_fail_allocation": (st, [C.c_int64]),
         "pppm_spatial_hash_noalloc": (st, [u32, vp, u32, C.c_float, C.POINTER(C.c_float), vp, vp, vp, vp, vp]),
         "pppm_advect_euler": (st, [vp, u32, vp, vp, vp, vp, C.c_double]),
         "pppm_advect_rk2": (st, [vp, u32, vp, vp, vp, vp, C.c_double]),

@@ -9,6 +9,44 @@
 
 #include "pppm_internal.cuh"
 
+namespace pppm {
+
+namespace {
+// Allocations still to succeed before one is made to fail (-1: none armed).
+std::atomic<long long> g_alloc_fail_after{-1};
+
+bool fail_this_allocation() {
+    long long c = g_alloc_fail_after.load();
+    while (c >= 0) {
+        if (g_alloc_fail_after.compare_exchange_weak(c, c - 1)) return c == 0;
+    }
+    return false;
+}
+}  // namespace
+
+cudaError_t device_malloc(void **p, size_t bytes) {
+    if (fail_this_allocation()) {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
+    return cudaMalloc(p, bytes);
+}
+
+cudaError_t host_malloc(void **p, size_t bytes) {
+    if (fail_this_allocation()) {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
+    return cudaMallocHost(p, bytes);
+}
+
+}  // namespace pppm
+
+extern "C" pppm_status pppm_debug_fail_allocation(int64_t after) {
+    pppm::g_alloc_fail_after.store(after < 0 ? -1 : (long long)after);
+    return PPPM_OK;
+}
+
 namespace {
 
 thread_local char g_err[512] = "";
@@ -48,7 +86,7 @@ pppm_status cuda_fail(const char *where, cudaError_t e) {
 
 template <typename T>
 cudaError_t dalloc(T **p, size_t count) {
-    return cudaMalloc((void **)p, sizeof(T) * (count ? count : 1));
+    return ::pppm::device_malloc((void **)p, sizeof(T) * (count ? count : 1));
 }
 
 void free_vortex_side(pppm_scene *s) {
@@ -83,10 +121,7 @@ cudaError_t alloc_hist(pppm_scene *s) {
     return cudaSuccess;
 }
 
-cudaError_t alloc_vortex_side(pppm_scene *s, uint32_t cap) {
-    std::lock_guard<std::recursive_mutex> lk(pppm::device_lock());
-    free_vortex_side(s);
-    s->capN = cap;
+cudaError_t alloc_vortex_buffers(pppm_scene *s, uint32_t cap) {
     PPPM_CUDA_TRY(dalloc(&s->vpos, cap));
     PPPM_CUDA_TRY(dalloc(&s->valpha, 3 * (size_t)cap));
     for (int q = 0; q < 2; q++) {
@@ -101,13 +136,30 @@ cudaError_t alloc_vortex_side(pppm_scene *s, uint32_t cap) {
     PPPM_CUDA_TRY(dalloc(&s->ts_kappa, cap));
     s->bbox_blocks = 148 * 2;
     PPPM_CUDA_TRY(dalloc(&s->bbox_partial, 6 * (size_t)s->bbox_blocks));
-    return alloc_hist(s);
+    return cudaSuccess;
 }
 
-cudaError_t alloc_eval_side(pppm_scene *s, uint32_t cap) {
+// A failed growth leaves the side empty with capacity 0, so that the next call
+// that needs it allocates again instead of using a freed buffer.
+cudaError_t alloc_vortex_side(pppm_scene *s, uint32_t cap) {
     std::lock_guard<std::recursive_mutex> lk(pppm::device_lock());
-    free_eval_side(s);
-    s->capM = cap;
+    free_vortex_side(s);
+    s->capN = 0;
+    s->vort_set = false;   // the vortices went with the old buffers
+    s->far_ready = false;
+    cudaError_t e = alloc_vortex_buffers(s, cap);
+    if (e == cudaSuccess) {
+        s->capN = cap;
+        e = alloc_hist(s);
+    }
+    if (e != cudaSuccess) {
+        free_vortex_side(s);
+        s->capN = 0;
+    }
+    return e;
+}
+
+cudaError_t alloc_eval_buffers(pppm_scene *s, uint32_t cap) {
     for (int q = 0; q < 2; q++) {
         PPPM_CUDA_TRY(dalloc(&s->ekey[q], cap));
         PPPM_CUDA_TRY(dalloc(&s->eidx[q], cap));
@@ -115,7 +167,23 @@ cudaError_t alloc_eval_side(pppm_scene *s, uint32_t cap) {
     PPPM_CUDA_TRY(dalloc(&s->stage_ea, cap));
     PPPM_CUDA_TRY(dalloc(&s->stage_eb, cap));
     PPPM_CUDA_TRY(dalloc(&s->stage_out, 3 * (size_t)cap));
-    return alloc_hist(s);
+    return cudaSuccess;
+}
+
+cudaError_t alloc_eval_side(pppm_scene *s, uint32_t cap) {
+    std::lock_guard<std::recursive_mutex> lk(pppm::device_lock());
+    free_eval_side(s);
+    s->capM = 0;
+    cudaError_t e = alloc_eval_buffers(s, cap);
+    if (e == cudaSuccess) {
+        s->capM = cap;
+        e = alloc_hist(s);
+    }
+    if (e != cudaSuccess) {
+        free_eval_side(s);
+        s->capM = 0;
+    }
+    return e;
 }
 
 cudaError_t alloc_grid_side(pppm_scene *s) {
@@ -359,7 +427,7 @@ extern "C" pppm_status pppm_count_pairs(pppm_scene *s, uint32_t M, const float *
     if (!s || !pairs) return PPPM_ERR_INVALID;
     std::lock_guard<std::recursive_mutex> lk(pppm::device_lock());
     float *tmp = nullptr;
-    cudaError_t e = cudaMalloc(&tmp, sizeof(float) * 3 * (size_t)(M ? M : 1));
+    cudaError_t e = ::pppm::device_malloc((void **)&tmp, sizeof(float) * 3 * (size_t)(M ? M : 1));
     if (e != cudaSuccess) return cuda_fail("pppm_count_pairs", e);
     pppm_status st = eval_common(s, M, ea, ea, 0, nullptr, nullptr, nullptr, tmp, 1);
     unsigned long long h = 0;
@@ -600,7 +668,7 @@ extern "C" pppm_status pppm_get_sorted_vortices(pppm_scene *s, float *pos4, doub
         if (e != cudaSuccess) return cuda_fail("pppm_get_sorted_vortices", e);
         s->ref_valid = true;
     }
-    if (ax || ay || az) e = cudaMalloc(&tmp, sizeof(double) * 3 * (size_t)s->N);
+    if (ax || ay || az) e = ::pppm::device_malloc((void **)&tmp, sizeof(double) * 3 * (size_t)s->N);
     if (e == cudaSuccess) e = pppm::launch_gather_sorted(s, reinterpret_cast<float4 *>(pos4), tmp);
     const size_t N = s->N;
     if (e == cudaSuccess && ax) e = cudaMemcpyAsync(ax, tmp, sizeof(double) * N, cudaMemcpyDeviceToDevice, s->stream);

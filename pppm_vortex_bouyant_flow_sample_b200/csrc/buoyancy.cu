@@ -254,12 +254,15 @@ template <typename T>
 cudaError_t grow(T **p, size_t count) {
     cudaFree(*p);
     *p = nullptr;
-    return cudaMalloc((void **)p, sizeof(T) * (count ? count : 1));
+    return ::pppm::device_malloc((void **)p, sizeof(T) * (count ? count : 1));
 }
 
+// Capacities are raised only once every buffer they cover exists; a failed
+// growth leaves capacity 0 so that the next call allocates again.
 cudaError_t ensure_heat(Buoyancy *b, uint32_t H) {
     if (H <= b->capH) return cudaSuccess;
     std::lock_guard<std::recursive_mutex> lk(device_lock());
+    b->capH = 0;
     for (int q = 0; q < 2; q++) {
         PPPM_CUDA_TRY(grow(&b->key[q], H));
         PPPM_CUDA_TRY(grow(&b->idx[q], H));
@@ -273,6 +276,8 @@ cudaError_t ensure_heat(Buoyancy *b, uint32_t H) {
 cudaError_t ensure_grid(Buoyancy *b, size_t cells, size_t parts) {
     std::lock_guard<std::recursive_mutex> lk(device_lock());
     if (cells > b->capC) {
+        b->capC = 0;
+        b->dim = 0;   // the last density grid went with the old buffers
         PPPM_CUDA_TRY(grow(&b->start, cells));
         PPPM_CUDA_TRY(grow(&b->end, cells));
         PPPM_CUDA_TRY(grow(&b->rho, cells));
@@ -280,6 +285,7 @@ cudaError_t ensure_grid(Buoyancy *b, size_t cells, size_t parts) {
         b->capC = cells;
     }
     if (parts > b->capPart) {
+        b->capPart = 0;
         PPPM_CUDA_TRY(grow(&b->part, parts));
         b->capPart = parts;
     }
@@ -319,9 +325,16 @@ extern "C" pppm_status pppm_baroclinic(pppm_scene *s, uint32_t H, const float *h
     cudaError_t e = cudaSuccess;
     if (!s->buoy) {
         std::lock_guard<std::recursive_mutex> lk(device_lock());
-        s->buoy = new Buoyancy;
-        e = cudaMalloc(&s->buoy->bbox, sizeof(float) * 6 * kBBoxBlocks);
-        if (e == cudaSuccess) e = cudaMallocHost(&s->buoy->host_bbox, sizeof(float) * 6 * kBBoxBlocks);
+        Buoyancy *nb = new Buoyancy;
+        e = ::pppm::device_malloc((void **)&nb->bbox, sizeof(float) * 6 * kBBoxBlocks);
+        if (e == cudaSuccess) e = ::pppm::host_malloc((void **)&nb->host_bbox, sizeof(float) * 6 * kBBoxBlocks);
+        if (e == cudaSuccess) {
+            s->buoy = nb;
+        } else {
+            free_buoyancy(nb);   // the next call starts over
+            pppm_set_error("pppm_baroclinic (alloc): %s", cudaGetErrorString(e));
+            return PPPM_ERR_OOM;
+        }
     }
     Buoyancy *b = s->buoy;
     if (e == cudaSuccess) e = ensure_heat(b, H);

@@ -522,12 +522,12 @@ extern "C" pppm_status pppm_hasher_create(uint32_t cap, uint32_t n, void *stream
     h->C = n * n * n;
     cudaError_t e = cudaSuccess;
     for (int q = 0; q < 2 && e == cudaSuccess; q++) {
-        e = cudaMalloc(&h->key[q], sizeof(uint32_t) * cap);
-        if (e == cudaSuccess) e = cudaMalloc(&h->idx[q], sizeof(uint32_t) * cap);
+        e = ::pppm::device_malloc((void **)&h->key[q], sizeof(uint32_t) * cap);
+        if (e == cudaSuccess) e = ::pppm::device_malloc((void **)&h->idx[q], sizeof(uint32_t) * cap);
     }
-    if (e == cudaSuccess) e = cudaMalloc(&h->hist, sizeof(uint32_t) * pppm::radix_hist_entries(cap));
-    if (e == cudaSuccess) e = cudaMalloc(&h->start, sizeof(uint32_t) * h->C);
-    if (e == cudaSuccess) e = cudaMalloc(&h->end, sizeof(uint32_t) * h->C);
+    if (e == cudaSuccess) e = ::pppm::device_malloc((void **)&h->hist, sizeof(uint32_t) * pppm::radix_hist_entries(cap));
+    if (e == cudaSuccess) e = ::pppm::device_malloc((void **)&h->start, sizeof(uint32_t) * h->C);
+    if (e == cudaSuccess) e = ::pppm::device_malloc((void **)&h->end, sizeof(uint32_t) * h->C);
     if (e != cudaSuccess) {
         pppm_set_error("pppm_hasher_create: %s", cudaGetErrorString(e));
         pppm_hasher_destroy(h);

@@ -479,12 +479,22 @@ template <typename T>
 cudaError_t grow(T **p, size_t count) {
     cudaFree(*p);
     *p = nullptr;
-    return cudaMalloc((void **)p, sizeof(T) * (count ? count : 1));
+    return ::pppm::device_malloc((void **)p, sizeof(T) * (count ? count : 1));
 }
 
-cudaError_t ensure_masses(pppm_potential *P, uint32_t N) {
-    if (N <= P->capN) return cudaSuccess;
-    std::lock_guard<std::recursive_mutex> lk(device_lock());
+// Capacities are raised only once every buffer they cover exists: a failed
+// growth leaves capacity 0 (and no masses), so the next call allocates again
+// instead of using a freed buffer.
+cudaError_t ensure_hist(pppm_potential *P) {
+    const size_t need = radix_hist_entries(std::max(P->capN, P->capM));
+    if (need <= P->hist_cap) return cudaSuccess;
+    P->hist_cap = 0;
+    PPPM_CUDA_TRY(grow(&P->hist, need));
+    P->hist_cap = need;
+    return cudaSuccess;
+}
+
+cudaError_t grow_masses(pppm_potential *P, uint32_t N) {
     PPPM_CUDA_TRY(grow(&P->mpos, N));
     PPPM_CUDA_TRY(grow(&P->mass, N));
     for (int q = 0; q < 2; q++) {
@@ -493,29 +503,32 @@ cudaError_t ensure_masses(pppm_potential *P, uint32_t N) {
     }
     PPPM_CUDA_TRY(grow(&P->srec, N));
     PPPM_CUDA_TRY(grow(&P->smass, N));
-    P->capN = N;
-    const size_t need = radix_hist_entries(std::max(P->capN, P->capM));
-    if (need > P->hist_cap) {
-        PPPM_CUDA_TRY(grow(&P->hist, need));
-        P->hist_cap = need;
-    }
     return cudaSuccess;
 }
 
-cudaError_t ensure_eval(pppm_potential *P, uint32_t M) {
-    if (M <= P->capM) return cudaSuccess;
+cudaError_t ensure_masses(pppm_potential *P, uint32_t N) {
     std::lock_guard<std::recursive_mutex> lk(device_lock());
-    for (int q = 0; q < 2; q++) {
-        PPPM_CUDA_TRY(grow(&P->ekey[q], M));
-        PPPM_CUDA_TRY(grow(&P->eidx[q], M));
+    if (N > P->capN) {
+        P->capN = 0;
+        P->N = 0;        // the masses went with the old buffers
+        P->built = 0;
+        PPPM_CUDA_TRY(grow_masses(P, N));
+        P->capN = N;
     }
-    P->capM = M;
-    const size_t need = radix_hist_entries(std::max(P->capN, P->capM));
-    if (need > P->hist_cap) {
-        PPPM_CUDA_TRY(grow(&P->hist, need));
-        P->hist_cap = need;
+    return ensure_hist(P);
+}
+
+cudaError_t ensure_eval(pppm_potential *P, uint32_t M) {
+    std::lock_guard<std::recursive_mutex> lk(device_lock());
+    if (M > P->capM) {
+        P->capM = 0;
+        for (int q = 0; q < 2; q++) {
+            PPPM_CUDA_TRY(grow(&P->ekey[q], M));
+            PPPM_CUDA_TRY(grow(&P->eidx[q], M));
+        }
+        P->capM = M;
     }
-    return cudaSuccess;
+    return ensure_hist(P);
 }
 
 }  // namespace
@@ -551,7 +564,7 @@ extern "C" pppm_status pppm_potential_create(uint32_t n, int K, uint32_t cap_mas
     if (e == cudaSuccess) e = grow(&P->mono, 4);
     if (e == cudaSuccess) e = grow(&P->mono_part, 5 * kRedBlocks);
     if (e == cudaSuccess) e = grow(&P->bbox, 6 * kRedBlocks);
-    if (e == cudaSuccess) e = cudaMallocHost(&P->host_bbox, sizeof(float) * 6 * kRedBlocks);
+    if (e == cudaSuccess) e = ::pppm::host_malloc((void **)&P->host_bbox, sizeof(float) * 6 * kRedBlocks);
     if (e == cudaSuccess) e = ensure_masses(P, std::max(cap_mass, 1u));
     if (e == cudaSuccess) e = ensure_eval(P, std::max(cap_eval, 1u));
     pppm_status st = PPPM_OK;

@@ -77,6 +77,12 @@ struct MGPlan {
     const double *coarse_op = nullptr;  // [cells][cells] FP64 map b -> x of the coarsest solve, or null
 };
 
+// Every device and pinned-host allocation of the library goes through these
+// two, so that a test can make one of them fail on purpose
+// (pppm_debug_fail_allocation) without a real out-of-memory condition.
+cudaError_t device_malloc(void **p, size_t bytes);
+cudaError_t host_malloc(void **p, size_t bytes);
+
 cudaError_t build_coarse_operator(int d, double *op, cudaStream_t st);
 cudaError_t mg_capture_graph(const MGPlan &m, cudaGraphExec_t *exec, unsigned *kernel_nodes);
 

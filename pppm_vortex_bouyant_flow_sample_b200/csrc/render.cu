@@ -369,12 +369,15 @@ template <typename T>
 cudaError_t grow(T **p, size_t count) {
     cudaFree(*p);
     *p = nullptr;
-    return cudaMalloc((void **)p, sizeof(T) * (count ? count : 1));
+    return ::pppm::device_malloc((void **)p, sizeof(T) * (count ? count : 1));
 }
 
+// Capacities are raised only once every buffer they cover exists; a failed
+// growth leaves capacity 0 so that the next call allocates again.
 cudaError_t ensure_particles(pppm_renderer *R, uint32_t n) {
     if (n <= R->capN) return cudaSuccess;
     std::lock_guard<std::recursive_mutex> lk(device_lock());
+    R->capN = 0;
     for (int q = 0; q < 2; q++) {
         PPPM_CUDA_TRY(grow(&R->key[q], n));
         PPPM_CUDA_TRY(grow(&R->idx[q], n));
@@ -393,6 +396,7 @@ cudaError_t ensure_particles(pppm_renderer *R, uint32_t n) {
 cudaError_t ensure_pairs(pppm_renderer *R, uint32_t pairs, uint32_t tiles) {
     std::lock_guard<std::recursive_mutex> lk(device_lock());
     if (pairs > R->capPairs) {
+        R->capPairs = 0;
         for (int q = 0; q < 2; q++) {
             PPPM_CUDA_TRY(grow(&R->pkey[q], pairs));
             PPPM_CUDA_TRY(grow(&R->pval[q], pairs));
@@ -401,10 +405,12 @@ cudaError_t ensure_pairs(pppm_renderer *R, uint32_t pairs, uint32_t tiles) {
     }
     const size_t need = radix_hist_entries(std::max(pairs, R->capN));
     if (need > R->hist_cap) {
+        R->hist_cap = 0;
         PPPM_CUDA_TRY(grow(&R->hist, need));
         R->hist_cap = need;
     }
     if (tiles > R->capTiles) {
+        R->capTiles = 0;
         PPPM_CUDA_TRY(grow(&R->tstart, tiles));
         PPPM_CUDA_TRY(grow(&R->tend, tiles));
         R->capTiles = tiles;
@@ -520,9 +526,9 @@ extern "C" pppm_status pppm_renderer_create(void *stream, pppm_renderer **out) {
     pppm_renderer *R = new pppm_renderer;
     R->stream = (cudaStream_t)stream;
     cudaGetDevice(&R->device);
-    cudaError_t e = cudaMalloc(&R->red, sizeof(float) * 6 * pppm::kRedBlocks);
-    if (e == cudaSuccess) e = cudaMallocHost(&R->host_red, sizeof(float) * 6 * pppm::kRedBlocks);
-    if (e == cudaSuccess) e = cudaMallocHost(&R->host_u32, sizeof(uint32_t) * 4);
+    cudaError_t e = ::pppm::device_malloc((void **)&R->red, sizeof(float) * 6 * pppm::kRedBlocks);
+    if (e == cudaSuccess) e = ::pppm::host_malloc((void **)&R->host_red, sizeof(float) * 6 * pppm::kRedBlocks);
+    if (e == cudaSuccess) e = ::pppm::host_malloc((void **)&R->host_u32, sizeof(uint32_t) * 4);
     if (e != cudaSuccess) {
         pppm_set_error("pppm_renderer_create: %s", cudaGetErrorString(e));
         pppm_renderer_destroy(R);
@@ -628,6 +634,8 @@ extern "C" pppm_status pppm_render_shadows(pppm_renderer *R, uint32_t n, const f
     const uint32_t cells = (uint32_t)npix * (uint32_t)npix;
     if (cells > R->capMap) {
         std::lock_guard<std::recursive_mutex> lk(device_lock());
+        R->capMap = 0;
+        R->npix = 0;   // no shadow map until this one is drawn
         e = grow(&R->map, cells);
         if (e != cudaSuccess) return render_fail("pppm_render_shadows (map)", e);
         R->capMap = cells;

@@ -120,9 +120,9 @@ pppm_status make_resident(SceneRec &r, cudaStream_t st) {
     std::unique_lock<std::recursive_mutex> lk(pppm::device_lock());
     pppm_status rc = pppm_scene_create(&r.prm, r.N, r.N, st, &r.scene);
     if (rc != PPPM_OK) return rc;
-    cudaError_t e = cudaMalloc(&r.dpos, sizeof(float) * 4 * (size_t)r.N);
-    if (e == cudaSuccess) e = cudaMalloc(&r.dalpha, sizeof(double) * 3 * (size_t)r.N);
-    if (e == cudaSuccess) e = cudaMalloc(&r.dvel, sizeof(double) * 3 * (size_t)r.N);
+    cudaError_t e = ::pppm::device_malloc((void **)&r.dpos, sizeof(float) * 4 * (size_t)r.N);
+    if (e == cudaSuccess) e = ::pppm::device_malloc((void **)&r.dalpha, sizeof(double) * 3 * (size_t)r.N);
+    if (e == cudaSuccess) e = ::pppm::device_malloc((void **)&r.dvel, sizeof(double) * 3 * (size_t)r.N);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(r.dpos, r.pos.data(), sizeof(float) * 4 * (size_t)r.N, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
