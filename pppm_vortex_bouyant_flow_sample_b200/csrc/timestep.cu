@@ -24,7 +24,8 @@
 // conversion, the move, the midpoint and the strength update are fused into
 // two elementwise kernels.  The smoothing walks the vortices in hash order, a
 // warp at a time, staging 32 records of a cell in shared memory as 16 record
-// pairs that Blackwell's packed f32x2 instructions process two at a time, and
+// pairs that Blackwell's packed f32x2 instructions process two at a time, in
+// coordinates scaled so that the squared distance is the exponent of 2^x, and
 // sums the weights in FP32 per staged chunk and in FP64 across chunks.
 #include <cmath>
 
@@ -191,8 +192,11 @@ __global__ void __launch_bounds__(kSmoothThreads) gaussian_smooth_kernel(
     const int zhi = min(__reduce_max_sync(0xffffffffu, ck) + 2, n - 1);
 
     double tw = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
-    const float2 tx = make_float2(ra.x, ra.x), ty = make_float2(ra.y, ra.y), tz = make_float2(ra.z, ra.z);
-    const float2 ws2 = make_float2(wscale, wscale);
+    // the staged walk works in coordinates scaled by sg = sqrt(-wscale), so
+    // that the squared scaled distance is the (negated) exponent itself
+    const float sg = sqrtf(-wscale);
+    const float2 tx = make_float2(ra.x * sg, ra.x * sg), ty = make_float2(ra.y * sg, ra.y * sg),
+                 tz = make_float2(ra.z * sg, ra.z * sg);
     auto walk = [&](int x0, int x1, int y0, int y1, int z0, int z1, bool member) {
         for (int z = z0; z <= z1; z++)
             for (int y = y0; y <= y1; y++)
@@ -212,7 +216,7 @@ __global__ void __launch_bounds__(kSmoothThreads) gaussian_smooth_kernel(
                         if ((uint32_t)lane < cnt) {
                             const float4 b = vrec[base + lane];
                             const float4 al = valf[base + lane];
-                            stage_pair(pk, lane >> 1, lane & 1, -b.x, -b.y, -b.z, al.x, al.y, al.z);
+                            stage_pair(pk, lane >> 1, lane & 1, -b.x * sg, -b.y * sg, -b.z * sg, al.x, al.y, al.z);
                         } else if ((uint32_t)lane == cnt && (cnt & 1u)) {
                             stage_pair(pk, lane >> 1, 1, 1e18f, 1e18f, 1e18f, 0.f, 0.f, 0.f);
                         }
@@ -220,6 +224,7 @@ __global__ void __launch_bounds__(kSmoothThreads) gaussian_smooth_kernel(
                         if (ok) {
                             float2 pw = make_float2(0.f, 0.f), px = pw, py = pw, pz = pw;
                             const uint32_t np = (cnt + 1) >> 1;
+#pragma unroll 4
                             for (uint32_t p = 0; p < np; p++) {
                                 const float4 A = s_pk[wpk + p], B = s_pk[wpk + kSlots + p];
                                 const float4 Cc = s_pk[wpk + 2 * kSlots + p];
@@ -227,8 +232,7 @@ __global__ void __launch_bounds__(kSmoothThreads) gaussian_smooth_kernel(
                                 const float2 dy = __fadd2_rn(ty, make_float2(A.z, A.w));
                                 const float2 dz = __fadd2_rn(tz, make_float2(B.x, B.y));
                                 const float2 dsq = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
-                                const float2 arg = __fmul2_rn(dsq, ws2);
-                                const float2 w = make_float2(ex2_approx(arg.x), ex2_approx(arg.y));
+                                const float2 w = make_float2(ex2_approx(-dsq.x), ex2_approx(-dsq.y));
                                 pw = __fadd2_rn(pw, w);
                                 px = __ffma2_rn(w, make_float2(B.z, B.w), px);
                                 py = __ffma2_rn(w, make_float2(Cc.x, Cc.y), py);
