@@ -215,10 +215,12 @@ pppm_status pppm_get_stats(pppm_scene *s, uint64_t *pairs, int32_t *mg_cycles,
 pppm_status pppm_count_pairs(pppm_scene *s, uint32_t M, const float *eval_a4_dev,
                              uint64_t *pairs);
 
-/* Per-stage timing with CUDA events on the scene stream (off by default;
- * no reference counterpart — the reference prints no timings).  Stages:
- * 0 domain, 1 vort_sort, 2 cells_reorder, 3 p2m, 4 multigrid, 5 farfield,
- * 6 eval_sort, 7 eval.  pppm_get_stage_times synchronises the stream and
+/* Per-stage timing with CUDA events on the scene stream (off by default, on
+ * from creation when the environment variable PPPM_PROFILE is set to anything
+ * but "" or "0"; no reference counterpart — the reference prints no timings).
+ * Stages: 0 domain, 1 vort_sort, 2 cells_reorder, 3 p2m, 4 multigrid,
+ * 5 farfield, 6 eval_sort, 7 eval, 8 segments, 9 seg_to_blob, 10 rehash,
+ * 11 gaussian_smooth.  pppm_get_stage_times synchronises the stream and
  * writes the last recorded duration of each stage in ms (-1 = not run). */
 pppm_status pppm_scene_set_profiling(pppm_scene *s, int on);
 const char *pppm_stage_name(int stage);

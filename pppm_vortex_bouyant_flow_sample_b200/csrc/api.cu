@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "pppm_internal.cuh"
@@ -326,6 +327,11 @@ extern "C" pppm_status pppm_scene_create(const pppm_params *p, uint32_t cap_vort
     s->prm = *p;
     s->n = p->n;
     s->stream = (cudaStream_t)stream;
+    {
+        // PPPM_PROFILE set to anything but "" or "0": stage timing from creation on
+        const char *env = std::getenv("PPPM_PROFILE");
+        s->profiling = env && env[0] && std::strcmp(env, "0") != 0;
+    }
     cudaGetDevice(&s->device);
     cudaError_t e = alloc_grid_side(s);
     if (e == cudaSuccess) e = alloc_vortex_side(s, cap_vort ? cap_vort : 1);

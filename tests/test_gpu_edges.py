@@ -168,3 +168,26 @@ def test_grid_256_ring_subsample(pb, oracle):
     assert pairs == int(d["pairs"][0])
     assert rel_l2(u, ref) <= VEL_TOL
     scene.close()
+
+
+def test_profile_environment_switch(pb, monkeypatch):
+    """PPPM_PROFILE=1 turns stage timing on at scene creation; unset (or "0")
+    it stays off until set_profiling."""
+    import torch
+    from pppm_vortex_bouyant_flow_sample_b200 import workloads as W
+    pos, al = W.uniform_cloud(4000, seed=6)
+    dpos = torch.from_numpy(pos).cuda()
+    dal = torch.from_numpy(np.ascontiguousarray(al)).cuda()
+    for env, timed in (("1", True), ("0", False), (None, False)):
+        if env is None:
+            monkeypatch.delenv("PPPM_PROFILE", raising=False)
+        else:
+            monkeypatch.setenv("PPPM_PROFILE", env)
+        scene = pb.Scene(16, cap_vort=len(pos), cap_eval=len(pos))
+        scene.set_vortices(dpos, dal)
+        scene.build_far_field()
+        scene.eval(dpos, dpos, 1)
+        st = scene.stage_times()
+        scene.close()
+        assert (st["eval"] > 0 and st["multigrid"] > 0) == timed, (env, st)
+        assert (min(st[k] for k in ("domain", "p2m", "farfield", "eval")) >= 0) == timed
