@@ -191,10 +191,15 @@ def test_potential_outruns_reference_kernels(refgpu):
     origin, L = np.asarray(grids["origin"]), grids["length"]
     h_f = np.float32(L / n)
     _, idx, s, e, hash_ms = refgpu.hash_particles(n, h_f, origin.astype(np.float32), src)
-    R = None
-    for _ in range(2):
-        R = refgpu.potential(n, K, src[idx], mass[idx], mass, s, e, grids["phi"].numpy(), origin, h_f, L, ev)
-    theirs = dict(R["stage_ms"], hash=hash_ms)
+    hash_ms = min(hash_ms, refgpu.hash_particles(n, h_f, origin.astype(np.float32), src)[4])
+    # the reference's far-field stage builds its table on the host and copies
+    # it per call, so its time varies from run to run: each stage takes its
+    # fastest of three runs after a warm-up run
+    runs = [refgpu.potential(n, K, src[idx], mass[idx], mass, s, e, grids["phi"].numpy(), origin, h_f, L, ev)
+            for _ in range(4)][1:]
+    R = runs[-1]
+    theirs = {k: min(r["stage_ms"][k] for r in runs) for k in R["stage_ms"]}
+    theirs["hash"] = hash_ms
     t_ref = sum(theirs.values())
     t_ours = float(np.median(ms))
     rel = float(np.linalg.norm(g - R["out"]) / np.linalg.norm(R["out"]))
