@@ -780,6 +780,9 @@ struct pppm_mg {
     pppm::MGPlan plan;
     float *pool = nullptr;
     double *r64 = nullptr, *e64 = nullptr;  // residual of the initial guess, its correction
+    double *coarse_op = nullptr;            // coarsest-level operator (levels >= 2)
+    cudaGraphExec_t graph = nullptr;        // reference-schedule solve of r64 into e64, captured on first use
+    unsigned graph_kernels = 0;
     uint32_t n = 0;
 };
 
@@ -836,12 +839,21 @@ extern "C" pppm_status pppm_mg_create(uint32_t n, void *stream, pppm_mg **out) {
     if (e == cudaSuccess) e = dalloc(&P.norms, 2);
     if (e == cudaSuccess) e = dalloc(&m->r64, P.lv[0].cells);
     if (e == cudaSuccess) e = dalloc(&m->e64, P.lv[0].cells);
+    if (e == cudaSuccess && P.levels >= 2) {
+        // the coarsest solve from x = 0 as one precomputed linear map, as for scenes
+        const uint32_t cc = P.lv[P.levels - 1].cells;
+        e = dalloc(&m->coarse_op, (size_t)cc * cc);
+        if (e == cudaSuccess) e = pppm::build_coarse_operator((int)P.lv[P.levels - 1].d, m->coarse_op, P.st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(P.st);
+        P.coarse_op = m->coarse_op;
+    }
     if (e != cudaSuccess) {
         pppm_status st = cuda_fail("pppm_mg_create", e);
         cudaFree(m->pool);
         cudaFree(P.norms);
         cudaFree(m->r64);
         cudaFree(m->e64);
+        cudaFree(m->coarse_op);
         delete m;
         return st;
     }
@@ -858,10 +870,12 @@ extern "C" pppm_status pppm_mg_destroy(pppm_mg *m) {
     if (!m) return PPPM_OK;
     if (m->plan.st) cudaStreamSynchronize(m->plan.st);
     std::lock_guard<std::recursive_mutex> lk(pppm::device_lock());
+    if (m->graph) cudaGraphExecDestroy(m->graph);
     cudaFree(m->pool);
     cudaFree(m->plan.norms);
     cudaFree(m->r64);
     cudaFree(m->e64);
+    cudaFree(m->coarse_op);
     delete m;
     return PPPM_OK;
 }
@@ -887,7 +901,19 @@ extern "C" pppm_status pppm_mg_full_multigrid(pppm_mg *m, double *x, const doubl
     cudaError_t e = cudaGetLastError();
     int cyc = 0;
     double rel = -1.0;
-    if (e == cudaSuccess) e = pppm::mg_solve(P, mode, tol, max_cycles > 0 ? max_cycles : 1, &cyc, &rel);
+    if (e == cudaSuccess && mode == PPPM_MG_REFERENCE) {
+        // the fixed schedule touches only this object's buffers: one graph
+        // launch, captured on first use
+        if (!m->graph) {
+            std::lock_guard<std::recursive_mutex> lk(pppm::device_lock());
+            e = pppm::mg_capture_graph(P, &m->graph, &m->graph_kernels);
+            if (e != cudaSuccess) m->graph = nullptr;
+        }
+        if (e == cudaSuccess) e = cudaGraphLaunch(m->graph, P.st);
+        for (unsigned q = 0; e == cudaSuccess && q < m->graph_kernels; q++) ::pppm::note_launch();
+    } else if (e == cudaSuccess) {
+        e = pppm::mg_solve(P, mode, tol, max_cycles > 0 ? max_cycles : 1, &cyc, &rel);
+    }
     if (e == cudaSuccess) {
         ::pppm::note_launch();
         add64_kernel<<<(unsigned)((C + 255) / 256), 256, 0, P.st>>>(x, m->e64, C);
