@@ -1,6 +1,7 @@
 """ctypes bindings of oracle/_ref/librefgpu.so: the reference's own GPU kernels
-(hybridFastSummation/GPU_kernel.cu, particle_hash/particle_hash_kernel.cu)
-behind ref_gpu/ref_gpu_shim.cu and ref_gpu/ref_hash_shim.cu, built by
+(hybridFastSummation/GPU_kernel.cu, particle_hash/particle_hash_kernel.cu,
+multigrid/MultiGrid_kernel.cu) behind ref_gpu/ref_gpu_shim.cu,
+ref_gpu/ref_hash_shim.cu and ref_gpu/ref_mg_shim.cu, built by
 `make -C oracle refgpu` where the reference's sources are present.  TEST
 INFRASTRUCTURE ONLY: the parity tests run it on the GPU as a checker of the
 oracle and of the product; the product never loads it.
@@ -54,8 +55,9 @@ def lib():
         L.refgpu_potential.argtypes = [C.c_uint32, C.c_int, C.c_uint32, f32p, f64p, f64p, u32p, u32p, f64p, f64p,
                                        C.c_float, C.c_double, C.c_uint32, f32p, C.c_int, C.c_void_p, C.c_void_p,
                                        f64p, f64p, f64p, f64p, C.c_void_p, f32p]
+        L.refgpu_mg_fmg.argtypes = [C.c_uint32, C.c_uint32, f64p, f64p]
         for name in ("refgpu_segments", "refgpu_segment_update", "refgpu_gaussian_smooth", "refgpu_baroclinic",
-                     "refgpu_potential"):
+                     "refgpu_potential", "refgpu_mg_fmg"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -218,3 +220,13 @@ def potential(n, K, sorted_pos4, sorted_mass, mass, start, end, phi, origin, h_f
     if dp is not None:
         out["dphidn"] = dp
     return out
+
+
+def mg_fmg(n, b):
+    """The reference's FP64 full multigrid (its own kernels, its V(4,4) / FMG
+    schedule and its racing coarsest solve) from x = 0 for each right-hand side
+    b[c] (shape (comps, n^3), FP64); returns x of the same shape."""
+    b = np.ascontiguousarray(b, dtype=np.float64).reshape(-1, n ** 3)
+    x = np.zeros_like(b)
+    _check(lib().refgpu_mg_fmg(n, b.shape[0], b, x), "refgpu_mg_fmg")
+    return x
