@@ -28,6 +28,30 @@ struct Dims {
     size_t cells() const { return (size_t)x * y * z; }
 };
 
+// Device time of every launch and memset when timing is on: each is
+// bracketed by CUDA events (the bindings synchronise the device anyway).
+bool g_time = false;
+double g_ms = 0.0;
+template <class F>
+void timed(F f) {
+    if (!g_time) {
+        f();
+        return;
+    }
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a);
+    f();
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    float t = 0.f;
+    cudaEventElapsedTime(&t, a, b);
+    g_ms += t;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+}
+
 // the texture stand-in reads through a managed pointer: no launch may still be
 // reading the old binding when it changes
 void bind(const void *p, const textureReference *t) {
@@ -47,12 +71,16 @@ void rbgs(double *x, double *b, int t, const Dims &d) {
         bind(b, &b_level_tex_double);
         const dim3 threads(32, 16);
         const dim3 blocks = grid_for(d);
-        red_sweep_GS_periodic_kerneld_type2<<<blocks, threads>>>(
-            x, d.x, d.y, d.z, 1.0 / (double)d.y, 1.0 / (double)(d.x * d.y), d.x * d.y, d.x, d.x - 1,
-            (d.y - 1) * d.x, (d.z - 1) * d.x * d.y, 1.0 / 6.0, 0, 0, (uint)d.cells());
-        black_sweep_GS_periodic_kerneld_type2<<<blocks, threads>>>(
-            x, d.x, d.y, d.z, 1.0 / (double)d.y, 1.0 / (double)(d.x * d.y), d.x * d.y, d.x, d.x - 1,
-            (d.y - 1) * d.x, (d.z - 1) * d.x * d.y, 1.0 / 6.0, 0, 0, (uint)d.cells());
+        timed([&] {
+            red_sweep_GS_periodic_kerneld_type2<<<blocks, threads>>>(
+                x, d.x, d.y, d.z, 1.0 / (double)d.y, 1.0 / (double)(d.x * d.y), d.x * d.y, d.x, d.x - 1,
+                (d.y - 1) * d.x, (d.z - 1) * d.x * d.y, 1.0 / 6.0, 0, 0, (uint)d.cells());
+        });
+        timed([&] {
+            black_sweep_GS_periodic_kerneld_type2<<<blocks, threads>>>(
+                x, d.x, d.y, d.z, 1.0 / (double)d.y, 1.0 / (double)(d.x * d.y), d.x * d.y, d.x, d.x - 1,
+                (d.y - 1) * d.x, (d.z - 1) * d.x * d.y, 1.0 / 6.0, 0, 0, (uint)d.cells());
+        });
     }
 }
 
@@ -60,32 +88,40 @@ void rbgs(double *x, double *b, int t, const Dims &d) {
 void residual(double *x, double *b, double *r, const Dims &d) {
     bind(x, &x_level_tex_double);
     bind(b, &b_level_tex_double);
-    compute_residual_periodic_kernel2<<<grid_for(d), dim3(32, 16)>>>(
-        x, b, r, d.x, d.y, d.z, 1.0 / (double)d.y, 1.0 / (double)(d.x * d.y), d.x * d.y, d.x, d.x - 1,
-        (d.y - 1) * d.x, (d.z - 1) * d.x * d.y, 1.0 / 6.0, 0, 0, (uint)d.cells());
+    timed([&] {
+        compute_residual_periodic_kernel2<<<grid_for(d), dim3(32, 16)>>>(
+            x, b, r, d.x, d.y, d.z, 1.0 / (double)d.y, 1.0 / (double)(d.x * d.y), d.x * d.y, d.x, d.x - 1,
+            (d.y - 1) * d.x, (d.z - 1) * d.x * d.y, 1.0 / 6.0, 0, 0, (uint)d.cells());
+    });
 }
 
 // mg_RestrictionPeriodic3D2 (Multigrid.cu:275-301): next from the fine r
 void restrict_to(double *next, double *cur, const Dims &nd) {
     bind(cur, &b_level_tex_double);
-    restriction_periodic_kernel2<<<grid_for(nd), dim3(32, 16)>>>(
-        next, nd.x, nd.y, nd.z, 1.0 / (double)nd.y, 1.0 / (double)(nd.x * nd.y), nd.x * nd.y * 4, nd.x * 2,
-        nd.x - 1, (nd.y - 1) * nd.x, (nd.z - 1) * nd.x * nd.y, 1.0 / 6.0, 0, (uint)nd.cells());
+    timed([&] {
+        restriction_periodic_kernel2<<<grid_for(nd), dim3(32, 16)>>>(
+            next, nd.x, nd.y, nd.z, 1.0 / (double)nd.y, 1.0 / (double)(nd.x * nd.y), nd.x * nd.y * 4, nd.x * 2,
+            nd.x - 1, (nd.y - 1) * nd.x, (nd.z - 1) * nd.x * nd.y, 1.0 / 6.0, 0, (uint)nd.cells());
+    });
 }
 
 // mg_ProlongationPeriodic3D2 (Multigrid.cu:303-330): next += coarse
 void prolong_into(double *next, double *coarse, const Dims &nd) {
     bind(coarse, &x_level_tex_double);
-    prolongation_periodic_kernel2<<<grid_for(nd), dim3(32, 16)>>>(
-        next, nd.x, nd.y, nd.z, 1.0 / (double)nd.y, 1.0 / (double)(nd.x * nd.y), nd.x * nd.y / 4, nd.x / 2,
-        nd.x - 1, (nd.y - 1) * nd.x, (nd.z - 1) * nd.x * nd.y, 1.0 / 6.0, 0, (uint)nd.cells());
+    timed([&] {
+        prolongation_periodic_kernel2<<<grid_for(nd), dim3(32, 16)>>>(
+            next, nd.x, nd.y, nd.z, 1.0 / (double)nd.y, 1.0 / (double)(nd.x * nd.y), nd.x * nd.y / 4, nd.x / 2,
+            nd.x - 1, (nd.y - 1) * nd.x, (nd.z - 1) * nd.x * nd.y, 1.0 / 6.0, 0, (uint)nd.cells());
+    });
 }
 
 // mg_exact_periodic3D2 (Multigrid.cu:46-55)
 void exact(double *x, double *b, double *res, const Dims &d) {
     cudaDeviceSynchronize();
-    exact_solve_period3D_jacobi_kerneld<<<1, std::min<int>(512, (int)d.cells())>>>(b, x, res, d.x, d.y, d.z,
-                                                                                   (uint)d.cells());
+    timed([&] {
+        exact_solve_period3D_jacobi_kerneld<<<1, std::min<int>(512, (int)d.cells())>>>(b, x, res, d.x, d.y, d.z,
+                                                                                       (uint)d.cells());
+    });
 }
 
 struct Solver {
@@ -93,7 +129,9 @@ struct Solver {
     std::vector<double *> xk, bk, rk;
     int L = 0;
 
-    void zero(double *p, const Dims &d) { cudaMemset(p, 0, sizeof(double) * d.cells()); }
+    void zero(double *p, const Dims &d) {
+        timed([&] { cudaMemset(p, 0, sizeof(double) * d.cells()); });
+    }
 
     // MultiGridSolver3DPeriod_double::m_Vcycle (MultiGrid.cpp:128-201)
     void vcycle(double *x, double *b, int level) {
@@ -149,9 +187,12 @@ struct Solver {
 
 // Solves sum_nbr(x) - 6x = b (zero ghost values) for comps right-hand sides
 // on an n^3 grid, each from x = 0 by one full multigrid, as m_SolvePoisson
-// does per component.  b_host, x_host: [comps][n^3] FP64.  Returns 0 or a CUDA
-// error code.
-extern "C" int refgpu_mg_fmg(uint32_t n, uint32_t comps, const double *b_host, double *x_host) {
+// does per component.  b_host, x_host: [comps][n^3] FP64.  ms (may be NULL):
+// the summed device time of the solves' launches and memsets.  Returns 0 or a
+// CUDA error code.
+extern "C" int refgpu_mg_fmg(uint32_t n, uint32_t comps, const double *b_host, double *x_host, float *ms) {
+    g_time = ms != nullptr;
+    g_ms = 0.0;
     Solver S;
     // MultiGrid<T>::m_ComputeLevels (MultiGrid.h:114-127)
     Dims d{(int)n, (int)n, (int)n};
@@ -190,7 +231,7 @@ extern "C" int refgpu_mg_fmg(uint32_t n, uint32_t comps, const double *b_host, d
         const size_t C = S.sys[0].cells();
         for (uint32_t c = 0; c < comps && rc == 0; c++) {
             cudaMemcpy(b0, b_host + c * C, sizeof(double) * C, cudaMemcpyHostToDevice);
-            cudaMemset(x0, 0, sizeof(double) * C);
+            timed([&] { cudaMemset(x0, 0, sizeof(double) * C); });   // m_SolvePoisson: psi = 0
             S.fmg(x0, b0);
             cudaError_t e = cudaDeviceSynchronize();
             if (e == cudaSuccess) e = cudaMemcpy(x_host + c * C, x0, sizeof(double) * C, cudaMemcpyDeviceToHost);
@@ -200,5 +241,7 @@ extern "C" int refgpu_mg_fmg(uint32_t n, uint32_t comps, const double *b_host, d
         rc = (int)cudaErrorMemoryAllocation;
     }
     for (double *p : owned) cudaFree(p);
+    if (ms) *ms = (float)g_ms;
+    g_time = false;
     return rc;
 }
