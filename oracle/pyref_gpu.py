@@ -55,7 +55,7 @@ def lib():
         L.refgpu_potential.argtypes = [C.c_uint32, C.c_int, C.c_uint32, f32p, f64p, f64p, u32p, u32p, f64p, f64p,
                                        C.c_float, C.c_double, C.c_uint32, f32p, C.c_int, C.c_void_p, C.c_void_p,
                                        f64p, f64p, f64p, f64p, C.c_void_p, f32p]
-        L.refgpu_mg_fmg.argtypes = [C.c_uint32, C.c_uint32, f64p, f64p, C.c_void_p]
+        L.refgpu_mg_fmg.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, f64p, f64p, C.c_void_p]
         for name in ("refgpu_segments", "refgpu_segment_update", "refgpu_gaussian_smooth", "refgpu_baroclinic",
                      "refgpu_potential", "refgpu_mg_fmg"):
             getattr(L, name).restype = C.c_int
@@ -222,15 +222,16 @@ def potential(n, K, sorted_pos4, sorted_mass, mass, start, end, phi, origin, h_f
     return out
 
 
-def mg_fmg(n, b, timing=None):
+def mg_fmg(n, b, timing=None, repeats=1):
     """The reference's FP64 full multigrid (its own kernels, its V(4,4) / FMG
     schedule and its racing coarsest solve) from x = 0 for each right-hand side
-    b[c] (shape (comps, n^3), FP64); returns x of the same shape.  timing (a
-    dict, optional) receives "ms": the summed device time of its launches."""
+    b[c] (shape (comps, n^3), FP64), repeated `repeats` times from the x the
+    previous call left; returns x of the same shape.  timing (a dict, optional)
+    receives "ms": the summed device time of its launches."""
     b = np.ascontiguousarray(b, dtype=np.float64).reshape(-1, n ** 3)
     x = np.zeros_like(b)
     ms = np.zeros(1, np.float32)
-    _check(lib().refgpu_mg_fmg(n, b.shape[0], b, x, ms.ctypes.data if timing is not None else None),
+    _check(lib().refgpu_mg_fmg(n, b.shape[0], repeats, b, x, ms.ctypes.data if timing is not None else None),
            "refgpu_mg_fmg")
     if timing is not None:
         timing["ms"] = float(ms[0])

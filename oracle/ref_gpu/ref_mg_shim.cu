@@ -186,11 +186,14 @@ struct Solver {
 }  // namespace
 
 // Solves sum_nbr(x) - 6x = b (zero ghost values) for comps right-hand sides
-// on an n^3 grid, each from x = 0 by one full multigrid, as m_SolvePoisson
-// does per component.  b_host, x_host: [comps][n^3] FP64.  ms (may be NULL):
-// the summed device time of the solves' launches and memsets.  Returns 0 or a
-// CUDA error code.
-extern "C" int refgpu_mg_fmg(uint32_t n, uint32_t comps, const double *b_host, double *x_host, float *ms) {
+// on an n^3 grid, each from x = 0 by `repeats` full multigrids in a row, each
+// from the x the previous one left: BiotSavartSolver::m_SolvePoisson runs one
+// per component, PotentialFieldSolver::m_SolvePoisson three
+// (HFS/PotentialFieldSolver.cpp:610-619).  b_host, x_host: [comps][n^3] FP64.
+// ms (may be NULL): the summed device time of the solves' launches and
+// memsets.  Returns 0 or a CUDA error code.
+extern "C" int refgpu_mg_fmg(uint32_t n, uint32_t comps, uint32_t repeats, const double *b_host, double *x_host,
+                             float *ms) {
     g_time = ms != nullptr;
     g_ms = 0.0;
     Solver S;
@@ -232,7 +235,7 @@ extern "C" int refgpu_mg_fmg(uint32_t n, uint32_t comps, const double *b_host, d
         for (uint32_t c = 0; c < comps && rc == 0; c++) {
             cudaMemcpy(b0, b_host + c * C, sizeof(double) * C, cudaMemcpyHostToDevice);
             timed([&] { cudaMemset(x0, 0, sizeof(double) * C); });   // m_SolvePoisson: psi = 0
-            S.fmg(x0, b0);
+            for (uint32_t r = 0; r < repeats; r++) S.fmg(x0, b0);
             cudaError_t e = cudaDeviceSynchronize();
             if (e == cudaSuccess) e = cudaMemcpy(x_host + c * C, x0, sizeof(double) * C, cudaMemcpyDeviceToHost);
             if (e != cudaSuccess) rc = (int)e;

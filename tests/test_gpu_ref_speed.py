@@ -221,13 +221,22 @@ def test_potential_outruns_reference_kernels(refgpu):
     R = runs[-1]
     theirs = {k: min(r["stage_ms"][k] for r in runs) for k in R["stage_ms"]}
     theirs["hash"] = hash_ms
+    # the reference's FP64 multigrid, three full multigrids in a row as its
+    # m_SolvePoisson runs them, on this build's right-hand side (equal to the
+    # reference's to round-off, tests/test_gpu_ref_kernels.py)
+    t = {}
+    phi_ref = refgpu.mg_fmg(n, grids["rhs"].numpy()[None, :], timing=t, repeats=3)[0]
     t_ref = sum(theirs.values())
     t_ours = float(np.median(ms))
     rel = float(np.linalg.norm(g - R["out"]) / np.linalg.norm(R["out"]))
     table = {"workload": f"scalar PPPM gradient, {Ns:,} sphere sources, {n}^3, {M:,} points",
              "reference_kernels_ms_without_multigrid": theirs, "reference_total_ms": t_ref,
              "this_build_total_ms_with_multigrid": t_ours, "speedup": t_ref / t_ours,
-             "rel_l2_gradient_vs_reference_kernels": rel}
+             "rel_l2_gradient_vs_reference_kernels": rel, "reference_multigrid_ms": t["ms"],
+             "reference_total_with_multigrid_ms": t_ref + t["ms"],
+             "speedup_with_multigrid": (t_ref + t["ms"]) / t_ours,
+             "rel_l2_phi_vs_reference_multigrid": float(np.linalg.norm(grids["phi"].numpy() - phi_ref)
+                                                        / np.linalg.norm(phi_ref))}
     print(json.dumps(table, indent=1))
     dest = os.environ.get("PPPM_TIMING_OUT")
     if dest:
