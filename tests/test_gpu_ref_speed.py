@@ -243,6 +243,7 @@ def test_potential_outruns_reference_kernels(refgpu):
         with open(dest.replace(".json", "_potential.json"), "w") as f:
             json.dump(table, f, indent=1)
     assert rel <= 1e-5
+    assert table["rel_l2_phi_vs_reference_multigrid"] <= 1e-8   # three chained solves: the race washes out
     assert t_ours < t_ref
 
 
