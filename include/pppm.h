@@ -412,15 +412,26 @@ pppm_status pppm_hasher_deorder(pppm_hasher *h, uint32_t N, const void *in_dev, 
 
 /* ---- spatial hash that allocates nothing ---------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
- * memory on this path (inside stream capture, under an allocator that must
- * not grow, or when another framework owns the device heap): the same result
- * as pppm_hasher_run (sorted keys, sorted original indices, cell start/end
- * tables of n^3 entries) into caller-provided device arrays, with the sort's
- * scratch in a fixed device array of PPPM_NOALLOC_SCRATCH_BYTES that every
- * GPU loading the library keeps until the process exits.
- *   - N must not exceed PPPM_NOALLOC_MAX_PARTICLES (else PPPM_ERR_INVALID).
- *   - The first call on a device looks up the array's device address; make
- *     that first call before any stream capture on that device.
+ * memory on this path: a simulation loop with a fixed per-frame budget, where
+ * cudaMalloc / cudaFree would synchronise the device and stall the frame; a
+ * host whose device allocator has a fixed size and must not grow; or a
+ * process in which another framework's pool already owns the device heap.
+ * It gives the same result as pppm_hasher_run into caller-provided device
+ * arrays, with the sort's scratch in a fixed device array of
+ * PPPM_NOALLOC_SCRATCH_BYTES that every GPU loading the library keeps until
+ * the process exits.
+ *   - pos4_dev: N float4 records (x, y, z, w; 16-byte stride, w ignored).
+ *   - sorted_key_dev, sorted_idx_dev: N entries each (cell keys in sorted
+ *     order, original indices in the same order).
+ *   - cell_start_dev, cell_end_dev: n^3 entries each; every entry is written
+ *     (0xFFFFFFFF for empty cells, filled first, then the occupied cells, in
+ *     stream order), so they need no initialisation.
+ *   - N must not exceed PPPM_NOALLOC_MAX_PARTICLES (else PPPM_ERR_INVALID,
+ *     before any device work).
+ *   - The first call on a device looks up the array's device address and
+ *     keeps it for the process; make that first call before any stream
+ *     capture on that device.  After cudaDeviceReset on that device the kept
+ *     address is stale: do not call this entry point again in that process.
  *   - All calls share the array: calls whose work overlaps on the GPU (other
  *     streams, other threads) race and corrupt each other's results.
  *   - No cudaMalloc, cudaFree or allocating library routine is called. */

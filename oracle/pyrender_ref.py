@@ -24,8 +24,9 @@ def available() -> bool:
 
 def build() -> bool:
     """Compile the reference renderer when its sources are present; True if the library exists."""
-    src = os.environ.get("PPPM_REFERENCE_ROOT", "/root/reference")
-    if os.path.isdir(src):
+    from oracle.refroot import reference_root
+    src = reference_root()
+    if src:
         subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF_ROOT={src}"], check=True)
     return available()
 

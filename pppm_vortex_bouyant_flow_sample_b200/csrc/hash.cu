@@ -626,9 +626,10 @@ extern "C" pppm_status pppm_hasher_deorder(pppm_hasher *h, uint32_t N, const voi
 // ---------------------------------------------------------------------------
 // Spatial hash that allocates nothing.
 //
-// For callers that cannot call cudaMalloc on this path: code running inside a
-// stream-capture region, under a host allocator that must not grow, or in a
-// process whose device memory is handed out by another framework.  The caller
+// For callers that cannot call cudaMalloc on this path: a simulation loop with
+// a fixed per-frame budget (cudaMalloc / cudaFree synchronise the device), a
+// host whose device allocator must not grow, or a process whose device memory
+// is handed out by another framework's pool.  The caller
 // passes the positions and the four output arrays; the radix sort's second
 // key/index buffer and its digit histograms live in the fixed device array
 // below, which every GPU that loads this library holds until the process

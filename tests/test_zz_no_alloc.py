@@ -1,9 +1,14 @@
 """pppm_spatial_hash_noalloc: the spatial hash for callers that cannot
-allocate device memory (inside stream capture, under a fixed allocator, or
-when another framework owns the device heap).  It must give exactly what the
+allocate device memory (a simulation loop whose frame budget cannot absorb the
+device synchronisation of cudaMalloc, an allocator of fixed size, or a device
+heap owned by another framework's pool).  It must give exactly what the
 allocating entry point pppm_hasher_run gives — sorted keys, sorted indices and
 cell start/end tables are integer results, so the comparison is bit-exact —
-on two calls in a row, whatever the shared scratch holds from before.
+on two calls in a row, whatever the shared scratch holds from before.  A small
+case is also checked against the CPU oracle's hash (its own keys, stable sort
+and cell tables), so a fault shared by both GPU entry points cannot hide, and
+a call made while every library allocation is armed to fail must still
+succeed: it allocates nothing.
 
 This file is collected last so that a run stopping at the first failure has
 already run every other test."""
@@ -99,3 +104,26 @@ def test_noalloc_rejects_oversize_without_touching_gpu(env):
                                        *[C.c_void_p(t.data_ptr()) for t in outs], None)
     assert rc == 1  # PPPM_ERR_INVALID
     assert b"exceeds the fixed scratch limit" in lib.pppm_last_error()
+
+
+def test_noalloc_matches_oracle_and_allocates_nothing(env):
+    lib, torch = env
+    from oracle import pyoracle as O
+    n, N = 32, 20_000
+    rng = np.random.default_rng(7)
+    pos = np.zeros((N, 4), np.float32)
+    pos[:, :3] = rng.random((N, 3), dtype=np.float32) * np.float32(0.9) + np.float32(0.03)
+    h, origin = np.float32(1.0 / n), np.array([0.0, 0.0, 0.0], np.float32)
+    dpos = torch.from_numpy(pos).cuda()
+    _noalloc(lib, torch, dpos, n, float(h), origin)  # warm: the scratch address is looked up once
+    key, idx = O.calc_hash(pos, n, h, origin)
+    skey, sidx = O.sort_by_key(key, idx)
+    start, end = O.find_cell_start(skey, n ** 3)
+    lib.pppm_debug_fail_allocation.argtypes = [C.c_int64]
+    lib.pppm_debug_fail_allocation(0)  # the next library allocation, if any, fails
+    try:
+        got = _noalloc(lib, torch, dpos, n, float(h), origin)
+    finally:
+        lib.pppm_debug_fail_allocation(-1)
+    for g, r, name in zip(got, (skey, sidx, start, end), ("sorted_key", "sorted_idx", "cell_start", "cell_end")):
+        assert np.array_equal(g, r), name
