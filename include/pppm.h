@@ -343,6 +343,16 @@ pppm_status pppm_mg_destroy(pppm_mg *mg);
  * receives. */
 pppm_status pppm_mg_full_multigrid(pppm_mg *mg, double *x_dev, const double *b_dev,
                                    int mode, double tol, int max_cycles, double *relres);
+/* m_Vcycle(x, b, tol, residual, level) (MG/MultiGrid.cpp:128-201): one V(4,4)
+ * cycle from `level` down to the coarsest level and back, on that level's FP64
+ * arrays x and b of d_level^3 entries (level 0 = the n^3 grid).  Applied as a
+ * defect correction: r = b - A x in FP64, an FP32 cycle on A e = r from
+ * e = 0, x += e in FP64 — the reference's cycle in exact arithmetic.  The
+ * reference ignores tol and leaves residual unset; so does the C++ mirror. */
+pppm_status pppm_mg_vcycle(pppm_mg *mg, double *x_dev, const double *b_dev, int level);
+/* Level count of the hierarchy (halve while a level has more than 512 cells,
+ * MG/MultiGrid.h:114-127) and the edge of each level (up to cap entries). */
+pppm_status pppm_mg_levels(const pppm_mg *mg, int *levels, uint32_t *edges, int cap);
 
 /* ---- scalar PPPM: PotentialFieldSolver (HFS/PotentialFieldSolver.h:10-91,
  * HFS/PotentialFieldSolver.cpp:45-739) ------------------------------------

@@ -8,11 +8,17 @@
 //   PotentialFieldSolver          hybridFastSummation/PotentialFieldSolver.h:10-91
 //
 // The reference passes gf::gf_GpuArray<T> objects (multigrid/gfGpuArray.h:
-// 26-89); DeviceArray<T> below keeps the two members its call sites use,
-// getDevicePtr() and getSize(), over caller-owned device memory.  Methods
-// return bool like the reference, but false on failure (the reference always
-// returns true and exits on CUDA errors); lastError() gives the reason.
+// 26-89); DeviceArray<T> below keeps the members its call sites use,
+// getDevicePtr(), getSize() and typeSize(), over device memory owned by the
+// caller or by the solver.  Element types are the CUDA vector types the
+// reference uses (float4 positions, double4 origin, double3 gradients), so
+// its call expressions — getU(0)->getDevicePtr(), getSortPos()->getDevicePtr(),
+// getOrigin().x — compile unchanged.  Methods return bool like the reference,
+// but false on failure (the reference always returns true and exits on CUDA
+// errors); lastError() gives the reason.
 #pragma once
+
+#include <cuda_runtime.h>  // float4, double4, double3, float3, uint3
 
 #include <cstdint>
 #include <cstring>
@@ -24,8 +30,10 @@ namespace pppm_compat {
 
 typedef unsigned int uint;
 
-struct float4_ { float x, y, z, w; };
-struct double4_ { double x, y, z, w; };
+// Earlier spellings of the element types, kept as aliases.
+typedef float4 float4_;
+typedef double4 double4_;
+typedef double3 double3_;
 
 template <typename T>
 class DeviceArray {
@@ -41,8 +49,9 @@ private:
     size_t n_ = 0;
 };
 
-typedef DeviceArray<float4_> GpuArrayf4;
+typedef DeviceArray<float4> GpuArrayf4;
 typedef DeviceArray<double> GpuArrayd;
+typedef DeviceArray<double3> GpuArrayd3;
 
 inline std::string lastError() { return pppm_last_error(); }
 
@@ -79,11 +88,11 @@ public:
     // HFS/BiotSavartSolverImp.cpp:318-360
     bool setVortParameter(uint n, GpuArrayf4 *pos, GpuArrayd *omega[]) {
         N_ = n;
-        vort_[0] = omega[0]->getDevicePtr();
-        vort_[1] = omega[1]->getDevicePtr();
-        vort_[2] = omega[2]->getDevicePtr();
-        return pppm_set_vortices(scene_, n, reinterpret_cast<const float *>(pos->getDevicePtr()), vort_[0],
-                                 vort_[1], vort_[2]) == PPPM_OK;
+        sorted_valid_ = false;
+        for (int c = 0; c < 3; c++) vort_arr_[c] = GpuArrayd(omega[c]->getDevicePtr(), n);
+        return pppm_set_vortices(scene_, n, reinterpret_cast<const float *>(pos->getDevicePtr()),
+                                 vort_arr_[0].getDevicePtr(), vort_arr_[1].getDevicePtr(),
+                                 vort_arr_[2].getDevicePtr()) == PPPM_OK;
     }
 
     // HFS/BiotSavartSolverImp.cpp:266-316
@@ -102,8 +111,10 @@ public:
         return pppm_eval(scene_, M_, eval_, eb, (int)is_segment, U_[0], U_[1], U_[2]) == PPPM_OK;
     }
 
-    double *getU(int i) { return U_[i]; }
-    const double *getVort(int i) { return vort_[i]; }
+    // HFS/BiotSavartSolver.h:24-27: the solver's own arrays, valid until the
+    // next call that resizes them or shutdown().
+    GpuArrayd *getU(int i) { return &u_arr_[i]; }
+    GpuArrayd *getVort(int i) { return &vort_arr_[i]; }
 
     // HFS/BiotSavartSolverImp.cpp:733-753: hash + reorder; the sorted copies are
     // produced on request by getSortPos / getSortVort.
@@ -111,28 +122,29 @@ public:
         ok_ = pppm_build_far_field(scene_) == PPPM_OK;
         sorted_valid_ = false;
     }
-    float4_ *getSortPos() { return refresh_sorted() ? spos_ : nullptr; }
-    double *getSortVort(int i) { return refresh_sorted() ? salpha_[i] : nullptr; }
+    GpuArrayf4 *getSortPos() { return refresh_sorted() ? &spos_arr_ : nullptr; }
+    GpuArrayd *getSortVort(int i) { return refresh_sorted() ? &salpha_arr_[i] : nullptr; }
 
-    const uint32_t *getVortStartTable() {
+    // HFS/BiotSavartSolver.h:28-29 (n^3 entries; empty cells hold 0xFFFFFFFF)
+    uint *getVortStartTable() {
         const uint32_t *s = nullptr, *e = nullptr;
         pppm_get_cell_tables(scene_, &s, &e);
-        return s;
+        return const_cast<uint *>(s);
     }
-    const uint32_t *getVortEndTable() {
+    uint *getVortEndTable() {
         const uint32_t *s = nullptr, *e = nullptr;
         pppm_get_cell_tables(scene_, &s, &e);
-        return e;
+        return const_cast<uint *>(e);
     }
     double getCellh() {
         double o[3], L = 0, h = 0;
         pppm_get_domain(scene_, o, &L, &h);
         return h;
     }
-    double4_ getOrigin() {
+    double4 getOrigin() {
         double o[3] = {0, 0, 0}, L = 0, h = 0;
         pppm_get_domain(scene_, o, &L, &h);
-        return double4_{o[0], o[1], o[2], 0.0};
+        return make_double4(o[0], o[1], o[2], 0.0);
     }
 
     // HFS/BiotSavartSolverImp.cpp:230-264
@@ -148,8 +160,8 @@ public:
 
 private:
     // Output arrays are owned by the solver, as m_particle_U is in the
-    // reference; device memory comes from the scene's allocator through a
-    // direct-sum-free path: plain cudaMalloc via the runtime the library uses.
+    // reference; they are allocated with the CUDA runtime the application
+    // links (cudaMalloc), outside the library.
     bool ensure_u(uint m);
     bool refresh_sorted();
     void free_buffers();
@@ -158,10 +170,11 @@ private:
     uint n_ = 0, M_ = 0, N_ = 0, capU_ = 0, capS_ = 0;
     int K_ = 1;
     const float *eval_ = nullptr;
-    const double *vort_[3] = {nullptr, nullptr, nullptr};
     double *U_[3] = {nullptr, nullptr, nullptr};
-    float4_ *spos_ = nullptr;
+    float4 *spos_ = nullptr;
     double *salpha_[3] = {nullptr, nullptr, nullptr};
+    GpuArrayd u_arr_[3], vort_arr_[3], salpha_arr_[3];
+    GpuArrayf4 spos_arr_;
     bool sorted_valid_ = false;
     bool ok_ = true;
 };
@@ -184,6 +197,12 @@ public:
         pppm_mg_full_multigrid(mg_, x->getDevicePtr(), b->getDevicePtr(), PPPM_MG_REFERENCE, tol, 1, &rr);
         residual = rr;
     }
+    // MG/MultiGrid.cpp:128-201: one V(4,4) cycle from `level` down, on that
+    // level's arrays (level 0 = the full grid).  As in the reference, tol is
+    // not used and residual is left as it is.
+    void m_Vcycle(GpuArrayd *x, GpuArrayd *b, double /*tol*/, double & /*residual*/, int level) {
+        pppm_mg_vcycle(mg_, x->getDevicePtr(), b->getDevicePtr(), level);
+    }
 
 private:
     pppm_mg *mg_ = nullptr;
@@ -191,7 +210,13 @@ private:
 
 class ParticleManager {
 public:
+    ParticleManager() = default;
+    // PH/SpaceHashClassImp.cpp:6-14: a 64^3 grid of cell size 1/64 at the
+    // origin; device tables come with initSpatialHash.
+    explicit ParticleManager(uint numParticles) : N_(numParticles) {}
     ~ParticleManager() { endSpatialHash(); }
+    ParticleManager(const ParticleManager &) = delete;
+    ParticleManager &operator=(const ParticleManager &) = delete;
     // PH/SpaceHashClassImp.cpp:47-69
     void initSpatialHash(uint numParticles, uint dimx, uint dimy, uint dimz, void *stream = nullptr) {
         endSpatialHash();
@@ -204,16 +229,16 @@ public:
         h_ = nullptr;
     }
     // PH/SpaceHashClass.h:46-54
-    void setSpatialHashGrid(uint size0, float h, const float bbmin[3], uint numParticles) {
+    void setSpatialHashGrid(uint size0, float h, float3 bbmin, uint numParticles) {
         n_ = size0;
         h_cell_ = h;
-        origin_[0] = bbmin[0];
-        origin_[1] = bbmin[1];
-        origin_[2] = bbmin[2];
+        origin_[0] = bbmin.x;
+        origin_[1] = bbmin.y;
+        origin_[2] = bbmin.z;
         N_ = numParticles;
     }
     void setHashParam() {}  // parameters travel with each call
-    void doSpatialHash(float4_ *pos, uint numParticles) {
+    void doSpatialHash(float4 *pos, uint numParticles) {
         pppm_hasher_run(h_, numParticles, reinterpret_cast<const float *>(pos), h_cell_, origin_);
     }
     void reorderData(uint numParticles, void *data, void *dataReorder, uint stride, uint precision) {
@@ -222,10 +247,15 @@ public:
     void deorderData(uint numParticles, void *data, void *dataReorder, uint stride, uint precision) {
         pppm_hasher_deorder(h_, numParticles, data, dataReorder, stride, precision);
     }
-    const uint32_t *getHashTable() { return table(0); }
-    const uint32_t *getStartTable() { return table(2); }
-    const uint32_t *getEndTable() { return table(3); }
-    float getCellSize() const { return h_cell_; }
+    // PH/SpaceHashClass.h:24-38, 67-69
+    uint *getHashTable() { return const_cast<uint *>(table(0)); }
+    uint *getStartTable() { return const_cast<uint *>(table(2)); }
+    uint *getEndTable() { return const_cast<uint *>(table(3)); }
+    int getNumParticles() const { return (int)N_; }
+    uint3 getGridSize() const { return make_uint3(n_, n_, n_); }
+    float3 getWorldOrigin() const { return make_float3(origin_[0], origin_[1], origin_[2]); }
+    float3 getCellSize() const { return make_float3(h_cell_, h_cell_, h_cell_); }
+    uint getNumCells() const { return n_ * n_ * n_; }
 
 private:
     const uint32_t *table(int which) {
@@ -234,13 +264,10 @@ private:
         return t[which];
     }
     pppm_hasher *h_ = nullptr;
-    uint n_ = 0, N_ = 0;
-    float h_cell_ = 0.f;
+    uint n_ = 64, N_ = 0;
+    float h_cell_ = 1.0f / 64.0f;
     float origin_[3] = {0.f, 0.f, 0.f};
 };
-
-struct double3_ { double x, y, z; };
-typedef DeviceArray<double3_> GpuArrayd3;
 
 // HFS/PotentialFieldSolver.h:10-91.  Output arrays are owned by the solver, as
 // m_particle_gradPhi / m_particle_dphidn are in the reference.
@@ -293,10 +320,10 @@ public:
         pppm_potential_grids(p_, ol, nullptr, nullptr, nullptr, nullptr, nullptr);
         return (double)(float)(ol[3] / (double)n_);
     }
-    double4_ getOrigin() {
+    double4 getOrigin() {
         double ol[4] = {0, 0, 0, 0};
         pppm_potential_grids(p_, ol, nullptr, nullptr, nullptr, nullptr, nullptr);
-        return double4_{ol[0], ol[1], ol[2], 0.0};
+        return make_double4(ol[0], ol[1], ol[2], 0.0);
     }
     bool shutdown();
     bool lastOk() const { return ok_; }
@@ -307,8 +334,8 @@ private:
     uint n_ = 0, M_ = 0, cap_ = 0;
     const float *eval_ = nullptr;
     const double *mass_ = nullptr, *areas_ = nullptr;
-    const double3_ *normals_ = nullptr;
-    double3_ *grad_ = nullptr;
+    const double3 *normals_ = nullptr;
+    double3 *grad_ = nullptr;
     double *dphidn_ = nullptr, *split_ = nullptr;  // split_: [6][cap] SoA scratch for computeDphiDn
     GpuArrayd3 grad_arr_;
     GpuArrayd dp_arr_;
@@ -319,18 +346,21 @@ private:
 
 // Out-of-line members that allocate: kept here so the header stays self
 // contained; they use the CUDA runtime the application already links.
-#include <cuda_runtime.h>
-
 namespace pppm_compat {
 
 inline bool BiotSavartSolver::ensure_u(uint m) {
-    if (m <= capU_) return true;
-    for (int c = 0; c < 3; c++) {
-        cudaFree(U_[c]);
-        U_[c] = nullptr;
-        if (cudaMalloc(&U_[c], sizeof(double) * (m ? m : 1)) != cudaSuccess) return false;
+    if (m > capU_) {
+        for (int c = 0; c < 3; c++) {
+            cudaFree(U_[c]);
+            U_[c] = nullptr;
+            u_arr_[c] = GpuArrayd();
+        }
+        capU_ = 0;
+        for (int c = 0; c < 3; c++)
+            if (cudaMalloc(&U_[c], sizeof(double) * (m ? m : 1)) != cudaSuccess) return false;
+        capU_ = m;
     }
-    capU_ = m;
+    for (int c = 0; c < 3; c++) u_arr_[c] = GpuArrayd(U_[c], m);
     return true;
 }
 
@@ -340,13 +370,16 @@ inline bool BiotSavartSolver::refresh_sorted() {
         cudaFree(spos_);
         spos_ = nullptr;
         for (int c = 0; c < 3; c++) { cudaFree(salpha_[c]); salpha_[c] = nullptr; }
-        if (cudaMalloc(&spos_, sizeof(float4_) * N_) != cudaSuccess) return false;
+        capS_ = 0;
+        if (cudaMalloc(&spos_, sizeof(float4) * N_) != cudaSuccess) return false;
         for (int c = 0; c < 3; c++)
             if (cudaMalloc(&salpha_[c], sizeof(double) * N_) != cudaSuccess) return false;
         capS_ = N_;
     }
     sorted_valid_ = pppm_get_sorted_vortices(scene_, reinterpret_cast<float *>(spos_), salpha_[0], salpha_[1],
                                              salpha_[2]) == PPPM_OK;
+    spos_arr_ = GpuArrayf4(spos_, N_);
+    for (int c = 0; c < 3; c++) salpha_arr_[c] = GpuArrayd(salpha_[c], N_);
     return sorted_valid_;
 }
 
@@ -360,6 +393,9 @@ inline void BiotSavartSolver::free_buffers() {
     cudaFree(spos_);
     spos_ = nullptr;
     capU_ = capS_ = 0;
+    for (int c = 0; c < 3; c++) u_arr_[c] = salpha_arr_[c] = GpuArrayd();
+    spos_arr_ = GpuArrayf4();
+    sorted_valid_ = false;
 }
 
 }  // namespace pppm_compat
@@ -373,7 +409,7 @@ inline bool pppm_compat::PotentialFieldSolver::ensure_out(uint m) {
     dphidn_ = nullptr;
     split_ = nullptr;
     const size_t k = m ? m : 1;
-    if (cudaMalloc(&grad_, sizeof(double3_) * k) != cudaSuccess) return false;
+    if (cudaMalloc(&grad_, sizeof(double3) * k) != cudaSuccess) return false;
     if (cudaMalloc(&dphidn_, sizeof(double) * k) != cudaSuccess) return false;
     if (cudaMalloc(&split_, sizeof(double) * 6 * k) != cudaSuccess) return false;
     cap_ = m;

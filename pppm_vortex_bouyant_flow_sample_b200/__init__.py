@@ -595,3 +595,18 @@ class MultiGridSolver3DPeriod_double:
         check(load().pppm_mg_full_multigrid(self._h, _ptr(x), _ptr(b.contiguous()), mode, tol, max_cycles,
                                             C.byref(rr)), "pppm_mg_full_multigrid")
         return rr.value
+
+    def m_Vcycle(self, x: torch.Tensor, b: torch.Tensor, tol: float = 1e-10, residual=None, level: int = 0):
+        """One V(4,4) cycle from `level` down (multigrid/MultiGrid.cpp:128-201)
+        on that level's float64 arrays (edge n >> level); tol and residual are
+        unused, as in the reference."""
+        if x.dtype != torch.float64 or b.dtype != torch.float64 or not x.is_cuda:
+            raise ValueError("x and b must be CUDA float64 tensors")
+        check(load().pppm_mg_vcycle(self._h, _ptr(x), _ptr(b.contiguous()), int(level)), "pppm_mg_vcycle")
+
+    def levels(self):
+        """Edges of the levels of the hierarchy, finest first."""
+        cnt = C.c_int()
+        edges = (C.c_uint32 * 16)()
+        check(load().pppm_mg_levels(self._h, C.byref(cnt), edges, 16), "pppm_mg_levels")
+        return [int(edges[i]) for i in range(cnt.value)]

@@ -34,7 +34,7 @@ EXPORTED = (
     "pppm_render_shadows", "pppm_render_shadow_map", "pppm_render_smoke", "pppm_potential_create",
     "pppm_potential_destroy", "pppm_potential_set_masses", "pppm_potential_build", "pppm_potential_eval_gradient",
     "pppm_potential_eval_scalar", "pppm_potential_dphidn", "pppm_potential_grids", "pppm_potential_eval_gradient3",
-    "pppm_debug_fail_allocation",
+    "pppm_debug_fail_allocation", "pppm_mg_vcycle", "pppm_mg_levels",
 )
 REQ_EVAL, REQ_ADVANCE = 0, 1
 NOALLOC_MAX_PARTICLES = 1048576  # PPPM_NOALLOC_MAX_PARTICLES in include/pppm.h
@@ -122,6 +122,8 @@ def load(build_if_missing: bool = True):
         "pppm_mg_create": (st, [u32, vp, C.POINTER(vp)]),
         "pppm_mg_destroy": (st, [vp]),
         "pppm_mg_full_multigrid": (st, [vp, vp, vp, C.c_int, C.c_double, C.c_int, C.POINTER(C.c_double)]),
+        "pppm_mg_vcycle": (st, [vp, vp, vp, C.c_int]),
+        "pppm_mg_levels": (st, [vp, C.POINTER(C.c_int), C.POINTER(u32), C.c_int]),
         "pppm_hasher_create": (st, [u32, u32, vp, C.POINTER(vp)]),
         "pppm_hasher_destroy": (st, [vp]),
         "pppm_hasher_run": (st, [vp, u32, vp, C.c_float, C.POINTER(C.c_float)]),

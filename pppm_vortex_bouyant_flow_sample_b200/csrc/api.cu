@@ -924,6 +924,38 @@ extern "C" pppm_status pppm_mg_full_multigrid(pppm_mg *m, double *x, const doubl
     return PPPM_OK;
 }
 
+extern "C" pppm_status pppm_mg_levels(const pppm_mg *m, int *levels, uint32_t *edges, int cap) {
+    if (!m || !levels) {
+        snprintf(g_err, sizeof(g_err), "pppm_mg_levels: invalid argument");
+        return PPPM_ERR_INVALID;
+    }
+    *levels = m->plan.levels;
+    for (int l = 0; edges && l < m->plan.levels && l < cap; l++) edges[l] = m->plan.lv[l].d;
+    return PPPM_OK;
+}
+
+extern "C" pppm_status pppm_mg_vcycle(pppm_mg *m, double *x, const double *b, int level) {
+    if (!m || !x || !b || level < 0 || level >= m->plan.levels) {
+        snprintf(g_err, sizeof(g_err), "pppm_mg_vcycle: invalid argument (level %d of %d)", level,
+                 m ? m->plan.levels : 0);
+        return PPPM_ERR_INVALID;
+    }
+    // The cycle runs on the levels from `level` down; x and b are that level's
+    // FP64 arrays.  r = b - A x seeds the level's FP32 right-hand side, the
+    // FP32 V-cycle solves for the correction from zero, and x += e.
+    pppm::MGPlan P = m->plan;
+    P.levels = m->plan.levels - level;
+    for (int l = 0; l < P.levels; l++) P.lv[l] = m->plan.lv[level + l];
+    P.coarse_op = (P.levels >= 2) ? m->coarse_op : nullptr;
+    const size_t C = P.lv[0].cells;
+    ::pppm::note_launch();
+    residual64_kernel<<<(unsigned)((C + 255) / 256), 256, 0, P.st>>>(x, b, m->r64, P.lv[0].b, (int)P.lv[0].d);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = pppm::mg_vcycle_update(P, x);
+    if (e != cudaSuccess) return cuda_fail("pppm_mg_vcycle", e);
+    return PPPM_OK;
+}
+
 // ---------------------------------------------------------------------------
 // FP64 direct sum (ground truth for the error reports).
 // ---------------------------------------------------------------------------

@@ -379,6 +379,20 @@ static cudaError_t dc_correct(const MGPlan &m) {
     return cudaGetLastError();
 }
 
+// One V(4,4) cycle applied to an FP64 iterate x64 as a defect correction:
+// lv[0].b already holds r = b - A x64 (FP32), then e = V32(0, r) and
+// x64 += e — the reference's m_Vcycle(x, b) in exact arithmetic, the V-cycle
+// being a consistent linear iteration (MG/MultiGrid.cpp:128-201).
+cudaError_t mg_vcycle_update(const MGPlan &m, double *x64) {
+    const uint32_t C0 = m.lv[0].cells;
+    PPPM_CUDA_TRY(cudaMemsetAsync(m.lv[0].x, 0, sizeof(float) * m.comps * (size_t)C0, m.st));
+    PPPM_CUDA_TRY(vcycle32(m, 0));
+    const size_t cnt = (size_t)m.comps * C0;
+    ::pppm::note_launch();
+    dc_update_kernel<<<(unsigned)((cnt + 255) / 256), 256, 0, m.st>>>(x64, m.lv[0].x, cnt, 0);
+    return cudaGetLastError();
+}
+
 static cudaError_t read_relres(const MGPlan &m, double *relres) {
     double h[2];
     PPPM_CUDA_TRY(cudaMemcpyAsync(h, m.norms, sizeof(h), cudaMemcpyDeviceToHost, m.st));

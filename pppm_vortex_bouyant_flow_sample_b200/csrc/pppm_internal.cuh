@@ -224,6 +224,7 @@ cudaError_t launch_move3(pppm_scene *s, float4 *pos, const double *u, const doub
 
 cudaError_t mg_solve(const MGPlan &m, int mode, double tol, int max_cycles, int *cycles_out,
                      double *relres_out);
+cudaError_t mg_vcycle_update(const MGPlan &m, double *x64);
 
 cudaError_t radix_sort_pairs(cudaStream_t st, uint32_t N, uint32_t bits, uint32_t *key[2], uint32_t *idx[2],
                              uint32_t *hist, uint32_t **sorted_key, uint32_t **sorted_idx);

@@ -1,8 +1,12 @@
 """The C++ classes of include/pppm_compat.hpp (BiotSavartSolver,
 ParticleManager, MultiGridSolver3DPeriod_double, PotentialFieldSolver) compiled with g++ into a
-driver that calls them like the reference's own callers, checked against the
-oracle: velocities <= 1e-5, hash keys and sorted indices bit-exact, and the
-multigrid solution against the oracle's FP64 reference schedule."""
+driver that calls them with the reference's own call expressions
+(getU(c)->getDevicePtr(), getSortPos()->getDevicePtr(), ParticleManager(N),
+setSpatialHashGrid(n, h, float3, N), m_Vcycle(x, b, tol, res, 0)), checked
+against the oracle: velocities <= 1e-5, hash keys, sorted indices, sorted
+positions and strengths and the cell start table bit-exact, and the multigrid
+solution (full multigrid, then one more V-cycle) against the oracle's FP64
+reference schedule."""
 import os
 import shutil
 import subprocess
@@ -54,14 +58,29 @@ def test_cpp_compat_classes_match_oracle(tmp_path, oracle):
     idx = np.frombuffer(raw, np.uint32, N, off); off += 4 * N
     h, ox, oy, oz = np.frombuffer(raw, np.float64, 4, off); off += 32
     x = np.frombuffer(raw, np.float64, n ** 3, off); off += 8 * n ** 3
-    grad = np.frombuffer(raw, np.float64, 3 * N, off).reshape(N, 3)
+    grad = np.frombuffer(raw, np.float64, 3 * N, off).reshape(N, 3); off += 24 * N
+    xv = np.frombuffer(raw, np.float64, n ** 3, off); off += 8 * n ** 3
+    spos = np.frombuffer(raw, np.float32, 4 * N, off).reshape(N, 4); off += 16 * N
+    svort = np.frombuffer(raw, np.float64, 3 * N, off).reshape(3, N).T; off += 24 * N
+    cstart = np.frombuffer(raw, np.uint32, n ** 3, off); off += 4 * n ** 3
+    gsize = np.frombuffer(raw, np.uint32, 3, off)
 
     ref, d = oracle.pppm(oracle.params(n), pos, al, pos, pos, 1, dump=True)
     assert rel_l2(u, ref) <= 1e-5
     assert h == float(d["h_f"][0]) and (ox, oy, oz) == tuple(d["origin"])
     assert np.array_equal(keys, d["vort_key"]) and np.array_equal(idx, d["vort_idx"])
     q = np.arange(n ** 3, dtype=np.float64)
-    xr, _, _ = oracle.mg_solve(np.sin(0.001 * q) - 0.5, n, mg_mode=0)
+    bq = np.sin(0.001 * q) - 0.5
+    xr, _, _ = oracle.mg_solve(bq, n, mg_mode=0)
     assert rel_l2(x, xr) <= 1e-6
+    # one more V(4,4) cycle from the solver's own x: the oracle's cycle from the same x
+    assert rel_l2(xv, oracle.mg_vcycle(x, bq, n)) <= 1e-6
+    assert rel_l2(xv, xr) > 0.0  # the cycle changed x
+    # computeStretching's inputs: sorted positions / strengths and the start table
+    order = d["vort_idx"]
+    assert np.array_equal(spos[:, :3], pos[order][:, :3])
+    assert np.array_equal(svort, al[order])
+    assert np.array_equal(cstart, d["cell_start"])
+    assert tuple(gsize) == (n, n, n)
     gref = oracle.potential(n, 1, pos, al[:, 0], pos)
     assert rel_l2(grad, gref) <= 1e-5

@@ -187,6 +187,31 @@ def test_mg_standalone_reference_and_converged(pb, oracle):
     mg.m_FinalMemoryEachLevel()
 
 
+@pytest.mark.parametrize("n", [32, 64, 96])
+def test_mg_vcycle_each_level(pb, oracle, n):
+    """m_Vcycle(x, b, tol, res, level) (MG/MultiGrid.cpp:128-201): one V(4,4)
+    cycle on level `level`'s arrays.  The hierarchy below level l is the one a
+    grid of that level's edge has, so the oracle's cycle on that edge is the
+    check, starting from a nonzero x."""
+    import torch
+    mg = pb.MultiGridSolver3DPeriod_double()
+    mg.m_InitialSystem(n, n, n)
+    edges = mg.levels()
+    assert edges[0] == n and len(edges) == oracle.mg_levels(n)
+    rng = np.random.default_rng(n)
+    for level, d in enumerate(edges):
+        b = rng.standard_normal(d ** 3)
+        x0 = 0.1 * rng.standard_normal(d ** 3)
+        x = _dev(x0)
+        mg.m_Vcycle(x, _dev(b), 1e-10, None, level)
+        want = oracle.mg_vcycle(x0, b, d)
+        assert rel_l2(x.cpu().numpy(), want) <= 1e-6, (level, d)
+    with pytest.raises(pb.PppmError):
+        mg.m_Vcycle(torch.zeros(8, dtype=torch.float64, device="cuda"), torch.zeros(8, dtype=torch.float64,
+                                                                                   device="cuda"), 0, None, len(edges))
+    mg.m_FinalMemoryEachLevel()
+
+
 def test_direct_sum_gpu_matches_oracle(pb, oracle):
     from pppm_vortex_bouyant_flow_sample_b200 import workloads as W
     pos, al = W.uniform_cloud(3000, seed=10)
