@@ -67,6 +67,9 @@ typedef struct pppm_params {
     int32_t mg_mode;         /* PPPM_MG_*                                         */
     double mg_tol;           /* relative residual target for CONVERGED            */
     int32_t mg_max_cycles;   /* cap on defect-correction cycles                   */
+    double a_cells;          /* > 0: smoothing radius in cells, a = a_cells * h with
+                                h the cell size of each build's domain (overrides a);
+                                0: a is absolute, as in the reference              */
 } pppm_params;
 
 typedef struct pppm_scene pppm_scene;
@@ -82,8 +85,15 @@ const char *pppm_last_error(void);
 const char *pppm_version(void);
 
 /* Defaults = the reference's constants: K = 1, a = 0.08, BBOX3X,
- * PPPM_MG_REFERENCE, mg_tol 1e-10, 50 cycles; n must still be set. */
+ * PPPM_MG_REFERENCE, mg_tol 1e-10, 50 cycles, a_cells = 0; n must still be
+ * set. */
 pppm_status pppm_params_default(pppm_params *p);
+/* The most accurate setting measured against the FP64 direct sum with the
+ * same smoothing kernel (no reference counterpart: the reference hard-codes
+ * a = 0.08, HFS/GPU_kernel.cu:2306): BBOX3X, smoothing radius one cell
+ * (a_cells = 1), near field K = 3, multigrid converged to mg_tol = 1e-6 in
+ * FP64 defect-correction cycles.  n must still be set. */
+pppm_status pppm_params_accurate(pppm_params *p);
 
 /* BiotSavartSolver::initializeSolver (HFS/BiotSavartSolverImp.cpp:44-229):
  * allocates every buffer for up to cap_vort vortices and cap_eval evaluation
@@ -194,6 +204,9 @@ pppm_status pppm_get_density(pppm_scene *s, uint32_t *dim, double origin[3], dou
  * non-finite domain edge (one vortex, or all coincident); pppm_eval then
  * returned zero velocities. */
 pppm_status pppm_get_domain(pppm_scene *s, double origin[3], double *length, double *cell_h);
+/* Smoothing radius a of the last far field (a, or a_cells times its cell
+ * size); synchronises the stream. */
+pppm_status pppm_get_smoothing(pppm_scene *s, double *a);
 /* getVortStartTable / getVortEndTable (HFS/BiotSavartSolver.h:28-29): device
  * pointers to n^3 uint32 tables (empty cells hold 0xFFFFFFFF in both). */
 pppm_status pppm_get_cell_tables(pppm_scene *s, const uint32_t **start_dev,

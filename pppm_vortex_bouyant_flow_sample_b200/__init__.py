@@ -69,14 +69,16 @@ class Scene:
     def __init__(self, n: int, K: int = 1, a: float = 0.08, domain: str = "bbox3x",
                  fixed_origin=(0.0, 0.0, 0.0), fixed_length: float = 1.0, mg: str = "reference",
                  mg_tol: float = 1e-10, mg_max_cycles: int = 50, cap_vort: int = 1, cap_eval: int = 1,
-                 stream: torch.cuda.Stream | None = None):
+                 stream: torch.cuda.Stream | None = None, a_cells: float = 0.0):
+        """a_cells > 0 ties the smoothing radius to the cell size of each build
+        (a = a_cells * h), overriding the absolute a."""
         _require_cuda()
         self._lib = load()
         self.params = default_params(
             n, K=K, a=a, domain_mode=DOMAIN_FIXED if domain == "fixed" else DOMAIN_BBOX3X,
             fixed_origin=fixed_origin, fixed_length=fixed_length,
             mg_mode=MG_CONVERGED if mg == "converged" else MG_REFERENCE, mg_tol=mg_tol,
-            mg_max_cycles=mg_max_cycles)
+            mg_max_cycles=mg_max_cycles, a_cells=a_cells)
         self.stream = stream if stream is not None else torch.cuda.current_stream()
         h = C.c_void_p()
         check(self._lib.pppm_scene_create(C.byref(self.params), cap_vort, cap_eval,
@@ -157,6 +159,12 @@ class Scene:
         h = C.c_double()
         check(self._lib.pppm_get_domain(self._h, o, C.byref(L), C.byref(h)), "pppm_get_domain")
         return (o[0], o[1], o[2]), L.value, h.value
+
+    def smoothing(self) -> float:
+        """Smoothing radius a of the last far field (absolute, or a_cells x h)."""
+        a = C.c_double()
+        check(self._lib.pppm_get_smoothing(self._h, C.byref(a)), "pppm_get_smoothing")
+        return a.value
 
     def cell_tables(self):
         """(start, end) as int64 CPU tensors of the uint32 tables (n^3 each)."""

@@ -34,7 +34,8 @@ EXPORTED = (
     "pppm_render_shadows", "pppm_render_shadow_map", "pppm_render_smoke", "pppm_potential_create",
     "pppm_potential_destroy", "pppm_potential_set_masses", "pppm_potential_build", "pppm_potential_eval_gradient",
     "pppm_potential_eval_scalar", "pppm_potential_dphidn", "pppm_potential_grids", "pppm_potential_eval_gradient3",
-    "pppm_debug_fail_allocation", "pppm_mg_vcycle", "pppm_mg_levels",
+    "pppm_debug_fail_allocation", "pppm_mg_vcycle", "pppm_mg_levels", "pppm_params_accurate",
+    "pppm_get_smoothing",
 )
 REQ_EVAL, REQ_ADVANCE = 0, 1
 NOALLOC_MAX_PARTICLES = 1048576  # PPPM_NOALLOC_MAX_PARTICLES in include/pppm.h
@@ -53,6 +54,7 @@ class PppmParams(C.Structure):
         ("mg_mode", C.c_int32),
         ("mg_tol", C.c_double),
         ("mg_max_cycles", C.c_int32),
+        ("a_cells", C.c_double),
     ]
 
 
@@ -122,6 +124,8 @@ def load(build_if_missing: bool = True):
         "pppm_mg_create": (st, [u32, vp, C.POINTER(vp)]),
         "pppm_mg_destroy": (st, [vp]),
         "pppm_mg_full_multigrid": (st, [vp, vp, vp, C.c_int, C.c_double, C.c_int, C.POINTER(C.c_double)]),
+        "pppm_params_accurate": (st, [C.POINTER(PppmParams)]),
+        "pppm_get_smoothing": (st, [vp, C.POINTER(C.c_double)]),
         "pppm_mg_vcycle": (st, [vp, vp, vp, C.c_int]),
         "pppm_mg_levels": (st, [vp, C.POINTER(C.c_int), C.POINTER(u32), C.c_int]),
         "pppm_hasher_create": (st, [u32, u32, vp, C.POINTER(vp)]),

@@ -60,7 +60,14 @@ bool valid_params(const pppm_params *p, char *why, size_t cap) {
         return false;
     }
     if (p->K < -1 || p->K > pppm::kMaxK) { snprintf(why, cap, "K=%d outside [-1, %d]", p->K, pppm::kMaxK); return false; }
-    if (!(p->a > 0.0) || !std::isfinite(p->a)) { snprintf(why, cap, "smoothing radius a=%g must be > 0", p->a); return false; }
+    if (!(p->a_cells >= 0.0) || !std::isfinite(p->a_cells)) {
+        snprintf(why, cap, "a_cells=%g must be finite and >= 0", p->a_cells);
+        return false;
+    }
+    if (p->a_cells == 0.0 && (!(p->a > 0.0) || !std::isfinite(p->a))) {
+        snprintf(why, cap, "smoothing radius a=%g must be > 0", p->a);
+        return false;
+    }
     if (p->domain_mode != PPPM_DOMAIN_BBOX3X && p->domain_mode != PPPM_DOMAIN_FIXED) {
         snprintf(why, cap, "unknown domain_mode %d", p->domain_mode);
         return false;
@@ -309,6 +316,17 @@ extern "C" pppm_status pppm_params_default(pppm_params *p) {
     p->fixed_length = 1.0;
     p->mg_mode = PPPM_MG_REFERENCE;
     p->mg_tol = 1e-10;
+    p->mg_max_cycles = 50;
+    return PPPM_OK;
+}
+
+extern "C" pppm_status pppm_params_accurate(pppm_params *p) {
+    if (!p) return PPPM_ERR_INVALID;
+    pppm_params_default(p);
+    p->a_cells = 1.0;
+    p->K = 3;
+    p->mg_mode = PPPM_MG_CONVERGED;
+    p->mg_tol = 1e-6;
     p->mg_max_cycles = 50;
     return PPPM_OK;
 }
@@ -636,6 +654,17 @@ extern "C" pppm_status pppm_get_domain(pppm_scene *s, double origin[3], double *
     if (length) *length = h.length;
     if (cell_h) *cell_h = h.cell_h;
     if (h.status != 0) { snprintf(g_err, sizeof(g_err), "degenerate domain (L = %g)", h.length); return PPPM_ERR_DOMAIN; }
+    return PPPM_OK;
+}
+
+extern "C" pppm_status pppm_get_smoothing(pppm_scene *s, double *a) {
+    if (!s || !a) return PPPM_ERR_INVALID;
+    if (!s->far_ready) { snprintf(g_err, sizeof(g_err), "pppm_get_smoothing: no far field built"); return PPPM_ERR_STATE; }
+    pppm::DevParams h;
+    cudaError_t e = cudaMemcpyAsync(&h, s->dparams, sizeof(h), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return cuda_fail("pppm_get_smoothing", e);
+    *a = h.a;
     return PPPM_OK;
 }
 

@@ -338,7 +338,9 @@ __global__ void __launch_bounds__(kEvalThreads, 8) eval_kernel(const SmoothSerie
     PairAcc2 acc2;
     float3 o_w = make_float3(0.f, 0.f, 0.f);
     if (K >= 0) {
-        const float cr = P->cr_f, inv_a3 = P->inv_a3_f, inv4pia3 = P->inv4pia3_f;
+        // FOLD: coefficients carry 1/(4 pi a^3); otherwise they have unit
+        // scale and the sums are scaled once per point below
+        const float cr = P->cr_f, inv_a3 = P->inv_a3_f, inv4pia3 = FOLD ? P->inv4pia3_f : 1.0f;
         const bool need_exp = P->need_exp != 0;
         const float *cf = sc.c;
         // some pair can reach t = 0.25: the degree-7 polynomial, exp above t = 2
@@ -447,9 +449,16 @@ __global__ void __launch_bounds__(kEvalThreads, 8) eval_kernel(const SmoothSerie
         const float Ax = acc2.ax.x + acc2.ax.y, Ay = acc2.ay.x + acc2.ay.y, Az = acc2.az.x + acc2.az.y;
         const float Bx = acc2.bx.x + acc2.bx.y, By = acc2.by.x + acc2.by.y, Bz = acc2.bz.x + acc2.bz.y;
         const float sx = ra.x - o_w.x, sy = ra.y - o_w.y, sz = ra.z - o_w.z;
-        ux += acc.x + (fmaf(Ay, sz, -(Az * sy)) - Bx);
-        uy += acc.y + (fmaf(Az, sx, -(Ax * sz)) - By);
-        uz += acc.z + (fmaf(Ax, sy, -(Ay * sx)) - Bz);
+        if (FOLD) {
+            ux += acc.x + (fmaf(Ay, sz, -(Az * sy)) - Bx);
+            uy += acc.y + (fmaf(Az, sx, -(Ax * sz)) - By);
+            uz += acc.z + (fmaf(Ax, sy, -(Ay * sx)) - Bz);
+        } else {
+            const float k = P->inv4pia3_f;
+            ux = fmaf(acc.x + (fmaf(Ay, sz, -(Az * sy)) - Bx), k, ux);
+            uy = fmaf(acc.y + (fmaf(Az, sx, -(Ax * sz)) - By), k, uy);
+            uz = fmaf(acc.z + (fmaf(Ax, sy, -(Ay * sx)) - Bz), k, uz);
+        }
         if (P->status != 0) {
             // zero or non-finite domain edge (one vortex, or all coincident):
             // the cell size is 0 and the sums above are meaningless; the
@@ -526,24 +535,31 @@ cudaError_t launch_eval(pppm_scene *s, const float4 *eval_a, const float4 *eval_
     const unsigned grid = (M + kEvalThreads - 1) / kEvalThreads;
     unsigned long long *pc = count_pairs ? s->pair_count : nullptr;
     SmoothSeries sc;
-    bool fold = true;
+    // With an absolute a (known here) the packed polynomials are in r^3
+    // (c_q / a^(3q), scaled by 1/(4 pi a^3)) while every coefficient stays a
+    // normal float far from overflow.  Otherwise (a tied to the cell size of
+    // the build, known only on the device, or extreme a) they are in
+    // t = (r/a)^3 with unit scale, and the kernel applies 1/(4 pi a^3) from
+    // the device parameters once per point.
+    bool fold = s->prm.a_cells <= 0.0;
     {
-        // the packed polynomials in r^3 (c_q / a^(3q)) while every coefficient
-        // stays a normal float far from overflow, else in t = (r/a)^3
-        const double a = s->prm.a;
-        const double k = 1.0 / (kFourPi * a * a * a);
-        const double ia3 = 1.0 / (a * a * a);
         double f4[5], f7[8];
         phi_chebyshev(4, 0.25, f4);
         phi_chebyshev(7, 2.0, f7);
-        double u4[5], u7[8], pw = 1.0;
-        for (int q = 0; q < 8; q++, pw *= ia3) {
-            if (q < 5) u4[q] = k * f4[q] * pw;
-            u7[q] = k * f7[q] * pw;
-            for (double x : {q < 5 ? u4[q] : 1.0, u7[q]})
-                if (!(std::fabs(x) <= 1e30 && std::fabs(x) >= 1e-30)) fold = false;
+        double u4[5], u7[8], k = 1.0;
+        if (fold) {
+            const double a = s->prm.a;
+            k = 1.0 / (kFourPi * a * a * a);
+            const double ia3 = 1.0 / (a * a * a);
+            double pw = 1.0;
+            for (int q = 0; q < 8; q++, pw *= ia3) {
+                if (q < 5) u4[q] = k * f4[q] * pw;
+                u7[q] = k * f7[q] * pw;
+                for (double x : {q < 5 ? u4[q] : 1.0, u7[q]})
+                    if (!(std::fabs(x) <= 1e30 && std::fabs(x) >= 1e-30)) fold = false;
+            }
         }
-        pw = 1.0;
+        if (!fold) k = 1.0;
         for (int q = 0; q < 8; q++) {
             if (q < 5) {
                 sc.c[q] = (float)(k * f4[q]);
@@ -553,7 +569,7 @@ cudaError_t launch_eval(pppm_scene *s, const float4 *eval_a, const float4 *eval_
             const float v7 = fold ? (float)u7[q] : (float)(k * f7[q]);
             sc.p7[q] = make_float2(v7, v7);
         }
-        sc.t7 = fold ? (float)(2.0 * a * a * a) : 2.0f;
+        sc.t7 = fold ? (float)(2.0 * s->prm.a * s->prm.a * s->prm.a) : 2.0f;
     }
 #define PPPM_EVAL_ARGS sc, sidx, M, eval_a, eval_b, s->far, s->cell_start, s->cell_end, s->sub_start, s->sub_end, \
                        s->vrec, s->valf, s->dparams, \

@@ -113,7 +113,8 @@ __global__ void params_kernel(const float *__restrict__ partial, int nblocks, pp
     P->cr_f = float_below(((double)prm.K + 0.5) / invh);
     P->vh3_f = (float)(h * h * h);
     P->kdiag_f = (float)(0.5 * invh * kDiagPsi * (h * h));
-    const double a = prm.a;
+    const double a = (prm.a_cells > 0.0) ? prm.a_cells * h : prm.a;
+    P->a = a;
     P->inv_a3_f = (float)(1.0 / (a * a * a));
     P->inv4pia3_f = (float)(1.0 / (kFourPi * a * a * a));
     {

@@ -1,0 +1,329 @@
+// Temporally blocked red-black SOR smoother for the multigrid levels that
+// stream from HBM or L2 (edge >= kTbMinEdge): T half sweeps — T/2 of the
+// reference's red-black iterations (MG/Multigrid.cu:202-239, odd cells first,
+// omega = 1.43f) — in one pass over the level, optionally fused with the
+// prolongation by injection that precedes the post-smoothing
+// (MG/MultiGrid_kernel.cu, mg_ProlongationPeriodic3D2).
+//
+// Each CTA owns an output tile of TX x TY cells in (x, y) and a chunk of z
+// planes.  It streams planes of x and b through a ring of T + 3 slots in
+// shared memory, each slot a (TX + 2H) x (TY + 2T) box loaded by one TMA
+// tensor copy (cp.async.bulk.tensor.4d, completion on an mbarrier; H = T
+// rounded up to 4 so that the box's x coordinate stays 16-byte aligned).  The
+// box's cells beyond the grid arrive as zeros (the tensor map's out-of-bounds
+// fill), which are exactly the zero ghost values of the reference's operator;
+// they are never updated.  At step s, half sweep t (colour 1 for odd t, 0 for
+// even t) updates plane s - t + 1 in the box shrunk by t cells on each side,
+// in place: a half sweep reads only the other colour, which the previous half
+// sweep of the same plane and its two neighbours left final.  Plane s - T + 1
+// is then final and its TX x TY interior is stored with 128-bit stores into a
+// second array (x_out != x_in: the boxes of neighbouring tiles overlap).  A
+// z-chunk starts T planes early and ends T planes late, updating a plane at
+// half sweep t only where its whole dependency cone lies inside the chunk's
+// loaded planes, so the stored planes equal T plain half sweeps bit for bit.
+//
+// Every wait on an mbarrier is bounded; on running out the kernel records
+// kTbErrTimeout in *err, waits (again bounded) for its copies in flight and
+// returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <cstring>
+
+#include "pppm_internal.cuh"
+
+namespace pppm {
+
+namespace {
+
+constexpr float kOmegaF = 1.43f;
+constexpr float kOneMinusOmegaF = 1.0f - 1.43f;  // formed in float, MG/MultiGrid_kernel.cu:766
+constexpr uint32_t kWaitLimit = 1u << 22;         // polls of one mbarrier phase (each poll itself blocks a while)
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// One 4-D tiled tensor copy global -> shared (no multicast), completing on bar.
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
+                                            uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ float sor(float x, float nb, float b) {
+    const float r = nb - b;
+    return kOneMinusOmegaF * x + (kOmegaF * r) * (1.0f / 6.0f);
+}
+
+}  // namespace
+
+// Shared-memory bytes of one configuration (ring of x and b plus barriers).
+template <int T, int TX, int TY>
+struct TbShape {
+    static constexpr int H = (T + 3) / 4 * 4;  // x halo, a multiple of 4 floats
+    static constexpr int BX = TX + 2 * H;
+    static constexpr int BY = TY + 2 * T;
+    static constexpr int R = T + 3;
+    static constexpr int PLANE = BX * BY;                    // floats per slot
+    static constexpr uint32_t PLANE_BYTES = PLANE * 4u;
+    static constexpr size_t SMEM = 2ull * R * PLANE_BYTES + 8ull * R + 128;
+    static_assert(PLANE_BYTES % 128 == 0, "slots must stay 128-byte aligned");
+    static_assert(BX <= 256 && BY <= 256, "TMA box edge above 256");
+    static_assert(T % 2 == 0, "whole red-black iterations only");
+};
+
+template <int T, int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT)
+tb_smooth_kernel(const __grid_constant__ CUtensorMap map_x, const __grid_constant__ CUtensorMap map_b,
+                 int load_x, const float *__restrict__ xc, float *__restrict__ x_out, int d, int zchunk,
+                 int zchunks, uint32_t *__restrict__ err) {
+    using S = TbShape<T, TX, TY>;
+    constexpr int H = S::H, BX = S::BX, BY = S::BY, R = S::R, PLANE = S::PLANE;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    float *ring_x = reinterpret_cast<float *>(smem_raw);
+    float *ring_b = ring_x + R * PLANE;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(ring_b + R * PLANE);
+    __shared__ int s_abort;
+
+    const int tid = threadIdx.x;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int comp = blockIdx.z / zchunks, chunk = blockIdx.z % zchunks;
+    const int zc0 = chunk * zchunk, zc1 = min(d, zc0 + zchunk);
+    const int p_first = zc0 - T, p_last = zc1 + T - 1;
+    const size_t cells = (size_t)d * d * d;
+    const int dc = d >> 1;
+    const float *xcc = xc ? xc + (size_t)comp * dc * dc * dc : nullptr;
+    float *xo = x_out + (size_t)comp * cells;
+
+    if (tid == 0) {
+        for (int r = 0; r < R; r++) mbar_init(&bars[r], 1);
+        s_abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    const uint32_t tx_bytes = (load_x ? 2u : 1u) * S::PLANE_BYTES;
+    auto slot_of = [&](int p) { return (p - p_first) % R; };
+    auto issue = [&](int p) {  // thread 0 only
+        const int sl = slot_of(p);
+        mbar_expect_tx(&bars[sl], tx_bytes);
+        if (load_x) tma_load_4d(ring_x + sl * PLANE, &map_x, x0 - H, y0 - T, p, comp, &bars[sl]);
+        tma_load_4d(ring_b + sl * PLANE, &map_b, x0 - H, y0 - T, p, comp, &bars[sl]);
+    };
+    // Waits for plane p, then applies the start value: x as loaded, zero
+    // (load_x = 0), plus the injected coarse correction xc[parent] (xc set);
+    // cells outside the grid stay zero.
+    auto wait_prep = [&](int p) -> bool {
+        const int sl = slot_of(p);
+        const uint32_t parity = (uint32_t)((p - p_first) / R) & 1u;
+        uint32_t it = 0;
+        while (!mbar_try_wait(&bars[sl], parity)) {
+            if (++it > kWaitLimit) {
+                atomicExch(err, kTbErrTimeout);
+                s_abort = 1;
+                break;
+            }
+        }
+        if (load_x && !xcc) return true;
+        float *X = ring_x + sl * PLANE;
+        const bool zin = (p >= 0 && p < d);
+        for (int q = tid; q < PLANE; q += NT) {
+            const int gy = y0 - T + q / BX, gx = x0 - H + q % BX;
+            float v = load_x ? X[q] : 0.0f;
+            if (xcc && zin && gx >= 0 && gx < d && gy >= 0 && gy < d)
+                v += xcc[((size_t)(p >> 1) * dc + (gy >> 1)) * dc + (gx >> 1)];
+            X[q] = v;
+        }
+        return true;
+    };
+
+    if (tid == 0) {
+        for (int p = p_first; p <= min(p_first + 2, p_last); p++) issue(p);
+    }
+    wait_prep(p_first);
+    wait_prep(p_first + 1);
+
+    const int s_begin = zc0 - T + 1, s_end = zc1 + T - 2;
+    for (int s = s_begin; s <= s_end; s++) {
+        // every thread's generic accesses to the slot about to be refilled are
+        // done and ordered before the asynchronous copy into it
+        fence_proxy_async();
+        __syncthreads();
+        if (s_abort) break;
+        if (tid == 0 && s + 2 <= p_last) issue(s + 2);
+        wait_prep(s + 1);
+        __syncthreads();
+        if (s_abort) break;
+#pragma unroll
+        for (int t = 1; t <= T; t++) {
+            const int p = s - t + 1;
+            if (p >= max(0, zc0 - T + t) && p < min(d, zc1 + T - t)) {
+                const int c = t & 1;  // odd half sweeps: colour 1 (odd cells) first
+                float *X = ring_x + slot_of(p) * PLANE;
+                const float *Xm = ring_x + slot_of(p - 1) * PLANE;
+                const float *Xp = ring_x + slot_of(p + 1) * PLANE;
+                const float *B = ring_b + slot_of(p) * PLANE;
+                const int ya = max(0, y0 - T + t), yb = min(d, y0 + TY + T - t);
+                const int xa = max(0, x0 - T + t), xb = min(d, x0 + TX + T - t);
+                constexpr int PAIRS = BX / 2;
+                for (int q = tid; q < BY * PAIRS; q += NT) {
+                    const int sy = q / PAIRS;
+                    const int gy = y0 - T + sy;
+                    // box x origin x0 - H is even, so box and grid parities agree
+                    const int sx = 2 * (q % PAIRS) + ((c - gy - p) & 1);
+                    const int gx = x0 - H + sx;
+                    if (gy < ya || gy >= yb || gx < xa || gx >= xb) continue;
+                    const int o = sy * BX + sx;
+                    const float nb = ((X[o - 1] + X[o + 1]) + (X[o + BX] + X[o - BX])) + (Xm[o] + Xp[o]);
+                    X[o] = sor(X[o], nb, B[o]);
+                }
+            }
+            __syncthreads();
+        }
+        const int p = s - T + 1;
+        if (p >= zc0 && p < zc1) {
+            // 128-bit stores of the final TX x TY interior (x0, d multiples of 4)
+            const float *X = ring_x + slot_of(p) * PLANE;
+            constexpr int V = TX / 4;
+            for (int q = tid; q < TY * V; q += NT) {
+                const int ry = q / V, rx = 4 * (q % V);
+                const int gy = y0 + ry, gx = x0 + rx;
+                if (gy < d && gx < d) {
+                    const float4 v = *reinterpret_cast<const float4 *>(X + (ry + T) * BX + rx + H);
+                    *reinterpret_cast<float4 *>(xo + ((size_t)p * d + gy) * d + gx) = v;
+                }
+            }
+        }
+    }
+    if (s_abort && tid == 0) {
+        // let copies still in flight land before the CTA's shared memory goes away
+        for (int r = 0; r < R; r++) {
+            uint32_t it = 0;
+            while (!mbar_try_wait(&bars[r], 0) && !mbar_try_wait(&bars[r], 1) && ++it < kWaitLimit) {
+            }
+        }
+    }
+}
+
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// The configurations built; TbConfig::variant indexes this table.
+struct TbVariant {
+    int T, TX, TY, NT;
+    size_t smem;
+    const void *kernel;
+};
+
+template <int T, int TX, int TY, int NT>
+TbVariant make_variant() {
+    return TbVariant{T, TX, TY, NT, TbShape<T, TX, TY>::SMEM, (const void *)tb_smooth_kernel<T, TX, TY, NT>};
+}
+
+const TbVariant *variants(int *count) {
+    static const TbVariant v[] = {
+        make_variant<2, 64, 16, 256>(),
+        make_variant<4, 64, 16, 256>(),
+        make_variant<8, 32, 16, 256>(),
+        make_variant<4, 32, 16, 256>(),
+    };
+    *count = (int)(sizeof(v) / sizeof(v[0]));
+    return v;
+}
+
+}  // namespace
+
+int tb_variant_count() {
+    int c = 0;
+    variants(&c);
+    return c;
+}
+
+void tb_variant_shape(int variant, int *T, int *TX, int *TY) {
+    int c = 0;
+    const TbVariant *v = variants(&c);
+    const TbVariant &w = v[(variant >= 0 && variant < c) ? variant : 0];
+    *T = w.T;
+    *TX = w.TX;
+    *TY = w.TY;
+}
+
+// 4-D tensor map {d, d, d, comps} of FP32 over `base`, box {BX, BY, 1, 1}.
+cudaError_t tb_make_map(CUtensorMap *map, float *base, int d, int comps, int variant) {
+    PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
+    if (!fn) return cudaErrorNotSupported;
+    int c = 0;
+    const TbVariant &w = variants(&c)[variant];
+    const int H = (w.T + 3) / 4 * 4;
+    const cuuint64_t dims[4] = {(cuuint64_t)d, (cuuint64_t)d, (cuuint64_t)d, (cuuint64_t)comps};
+    const cuuint64_t strides[3] = {(cuuint64_t)d * 4, (cuuint64_t)d * d * 4, (cuuint64_t)d * d * d * 4};
+    const cuuint32_t box[4] = {(cuuint32_t)(w.TX + 2 * H), (cuuint32_t)(w.TY + 2 * w.T), 1, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    memset(map, 0, sizeof(*map));
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+// One pass of T half sweeps over a level: x_out = S^T(x_in [+ P xc], b).
+// map_x describes x_in (ignored when load_x = 0, start from zero); xc is the
+// coarser level's x for a fused prolongation, or null.
+cudaError_t tb_smooth(int variant, const CUtensorMap &map_x, const CUtensorMap &map_b, int load_x, const float *xc,
+                      float *x_out, int d, int comps, int zchunk, uint32_t *err, cudaStream_t st) {
+    int c = 0;
+    const TbVariant &w = variants(&c)[variant];
+    static bool attr_done[16] = {};
+    if (!attr_done[variant]) {
+        PPPM_CUDA_TRY(cudaFuncSetAttribute(w.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w.smem));
+        attr_done[variant] = true;
+    }
+    const int zchunks = (d + zchunk - 1) / zchunk;
+    const dim3 grid((d + w.TX - 1) / w.TX, (d + w.TY - 1) / w.TY, comps * zchunks);
+    void *args[] = {(void *)&map_x, (void *)&map_b, &load_x, (void *)&xc, &x_out, &d, &zchunk, (void *)&zchunks,
+                    &err};
+    ::pppm::note_launch();
+    return cudaLaunchKernel(w.kernel, grid, dim3(w.NT), args, w.smem, st);
+}
+
+}  // namespace pppm

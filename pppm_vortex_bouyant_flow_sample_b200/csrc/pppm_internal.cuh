@@ -45,6 +45,7 @@ struct DevParams {
     float cr_f;         // largest float strictly below (K+0.5)/invh
     float vh3_f;        // (float)(h^3) for the mesh correction
     float kdiag_f;      // (float)(0.5 * invh * 0.250580605913965 * h^2)
+    double a;           // smoothing radius of this build (prm.a, or prm.a_cells * cell_h)
     float inv_a3_f;     // 1/a^3
     float inv4pia3_f;   // 1/(4 pi a^3)
     int32_t need_exp;   // some pair inside the box can reach (r/a)^3 >= 0.25

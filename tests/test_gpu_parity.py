@@ -192,7 +192,9 @@ def test_mg_vcycle_each_level(pb, oracle, n):
     """m_Vcycle(x, b, tol, res, level) (MG/MultiGrid.cpp:128-201): one V(4,4)
     cycle on level `level`'s arrays.  The hierarchy below level l is the one a
     grid of that level's edge has, so the oracle's cycle on that edge is the
-    check, starting from a nonzero x."""
+    check, starting from a nonzero x.  The cycle's correction is computed in
+    FP32 (r = b - A x in FP64, e = V32(0, r), x += e), so a random b and x hold
+    it to 2e-6."""
     import torch
     mg = pb.MultiGridSolver3DPeriod_double()
     mg.m_InitialSystem(n, n, n)
@@ -205,7 +207,7 @@ def test_mg_vcycle_each_level(pb, oracle, n):
         x = _dev(x0)
         mg.m_Vcycle(x, _dev(b), 1e-10, None, level)
         want = oracle.mg_vcycle(x0, b, d)
-        assert rel_l2(x.cpu().numpy(), want) <= 1e-6, (level, d)
+        assert rel_l2(x.cpu().numpy(), want) <= 2e-6, (level, d)
     with pytest.raises(pb.PppmError):
         mg.m_Vcycle(torch.zeros(8, dtype=torch.float64, device="cuda"), torch.zeros(8, dtype=torch.float64,
                                                                                    device="cuda"), 0, None, len(edges))
