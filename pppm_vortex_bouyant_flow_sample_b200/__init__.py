@@ -63,6 +63,14 @@ def _alpha3(t: torch.Tensor, N: int):
     return [t[c].contiguous() for c in range(3)]
 
 
+def tuning_report() -> str:
+    """The multigrid smoother autotuner's measurements (pppm_tuning_report)."""
+    buf = C.create_string_buffer(8192)
+    n = C.c_size_t()
+    check(load().pppm_tuning_report(buf, 8192, C.byref(n)), "pppm_tuning_report")
+    return buf.value.decode()
+
+
 class Scene:
     """One resident PPPM scene (pppm_scene)."""
 

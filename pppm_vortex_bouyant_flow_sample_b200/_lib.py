@@ -35,7 +35,7 @@ EXPORTED = (
     "pppm_potential_destroy", "pppm_potential_set_masses", "pppm_potential_build", "pppm_potential_eval_gradient",
     "pppm_potential_eval_scalar", "pppm_potential_dphidn", "pppm_potential_grids", "pppm_potential_eval_gradient3",
     "pppm_debug_fail_allocation", "pppm_mg_vcycle", "pppm_mg_levels", "pppm_params_accurate",
-    "pppm_get_smoothing",
+    "pppm_get_smoothing", "pppm_tuning_report",
 )
 REQ_EVAL, REQ_ADVANCE = 0, 1
 NOALLOC_MAX_PARTICLES = 1048576  # PPPM_NOALLOC_MAX_PARTICLES in include/pppm.h
@@ -124,6 +124,7 @@ def load(build_if_missing: bool = True):
         "pppm_mg_create": (st, [u32, vp, C.POINTER(vp)]),
         "pppm_mg_destroy": (st, [vp]),
         "pppm_mg_full_multigrid": (st, [vp, vp, vp, C.c_int, C.c_double, C.c_int, C.POINTER(C.c_double)]),
+        "pppm_tuning_report": (st, [C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
         "pppm_params_accurate": (st, [C.POINTER(PppmParams)]),
         "pppm_get_smoothing": (st, [vp, C.POINTER(C.c_double)]),
         "pppm_mg_vcycle": (st, [vp, vp, vp, C.c_int]),

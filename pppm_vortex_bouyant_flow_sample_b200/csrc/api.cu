@@ -212,6 +212,24 @@ cudaError_t alloc_grid_side(pppm_scene *s) {
         s->lv[l].x = p; p += 3 * (size_t)s->lv[l].cells;
         s->lv[l].b = p; p += 3 * (size_t)s->lv[l].cells;
     }
+    {
+        // second x copies and tensor maps of the blocked-smoother levels
+        pppm::MGPlan m;
+        m.levels = s->levels;
+        for (int l = 0; l < s->levels; l++) m.lv[l] = s->lv[l];
+        m.comps = 3;
+        const int variant = pppm::mg_tb_default_variant();
+        const size_t extra = variant != -1 ? pppm::mg_tb_extra_floats(m) : 0;
+        if (extra) {
+            PPPM_CUDA_TRY(dalloc(&s->mg_x2_pool, extra));
+            PPPM_CUDA_TRY(dalloc(&s->mg_err, 1));
+            PPPM_CUDA_TRY(cudaMemset(s->mg_err, 0, sizeof(uint32_t)));
+            m.err = s->mg_err;
+            PPPM_CUDA_TRY(pppm::mg_tb_setup(m, s->mg_x2_pool, variant));
+            for (int l = 0; l < s->levels; l++) s->lv[l].x2 = m.lv[l].x2;
+        }
+        s->mg_tb = m;
+    }
     PPPM_CUDA_TRY(dalloc(&s->vort, 3 * (size_t)s->C));
     PPPM_CUDA_TRY(dalloc(&s->psi, 3 * (size_t)s->C));
     PPPM_CUDA_TRY(dalloc(&s->far, 3 * (size_t)s->C));
@@ -252,6 +270,8 @@ void destroy_scene(pppm_scene *s) {
     free_eval_side(s);
     cudaFree(s->hist);
     cudaFree(s->mg_pool);
+    cudaFree(s->mg_x2_pool);
+    cudaFree(s->mg_err);
     cudaFree(s->vort);
     cudaFree(s->psi);
     cudaFree(s->far);
@@ -317,6 +337,17 @@ extern "C" pppm_status pppm_params_default(pppm_params *p) {
     p->mg_mode = PPPM_MG_REFERENCE;
     p->mg_tol = 1e-10;
     p->mg_max_cycles = 50;
+    return PPPM_OK;
+}
+
+extern "C" pppm_status pppm_tuning_report(char *buf, size_t cap, size_t *written) {
+    if (!buf || cap == 0) {
+        snprintf(g_err, sizeof(g_err), "pppm_tuning_report: empty buffer");
+        return PPPM_ERR_INVALID;
+    }
+    const size_t w = pppm::mg_tune_report(buf, cap);
+    buf[w < cap ? w : cap - 1] = 0;
+    if (written) *written = w < cap ? w : cap - 1;
     return PPPM_OK;
 }
 
@@ -808,6 +839,8 @@ extern "C" pppm_status pppm_get_stats(pppm_scene *s, uint64_t *pairs, int32_t *m
 struct pppm_mg {
     pppm::MGPlan plan;
     float *pool = nullptr;
+    float *x2_pool = nullptr;               // second x copies of the blocked-smoother levels
+    uint32_t *err = nullptr;                // its device error flag
     double *r64 = nullptr, *e64 = nullptr;  // residual of the initial guess, its correction
     double *coarse_op = nullptr;            // coarsest-level operator (levels >= 2)
     cudaGraphExec_t graph = nullptr;        // reference-schedule solve of r64 into e64, captured on first use
@@ -891,6 +924,29 @@ extern "C" pppm_status pppm_mg_create(uint32_t n, void *stream, pppm_mg **out) {
         P.lv[l].x = p; p += P.lv[l].cells;
         P.lv[l].b = p; p += P.lv[l].cells;
     }
+    {
+        const int variant = pppm::mg_tb_default_variant();
+        const size_t extra = variant != -1 ? pppm::mg_tb_extra_floats(P) : 0;
+        if (extra) {
+            e = dalloc(&m->x2_pool, extra);
+            if (e == cudaSuccess) e = dalloc(&m->err, 1);
+            if (e == cudaSuccess) e = cudaMemset(m->err, 0, sizeof(uint32_t));
+            P.err = m->err;
+            if (e == cudaSuccess) e = pppm::mg_tb_setup(P, m->x2_pool, variant);
+        }
+        if (e != cudaSuccess) {
+            pppm_status st = cuda_fail("pppm_mg_create", e);
+            cudaFree(m->pool);
+            cudaFree(P.norms);
+            cudaFree(m->r64);
+            cudaFree(m->e64);
+            cudaFree(m->coarse_op);
+            cudaFree(m->x2_pool);
+            cudaFree(m->err);
+            delete m;
+            return st;
+        }
+    }
     *out = m;
     return PPPM_OK;
 }
@@ -905,6 +961,8 @@ extern "C" pppm_status pppm_mg_destroy(pppm_mg *m) {
     cudaFree(m->r64);
     cudaFree(m->e64);
     cudaFree(m->coarse_op);
+    cudaFree(m->x2_pool);
+    cudaFree(m->err);
     delete m;
     return PPPM_OK;
 }
@@ -974,7 +1032,11 @@ extern "C" pppm_status pppm_mg_vcycle(pppm_mg *m, double *x, const double *b, in
     // FP32 V-cycle solves for the correction from zero, and x += e.
     pppm::MGPlan P = m->plan;
     P.levels = m->plan.levels - level;
-    for (int l = 0; l < P.levels; l++) P.lv[l] = m->plan.lv[level + l];
+    for (int l = 0; l < P.levels; l++) {
+        P.lv[l] = m->plan.lv[level + l];
+        P.tb_maps[l] = m->plan.tb_maps[level + l];
+        P.tb_zchunk[l] = m->plan.tb_zchunk[level + l];
+    }
     P.coarse_op = (P.levels >= 2) ? m->coarse_op : nullptr;
     const size_t C = P.lv[0].cells;
     ::pppm::note_launch();

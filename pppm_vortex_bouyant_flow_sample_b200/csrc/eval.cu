@@ -174,6 +174,26 @@ __device__ __forceinline__ float sqrt_approx(float x) {
     return r;
 }
 
+// rsqrt.approx.ftz.f32 and ex2.approx.ftz.f32: one special-function op each.
+__device__ __forceinline__ float rsqrt_approx(float x) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float ex2_approx(float x) {
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// Exp-form constants of the warp-uniform walk for scenes whose pairs reach
+// t = (r/a)^3 >= 2 (smoothing radius of about a cell or less).
+struct ExpForm {
+    float2 inv_a3;   // {1/a^3, 1/a^3}
+    float2 nl2a3;    // {-log2(e)/a^3, ...}: the exponent of e^-t in base 2, per r^3
+    float tsmall;    // below it phi comes from the polynomial (1 - e^-t cancels)
+};
+
 __device__ __forceinline__ void stage_record(float *__restrict__ pk, int slot, int half, float4 r, float4 a,
                                              float3 o) {
     float *A = pk + 4 * (0 * kPackSlots + slot), *B = pk + 4 * (1 * kPackSlots + slot);
@@ -204,7 +224,7 @@ __device__ __forceinline__ void cell_pairs_packed(const float4 *__restrict__ vre
                                                   const float3 rb, float3 o, const float3 blo, const float3 bhi,
                                                   float2 inv_a3, const float2 *cf, float tbig, float inv4pia3,
                                                   bool need_exp, float4 *__restrict__ pk4, int lane,
-                                                  PairAcc2 &acc) {
+                                                  PairAcc2 &acc, const ExpForm &xf) {
     float *pk = reinterpret_cast<float *>(pk4);
     const float2 tx = make_float2(ra.x, ra.x), ty = make_float2(ra.y, ra.y), tz = make_float2(ra.z, ra.z);
     for (uint32_t base = ps; base < pe; base += 32) {
@@ -249,9 +269,33 @@ __device__ __forceinline__ void cell_pairs_packed(const float4 *__restrict__ vre
                 ok0 = ok0 && !(e2.x < 1e-24f);
                 ok1 = ok1 && !(e2.y < 1e-24f);
             }
+            float2 c;
+            if constexpr (DEG == 0) {
+                // exp form, c * 4 pi = (1 - e^-t) / r^3 with t = r^3 / a^3: r^-1
+                // from rsqrt, e^-t from ex2 (two special-function ops); where
+                // some lane has t < tsmall (1 - e^-t cancels, or r = 0) the
+                // degree-5 polynomial phi(t) / a^3 replaces it
+                const float2 r2c = make_float2(fmaxf(r2.x, 1e-30f), fmaxf(r2.y, 1e-30f));
+                const float2 rs = make_float2(rsqrt_approx(r2c.x), rsqrt_approx(r2c.y));
+                const float2 r3 = __fmul2_rn(r2c, __fmul2_rn(r2c, rs));
+                const float2 ri3 = __fmul2_rn(__fmul2_rn(rs, rs), rs);
+                const float2 ex = __fmul2_rn(r3, xf.nl2a3);
+                const float2 e = make_float2(ex2_approx(ex.x), ex2_approx(ex.y));
+                c = __ffma2_rn(make_float2(-e.x, -e.y), ri3, ri3);
+                const float2 t = __fmul2_rn(r3, xf.inv_a3);
+                const bool s0 = ok0 && t.x < xf.tsmall, s1 = ok1 && t.y < xf.tsmall;
+                if (__any_sync(0xffffffffu, s0 || s1)) {
+                    float2 p = __ffma2_rn(cf[5], t, cf[4]);
+#pragma unroll
+                    for (int q = 3; q >= 0; q--) p = __ffma2_rn(p, t, cf[q]);
+                    p = __fmul2_rn(p, xf.inv_a3);
+                    c.x = s0 ? p.x : c.x;
+                    c.y = s1 ? p.y : c.y;
+                }
+            } else {
             const float2 r3 = __fmul2_rn(r2, make_float2(sqrt_approx(r2.x), sqrt_approx(r2.y)));
             const float2 t = FOLD ? r3 : __fmul2_rn(r3, inv_a3);
-            float2 c = __ffma2_rn(cf[DEG], t, cf[DEG - 1]);
+            c = __ffma2_rn(cf[DEG], t, cf[DEG - 1]);
 #pragma unroll
             for (int q = DEG - 2; q >= 0; q--) c = __ffma2_rn(c, t, cf[q]);
             if (DEG > 4 && need_exp) {
@@ -263,6 +307,7 @@ __device__ __forceinline__ void cell_pairs_packed(const float4 *__restrict__ vre
                     c.x = big0 ? e0 : c.x;
                     c.y = big1 ? e1 : c.y;
                 }
+            }
             }
             const float2 coeff = make_float2(ok0 ? c.x : 0.0f, ok1 ? c.y : 0.0f);
             acc.ax = __ffma2_rn(coeff, make_float2(B.z, B.w), acc.ax);
@@ -290,6 +335,7 @@ struct SmoothSeries {
     float c[5];    // degree 4 on [0, 0.25], in t (a lane's own walk)
     float2 p4[5];  // degree 4 on [0, 0.25], packed
     float2 p7[8];  // degree 7 on [0, 2], packed
+    float2 p5[6];  // degree 5 on [0, 0.5] in t, unit scale (exp-form walk)
     float t7;      // 2 in the packed polynomials' variable: where the exp form takes over
 };
 
@@ -337,15 +383,21 @@ __global__ void __launch_bounds__(kEvalThreads, 8) eval_kernel(const SmoothSerie
     PairAcc acc;
     PairAcc2 acc2;
     float3 o_w = make_float3(0.f, 0.f, 0.f);
+    // some pair can reach t = 2: the exp-form walk (its sums carry 4 pi)
+    const bool tier0 = P->need_exp2 != 0;
     if (K >= 0) {
         // FOLD: coefficients carry 1/(4 pi a^3); otherwise they have unit
         // scale and the sums are scaled once per point below
         const float cr = P->cr_f, inv_a3 = P->inv_a3_f, inv4pia3 = FOLD ? P->inv4pia3_f : 1.0f;
         const bool need_exp = P->need_exp != 0;
         const float *cf = sc.c;
-        // some pair can reach t = 0.25: the degree-7 polynomial, exp above t = 2
-        const bool tier7 = need_exp;
+        // some pair can reach t = 0.25 (but not 2): the degree-7 polynomial
+        const bool tier7 = need_exp && !tier0;
         const bool need_exp2 = P->need_exp2 != 0;
+        ExpForm xf;
+        xf.inv_a3 = make_float2(inv_a3, inv_a3);
+        xf.nl2a3 = make_float2(-1.4426950408889634f * inv_a3, -1.4426950408889634f * inv_a3);
+        xf.tsmall = 0.5f;
         // warp origin of the packed accumulation: lane 0's position
         const float3 o = make_float3(__shfl_sync(0xffffffffu, ra.x, 0), __shfl_sync(0xffffffffu, ra.y, 0),
                                      __shfl_sync(0xffffffffu, ra.z, 0));
@@ -423,14 +475,15 @@ __global__ void __launch_bounds__(kEvalThreads, 8) eval_kernel(const SmoothSerie
                         if (ps == kEmpty) continue;
                         const bool lane_ok = act && ci >= rlo[0] && ci <= rhi[0] && cj >= rlo[1] && cj <= rhi[1] &&
                                              ck >= rlo[2] && ck <= rhi[2];
-                        cell_pairs_packed<SEG, COUNT, FOLD, D>(vrec, valf, ps, pe, lane_ok ? cr : -1.0f, ra, rb, o,
-                                                               blo, bhi, inv_a3_2, D == 7 ? sc.p7 : sc.p4,
-                                                               sc.t7, inv4pia3, D == 7 && need_exp2, pk, lane,
-                                                               acc2);
+                        cell_pairs_packed<SEG, COUNT, FOLD, D>(
+                            vrec, valf, ps, pe, lane_ok ? cr : -1.0f, ra, rb, o, blo, bhi, inv_a3_2,
+                            D == 0 ? sc.p5 : (D == 7 ? sc.p7 : sc.p4), sc.t7, inv4pia3, D == 7 && need_exp2, pk,
+                            lane, acc2, xf);
                     }
         };
         if (vol > 0 && vol <= kUniformMaxSub) {
-            if (tier7) uniform_walk(std::integral_constant<int, 7>{});
+            if (tier0) uniform_walk(std::integral_constant<int, 0>{});
+            else if (tier7) uniform_walk(std::integral_constant<int, 7>{});
             else uniform_walk(std::integral_constant<int, 4>{});
         } else if (act && lo[0] <= hi[0]) {
             // scattered warp (points outside the grid, sparse regions): own walk
@@ -449,7 +502,15 @@ __global__ void __launch_bounds__(kEvalThreads, 8) eval_kernel(const SmoothSerie
         const float Ax = acc2.ax.x + acc2.ax.y, Ay = acc2.ay.x + acc2.ay.y, Az = acc2.az.x + acc2.az.y;
         const float Bx = acc2.bx.x + acc2.bx.y, By = acc2.by.x + acc2.by.y, Bz = acc2.bz.x + acc2.bz.y;
         const float sx = ra.x - o_w.x, sy = ra.y - o_w.y, sz = ra.z - o_w.z;
-        if (FOLD) {
+        if (tier0) {
+            // exp-form sums carry 4 pi (the reference's literal); the lane's
+            // own walk carries the scale of its coefficients
+            const float kown = FOLD ? 1.0f : P->inv4pia3_f;
+            const float k4 = (float)(1.0 / kFourPi);
+            ux = fmaf(fmaf(Ay, sz, -(Az * sy)) - Bx, k4, fmaf(acc.x, kown, ux));
+            uy = fmaf(fmaf(Az, sx, -(Ax * sz)) - By, k4, fmaf(acc.y, kown, uy));
+            uz = fmaf(fmaf(Ax, sy, -(Ay * sx)) - Bz, k4, fmaf(acc.z, kown, uz));
+        } else if (FOLD) {
             ux += acc.x + (fmaf(Ay, sz, -(Az * sy)) - Bx);
             uy += acc.y + (fmaf(Az, sx, -(Ax * sz)) - By);
             uz += acc.z + (fmaf(Ax, sy, -(Ay * sx)) - Bz);
@@ -543,9 +604,11 @@ cudaError_t launch_eval(pppm_scene *s, const float4 *eval_a, const float4 *eval_
     // the device parameters once per point.
     bool fold = s->prm.a_cells <= 0.0;
     {
-        double f4[5], f7[8];
+        double f4[5], f7[8], f5[6];
         phi_chebyshev(4, 0.25, f4);
         phi_chebyshev(7, 2.0, f7);
+        phi_chebyshev(5, 0.5, f5);
+        for (int q = 0; q < 6; q++) sc.p5[q] = make_float2((float)f5[q], (float)f5[q]);
         double u4[5], u7[8], k = 1.0;
         if (fold) {
             const double a = s->prm.a;

@@ -18,7 +18,11 @@
 // V(psi, b) in exact arithmetic because the V-cycle is a consistent linear
 // iteration.  The coarsest solve is FP64.  Every kernel handles the three
 // potential components of a scene in one launch (grid y = component).
+#include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <cstdio>
+#include <mutex>
 
 #include "pppm_internal.cuh"
 
@@ -298,37 +302,88 @@ bool mg_shape_ok(uint32_t n) {
     return true;
 }
 
-// One FP32 V(4,4) cycle from level `level` down (MG/MultiGrid.cpp:128-201).
-static cudaError_t vcycle32(const MGPlan &m, int level) {
-    const int L = m.levels;
-    for (int j = level + 1; j < L; j++)
-        PPPM_CUDA_TRY(cudaMemsetAsync(m.lv[j].x, 0, sizeof(float) * m.comps * (size_t)m.lv[j].cells, m.st));
-    for (int j = level; j < L - 1; j++) {
-        const int d = (int)m.lv[j].d;
-        const dim3 g = grid_for((uint32_t)(d / 2) * d * d, m.comps);
-        for (int it = 0; it < 4; it++) {
+// Where a level's x lives between kernels of the blocked smoother.
+enum XAt { kXZero = 0, kXMain = 1, kXAlt = 2 };
+
+static bool tb_level(const MGPlan &m, int j) { return m.tb_var[j] >= 0 && m.lv[j].x2; }
+
+static float *x_ptr(const MGPlan &m, int j, XAt at) { return at == kXAlt ? m.lv[j].x2 : m.lv[j].x; }
+
+// Four red-black iterations (8 half sweeps, odd cells first) at level j,
+// starting from `in` (zero, or x in one of the two copies) plus, when xc is
+// set, the injected coarse correction xc[parent] (the prolongation that
+// precedes the reference's post-smoothing).  Blocked levels run 8 / T passes
+// of the blocked smoother, ping-ponging between the two copies; the others run
+// the half sweeps in place on the main copy.  Returns where the result is:
+// a pre-smoothing from zero ends in the main copy for an even pass count and
+// in the second copy for an odd one, a post-smoothing from there always ends
+// in the main copy.
+static cudaError_t smooth(const MGPlan &m, int j, XAt in, const float *xc, XAt *out) {
+    const Level &L = m.lv[j];
+    const int d = (int)L.d;
+    if (tb_level(m, j)) {
+        int T = 0, TX = 0, TY = 0;
+        tb_variant_shape(m.tb_var[j], &T, &TX, &TY);
+        const int passes = 8 / T;
+        if (xc && !m.tb_fuse_prolong) {
+            // the prolongation as its own kernel into the pass's input
+            const XAt at = (in == kXZero) ? kXMain : in;
+            float *dst = x_ptr(m, j, at);
+            if (in == kXZero) PPPM_CUDA_TRY(cudaMemsetAsync(dst, 0, sizeof(float) * m.comps * (size_t)L.cells, m.st));
             ::pppm::note_launch();
-            rbsor_kernel<<<g, kMGThreads, 0, m.st>>>(m.lv[j].x, m.lv[j].b, d, 1, edge_log2(d));
-            ::pppm::note_launch();
-            rbsor_kernel<<<g, kMGThreads, 0, m.st>>>(m.lv[j].x, m.lv[j].b, d, 0, edge_log2(d));
+            prolong_kernel<<<grid_for(L.cells, m.comps), kMGThreads, 0, m.st>>>(dst, xc, d, edge_log2(d));
+            in = at;
+            xc = nullptr;
         }
+        XAt cur = in;
+        for (int p = 0; p < passes; p++) {
+            const XAt dst = (cur == kXAlt) ? kXMain : kXAlt;
+            const CUtensorMap &mx = (cur == kXAlt) ? m.tb_maps[j].x2 : m.tb_maps[j].x;
+            PPPM_CUDA_TRY(tb_smooth(m.tb_var[j], mx, m.tb_maps[j].b, L.b, cur != kXZero, p == 0 ? xc : nullptr,
+                                    x_ptr(m, j, dst), d, m.comps, m.tb_zchunk[j], m.err, m.st));
+            cur = dst;
+        }
+        *out = cur;
+        return cudaSuccess;
+    }
+    if (in == kXZero) PPPM_CUDA_TRY(cudaMemsetAsync(L.x, 0, sizeof(float) * m.comps * (size_t)L.cells, m.st));
+    if (xc) {
+        ::pppm::note_launch();
+        prolong_kernel<<<grid_for(L.cells, m.comps), kMGThreads, 0, m.st>>>(L.x, xc, d, edge_log2(d));
+    }
+    const dim3 g = grid_for((uint32_t)(d / 2) * d * d, m.comps);
+    for (int it = 0; it < 4; it++) {
+        ::pppm::note_launch();
+        rbsor_kernel<<<g, kMGThreads, 0, m.st>>>(L.x, L.b, d, 1, edge_log2(d));
+        ::pppm::note_launch();
+        rbsor_kernel<<<g, kMGThreads, 0, m.st>>>(L.x, L.b, d, 0, edge_log2(d));
+    }
+    *out = kXMain;
+    return cudaGetLastError();
+}
+
+// One FP32 V(4,4) cycle from level `level` down (MG/MultiGrid.cpp:128-201).
+// The cycle's x at `level` starts at zero plus, when xc is set, the injected
+// correction from level + 1 (the full multigrid's prolongation); the coarser
+// levels start at zero as the reference zeroes them.  The result is left in
+// lv[level].x.
+static cudaError_t vcycle32(const MGPlan &m, int level, const float *xc = nullptr) {
+    const int L = m.levels;
+    XAt at[kMaxLevels];
+    for (int j = level; j < L - 1; j++) {
+        PPPM_CUDA_TRY(smooth(m, j, kXZero, j == level ? xc : nullptr, &at[j]));
         ::pppm::note_launch();
         resid_restrict_kernel<<<grid_for(m.lv[j + 1].cells, m.comps), kMGThreads, 0, m.st>>>(
-            m.lv[j].x, m.lv[j].b, m.lv[j + 1].b, (int)m.lv[j + 1].d, 0, edge_log2((int)m.lv[j + 1].d));
+            x_ptr(m, j, at[j]), m.lv[j].b, m.lv[j + 1].b, (int)m.lv[j + 1].d, 0, edge_log2((int)m.lv[j + 1].d));
     }
+    // the coarsest solve starts from zero (a cycle on the coarsest level alone
+    // included: it is only ever asked for from a zero start)
+    if (level == L - 1 || !m.coarse_op)
+        PPPM_CUDA_TRY(cudaMemsetAsync(m.lv[L - 1].x, 0, sizeof(float) * m.comps * (size_t)m.lv[L - 1].cells, m.st));
     coarse_solve(m);
     for (int j = L - 2; j >= level; j--) {
-        const int d = (int)m.lv[j].d;
-        ::pppm::note_launch();
-        prolong_kernel<<<grid_for(m.lv[j].cells, m.comps), kMGThreads, 0, m.st>>>(m.lv[j].x, m.lv[j + 1].x, d,
-                                                                                  edge_log2(d));
-        const dim3 g = grid_for((uint32_t)(d / 2) * d * d, m.comps);
-        for (int it = 0; it < 4; it++) {
-            ::pppm::note_launch();
-            rbsor_kernel<<<g, kMGThreads, 0, m.st>>>(m.lv[j].x, m.lv[j].b, d, 1, edge_log2(d));
-            ::pppm::note_launch();
-            rbsor_kernel<<<g, kMGThreads, 0, m.st>>>(m.lv[j].x, m.lv[j].b, d, 0, edge_log2(d));
-        }
+        XAt res;
+        PPPM_CUDA_TRY(smooth(m, j, at[j], m.lv[j + 1].x, &res));
     }
     return cudaGetLastError();
 }
@@ -338,21 +393,15 @@ static cudaError_t vcycle32(const MGPlan &m, int level) {
 // plain restriction of b).
 static cudaError_t fmg32(const MGPlan &m) {
     const int L = m.levels;
-    for (int j = 0; j < L; j++)
-        PPPM_CUDA_TRY(cudaMemsetAsync(m.lv[j].x, 0, sizeof(float) * m.comps * (size_t)m.lv[j].cells, m.st));
     for (int j = 0; j < L - 1; j++) {
         ::pppm::note_launch();
         resid_restrict_kernel<<<grid_for(m.lv[j + 1].cells, m.comps), kMGThreads, 0, m.st>>>(
             m.lv[j].x, m.lv[j].b, m.lv[j + 1].b, (int)m.lv[j + 1].d, 1, edge_log2((int)m.lv[j + 1].d));
     }
+    PPPM_CUDA_TRY(cudaMemsetAsync(m.lv[L - 1].x, 0, sizeof(float) * m.comps * (size_t)m.lv[L - 1].cells, m.st));
     coarse_solve(m);
     PPPM_CUDA_TRY(cudaGetLastError());
-    for (int j = L - 2; j >= 0; j--) {
-        ::pppm::note_launch();
-        prolong_kernel<<<grid_for(m.lv[j].cells, m.comps), kMGThreads, 0, m.st>>>(
-            m.lv[j].x, m.lv[j + 1].x, (int)m.lv[j].d, edge_log2((int)m.lv[j].d));
-        PPPM_CUDA_TRY(vcycle32(m, j));
-    }
+    for (int j = L - 2; j >= 0; j--) PPPM_CUDA_TRY(vcycle32(m, j, m.lv[j + 1].x));
     return cudaGetLastError();
 }
 
@@ -371,7 +420,6 @@ static cudaError_t dc_residual(const MGPlan &m, bool want_norms) {
 // e = V32(0, r); psi += e.
 static cudaError_t dc_correct(const MGPlan &m) {
     const uint32_t C0 = m.lv[0].cells;
-    PPPM_CUDA_TRY(cudaMemsetAsync(m.lv[0].x, 0, sizeof(float) * m.comps * (size_t)C0, m.st));
     PPPM_CUDA_TRY(vcycle32(m, 0));
     const size_t cnt = (size_t)m.comps * C0;
     ::pppm::note_launch();
@@ -385,7 +433,6 @@ static cudaError_t dc_correct(const MGPlan &m) {
 // being a consistent linear iteration (MG/MultiGrid.cpp:128-201).
 cudaError_t mg_vcycle_update(const MGPlan &m, double *x64) {
     const uint32_t C0 = m.lv[0].cells;
-    PPPM_CUDA_TRY(cudaMemsetAsync(m.lv[0].x, 0, sizeof(float) * m.comps * (size_t)C0, m.st));
     PPPM_CUDA_TRY(vcycle32(m, 0));
     const size_t cnt = (size_t)m.comps * C0;
     ::pppm::note_launch();
@@ -451,8 +498,218 @@ cudaError_t mg_capture_graph(const MGPlan &m_in, cudaGraphExec_t *exec, unsigned
     return e;
 }
 
+size_t mg_tb_extra_floats(const MGPlan &m) {
+    size_t f = 0;
+    for (int j = 0; j < m.levels; j++)
+        if (m.lv[j].d >= m.tb_min_edge && (m.lv[j].d % 4) == 0) f += (size_t)m.comps * m.lv[j].cells;
+    return f;
+}
+
+// z-chunk length of a level for a variant: fill the resident CTA slots in
+// whole waves, each chunk paying 2T extra planes of pipeline start and end.
+static int pick_zchunk(int d, int comps, int variant, int sms, int per_sm) {
+    int T = 0, TX = 0, TY = 0;
+    tb_variant_shape(variant, &T, &TX, &TY);
+    const long slots = (long)sms * std::max(per_sm, 1);
+    const long tiles = (long)((d + TX - 1) / TX) * ((d + TY - 1) / TY) * comps;
+    const long cmax = std::max(1L, (long)(d / (2 * T)));
+    long best_c = 1;
+    double best = -1.0;
+    for (long c = 1; c <= cmax; c++) {
+        const long zc = (d + c - 1) / c, n_cta = tiles * ((d + zc - 1) / zc);
+        const long waves = (n_cta + slots - 1) / slots;
+        const double eff = (double)n_cta / (double)(waves * slots) * (double)zc / (double)(zc + 2 * T);
+        if (eff > best + 1e-9) {
+            best = eff;
+            best_c = c;
+        }
+    }
+    return (int)((d + best_c - 1) / best_c);
+}
+
+namespace {
+// Autotuner results: fastest smoother (variant, or -1 for the plain half
+// sweeps) per (device, level edge, components), measured once per process.
+struct TuneKey {
+    int dev, d, comps;
+    bool operator==(const TuneKey &o) const { return dev == o.dev && d == o.d && comps == o.comps; }
+};
+struct TuneEntry {
+    TuneKey key;
+    int variant;
+    float ms[16];  // measured time of 8 half sweeps per candidate (index variant + 1)
+};
+std::mutex g_tune_mutex;
+TuneEntry g_tune[64];
+int g_tune_count = 0;
+}  // namespace
+
+// Times 8 half sweeps (four red-black iterations) of level j with the plain
+// kernels and with every blocked variant, on the level's own buffers (zeroed
+// first), and returns the fastest.  Every candidate computes the same values
+// bit for bit, so the choice only changes the time.
+static cudaError_t tune_level(MGPlan &m, int j, int sms, int dev, int *best_out, float *ms_out) {
+    Level &L = m.lv[j];
+    const int d = (int)L.d;
+    const int nvar = tb_variant_count();
+    cudaStream_t st = nullptr;
+    PPPM_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    const size_t bytes = sizeof(float) * m.comps * (size_t)L.cells;
+    if (e == cudaSuccess) e = cudaMemsetAsync(L.x, 0, bytes, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(L.x2, 0, bytes, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(L.b, 0, bytes, st);
+    int best = -1;
+    float best_ms = 1e30f;
+    for (int v = -1; v < nvar && e == cudaSuccess; v++) {
+        MGPlan t = m;
+        t.st = st;
+        for (int q = 0; q < kMaxLevels; q++) t.tb_var[q] = -1;
+        if (v >= 0) {
+            int per_sm = 1;
+            e = tb_prepare(v, &per_sm);
+            if (e == cudaSuccess) e = tb_make_map(&t.tb_maps[j].x, L.x, d, m.comps, v);
+            if (e == cudaSuccess) e = tb_make_map(&t.tb_maps[j].x2, L.x2, d, m.comps, v);
+            if (e == cudaSuccess) e = tb_make_map(&t.tb_maps[j].b, L.b, d, m.comps, v);
+            if (e != cudaSuccess) break;
+            t.tb_var[j] = v;
+            t.tb_zchunk[j] = pick_zchunk(d, m.comps, v, sms, per_sm);
+        }
+        float tmin = 1e30f;
+        for (int rep = 0; rep < 4 && e == cudaSuccess; rep++) {
+            XAt out;
+            e = cudaEventRecord(e0, st);
+            if (e == cudaSuccess) e = smooth(t, j, kXMain, nullptr, &out);
+            if (e == cudaSuccess) e = cudaEventRecord(e1, st);
+            if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+            float ms = 0.f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+            if (rep > 0) tmin = std::min(tmin, ms);  // the first run warms up
+        }
+        if (e != cudaSuccess) break;
+        if (v + 1 < 16) ms_out[v + 1] = tmin;
+        if (tmin < best_ms) {
+            best_ms = tmin;
+            best = v;
+        }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    *best_out = best;
+    (void)dev;
+    return e;
+}
+
+// Points each qualifying level's x2 into `pool` (mg_tb_extra_floats floats),
+// picks its smoother — `forced` (a variant, or -1 for the plain half sweeps)
+// when >= -1, else the autotuner's choice — and builds its tensor maps and
+// z-chunk.
+cudaError_t mg_tb_setup(MGPlan &m, float *pool, int forced) {
+    for (int j = 0; j < kMaxLevels; j++) m.tb_var[j] = -1;
+    if (!pool) return cudaSuccess;
+    {
+        // Once the blocked smoother (up to ~200 KB of shared memory per CTA)
+        // has run, the SMs stay partitioned for shared memory unless a kernel
+        // asks otherwise; the plain stencil kernels read their neighbours
+        // through L1 and measured 11% slower at 128^3 in that state.  They
+        // ask for the largest L1.
+        static std::once_flag once;
+        static cudaError_t carve = cudaSuccess;
+        std::call_once(once, [] {
+            const void *k[] = {(const void *)rbsor_kernel, (const void *)resid_restrict_kernel,
+                               (const void *)prolong_kernel, (const void *)dc_residual_kernel,
+                               (const void *)dc_update_kernel};
+            for (const void *f : k)
+                if (carve == cudaSuccess)
+                    carve = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                                 cudaSharedmemCarveoutMaxL1);
+        });
+        PPPM_CUDA_TRY(carve);
+    }
+    int dev = 0, sms = 148;
+    PPPM_CUDA_TRY(cudaGetDevice(&dev));
+    PPPM_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const char *f = getenv("PPPM_MG_TB_FUSE");
+    m.tb_fuse_prolong = (f && *f == '1');
+    for (int j = 0; j < m.levels; j++) {
+        Level &L = m.lv[j];
+        if (!(L.d >= m.tb_min_edge && (L.d % 4) == 0)) continue;
+        L.x2 = pool;
+        pool += (size_t)m.comps * L.cells;
+    }
+    for (int j = 0; j < m.levels; j++) {
+        Level &L = m.lv[j];
+        if (!L.x2) continue;
+        int v = forced;
+        if (forced < -1) {
+            const TuneKey key{dev, (int)L.d, m.comps};
+            bool found = false;
+            {
+                std::lock_guard<std::mutex> lk(g_tune_mutex);
+                for (int q = 0; q < g_tune_count; q++)
+                    if (g_tune[q].key == key) { v = g_tune[q].variant; found = true; }
+            }
+            if (!found) {
+                TuneEntry te{};
+                te.key = key;
+                for (float &x : te.ms) x = -1.f;
+                PPPM_CUDA_TRY(tune_level(m, j, sms, dev, &te.variant, te.ms));
+                v = te.variant;
+                std::lock_guard<std::mutex> lk(g_tune_mutex);
+                if (g_tune_count < 64) g_tune[g_tune_count++] = te;
+            }
+        }
+        if (v < 0 || v >= tb_variant_count()) continue;
+        int per_sm = 1;
+        PPPM_CUDA_TRY(tb_prepare(v, &per_sm));
+        PPPM_CUDA_TRY(tb_make_map(&m.tb_maps[j].x, L.x, (int)L.d, m.comps, v));
+        PPPM_CUDA_TRY(tb_make_map(&m.tb_maps[j].x2, L.x2, (int)L.d, m.comps, v));
+        PPPM_CUDA_TRY(tb_make_map(&m.tb_maps[j].b, L.b, (int)L.d, m.comps, v));
+        m.tb_zchunk[j] = pick_zchunk((int)L.d, m.comps, v, sms, per_sm);
+        m.tb_var[j] = v;
+    }
+    return cudaSuccess;
+}
+
+// Text summary of the autotuner's measurements (one line per level edge).
+size_t mg_tune_report(char *buf, size_t cap) {
+    std::lock_guard<std::mutex> lk(g_tune_mutex);
+    size_t w = 0;
+    auto put = [&](const char *fmt, auto... args) {
+        if (w < cap) {
+            const int k = snprintf(buf + w, cap - w, fmt, args...);
+            if (k > 0) w += (size_t)k;
+        }
+    };
+    for (int q = 0; q < g_tune_count; q++) {
+        const TuneEntry &t = g_tune[q];
+        put("edge %d comps %d: chosen %d; ms per 8 half sweeps: plain %.4f", t.key.d, t.key.comps, t.variant,
+            (double)t.ms[0]);
+        for (int v = 0; v + 1 < 16 && v < tb_variant_count(); v++) {
+            int T = 0, TX = 0, TY = 0;
+            tb_variant_shape(v, &T, &TX, &TY);
+            put(", v%d(T%d %dx%d) %.4f", v, T, TX, TY, (double)t.ms[v + 1]);
+        }
+        put("\n");
+    }
+    return w < cap ? w : cap;
+}
+
+int mg_tb_default_variant() {
+    const char *e = getenv("PPPM_MG_TB");
+    if (e && *e) {
+        const int v = atoi(e);
+        return (v >= 0 && v < tb_variant_count()) ? v : -1;
+    }
+    return -2;  // autotune
+}
+
 static MGPlan scene_plan(pppm_scene *s) {
-    MGPlan m;
+    MGPlan m = s->mg_tb;  // blocked-smoother variant, maps, z-chunks, error flag
     m.levels = s->levels;
     for (int l = 0; l < s->levels; l++) m.lv[l] = s->lv[l];
     m.comps = 3;
@@ -475,17 +732,7 @@ cudaError_t prepare_multigrid_graph(pppm_scene *s) {
 }
 
 cudaError_t run_multigrid(pppm_scene *s) {
-    MGPlan m;
-    m.levels = s->levels;
-    for (int l = 0; l < s->levels; l++) m.lv[l] = s->lv[l];
-    m.comps = 3;
-    m.st = s->stream;
-    m.psi = s->psi;
-    m.b64 = nullptr;
-    m.vort = s->vort;
-    m.P = s->dparams;
-    m.norms = s->norms;
-    m.coarse_op = s->coarse_op;
+    MGPlan m = scene_plan(s);
     int cyc = 0;
     double rel = -1.0;
     if (s->prm.mg_mode == PPPM_MG_REFERENCE) {

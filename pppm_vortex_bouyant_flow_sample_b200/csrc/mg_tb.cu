@@ -6,7 +6,7 @@
 // (MG/MultiGrid_kernel.cu, mg_ProlongationPeriodic3D2).
 //
 // Each CTA owns an output tile of TX x TY cells in (x, y) and a chunk of z
-// planes.  It streams planes of x and b through a ring of T + 3 slots in
+// planes.  It streams planes of x and b through a ring of T + 2 + PF slots (PF planes loaded ahead) in
 // shared memory, each slot a (TX + 2H) x (TY + 2T) box loaded by one TMA
 // tensor copy (cp.async.bulk.tensor.4d, completion on an mbarrier; H = T
 // rounded up to 4 so that the box's x coordinate stays 16-byte aligned).  The
@@ -84,33 +84,38 @@ __device__ __forceinline__ float sor(float x, float nb, float b) {
 
 }  // namespace
 
-// Shared-memory bytes of one configuration (ring of x and b plus barriers).
-template <int T, int TX, int TY>
+// Shared-memory bytes of one configuration (ring of x, and of b unless BG,
+// plus barriers).  PF: planes loaded ahead of the one a step needs (copies in
+// flight).  BG: b is read from global memory where a cell is updated instead
+// of being staged (each b value is read once per pass either way).
+template <int T, int TX, int TY, int PF, bool BG>
 struct TbShape {
     static constexpr int H = (T + 3) / 4 * 4;  // x halo, a multiple of 4 floats
     static constexpr int BX = TX + 2 * H;
     static constexpr int BY = TY + 2 * T;
-    static constexpr int R = T + 3;
+    static constexpr int R = T + 2 + PF;
     static constexpr int PLANE = BX * BY;                    // floats per slot
     static constexpr uint32_t PLANE_BYTES = PLANE * 4u;
-    static constexpr size_t SMEM = 2ull * R * PLANE_BYTES + 8ull * R + 128;
+    static constexpr size_t SMEM = (BG ? 1ull : 2ull) * R * PLANE_BYTES + 8ull * R + 128;
     static_assert(PLANE_BYTES % 128 == 0, "slots must stay 128-byte aligned");
     static_assert(BX <= 256 && BY <= 256, "TMA box edge above 256");
     static_assert(T % 2 == 0, "whole red-black iterations only");
 };
 
-template <int T, int TX, int TY, int NT>
+template <int T, int TX, int TY, int NT, int PF, bool BG>
 __global__ void __launch_bounds__(NT)
 tb_smooth_kernel(const __grid_constant__ CUtensorMap map_x, const __grid_constant__ CUtensorMap map_b,
                  int load_x, const float *__restrict__ xc, float *__restrict__ x_out, int d, int zchunk,
-                 int zchunks, uint32_t *__restrict__ err) {
-    using S = TbShape<T, TX, TY>;
+                 int zchunks, uint32_t *__restrict__ err, const float *__restrict__ bg) {
+    using S = TbShape<T, TX, TY, PF, BG>;
     constexpr int H = S::H, BX = S::BX, BY = S::BY, R = S::R, PLANE = S::PLANE;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     float *ring_x = reinterpret_cast<float *>(smem_raw);
-    float *ring_b = ring_x + R * PLANE;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(ring_b + R * PLANE);
+    float *ring_b = ring_x + R * PLANE;  // (BG: no b ring)
+    uint64_t *bars = reinterpret_cast<uint64_t *>(ring_x + (BG ? 1 : 2) * R * PLANE);
+    const float *bgc = BG ? bg + (size_t)(blockIdx.z / zchunks) * d * d * d : nullptr;
     __shared__ int s_abort;
+    __shared__ uint32_t s_issued[R];  // loads issued per slot (thread 0)
 
     const int tid = threadIdx.x;
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
@@ -123,19 +128,34 @@ tb_smooth_kernel(const __grid_constant__ CUtensorMap map_x, const __grid_constan
     float *xo = x_out + (size_t)comp * cells;
 
     if (tid == 0) {
-        for (int r = 0; r < R; r++) mbar_init(&bars[r], 1);
+        for (int r = 0; r < R; r++) {
+            mbar_init(&bars[r], 1);
+            s_issued[r] = 0;
+        }
         s_abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
 
-    const uint32_t tx_bytes = (load_x ? 2u : 1u) * S::PLANE_BYTES;
+    // this thread's (row, pair) slots of the box, the same for every half sweep
+    constexpr int PAIRS = BX / 2;
+    constexpr int ITEMS = (BY * PAIRS + NT - 1) / NT;
+    int it_sy[ITEMS], it_px[ITEMS];
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+        const int q = tid + i * NT;
+        it_sy[i] = (q < BY * PAIRS) ? q / PAIRS : -1;
+        it_px[i] = q % PAIRS;
+    }
+
+    const uint32_t tx_bytes = ((load_x ? 1u : 0u) + (BG ? 0u : 1u)) * S::PLANE_BYTES;
     auto slot_of = [&](int p) { return (p - p_first) % R; };
     auto issue = [&](int p) {  // thread 0 only
         const int sl = slot_of(p);
+        s_issued[sl]++;
         mbar_expect_tx(&bars[sl], tx_bytes);
         if (load_x) tma_load_4d(ring_x + sl * PLANE, &map_x, x0 - H, y0 - T, p, comp, &bars[sl]);
-        tma_load_4d(ring_b + sl * PLANE, &map_b, x0 - H, y0 - T, p, comp, &bars[sl]);
+        if (!BG) tma_load_4d(ring_b + sl * PLANE, &map_b, x0 - H, y0 - T, p, comp, &bars[sl]);
     };
     // Waits for plane p, then applies the start value: x as loaded, zero
     // (load_x = 0), plus the injected coarse correction xc[parent] (xc set);
@@ -164,23 +184,23 @@ tb_smooth_kernel(const __grid_constant__ CUtensorMap map_x, const __grid_constan
         return true;
     };
 
+    const bool prep = !(load_x && !xcc);  // the start value is written by the threads
     if (tid == 0) {
-        for (int p = p_first; p <= min(p_first + 2, p_last); p++) issue(p);
+        for (int p = p_first; p <= min(p_first + 1 + PF, p_last); p++) issue(p);
     }
     wait_prep(p_first);
     wait_prep(p_first + 1);
+    fence_proxy_async();
+    __syncthreads();
 
     const int s_begin = zc0 - T + 1, s_end = zc1 + T - 2;
     for (int s = s_begin; s <= s_end; s++) {
-        // every thread's generic accesses to the slot about to be refilled are
-        // done and ordered before the asynchronous copy into it
-        fence_proxy_async();
-        __syncthreads();
-        if (s_abort) break;
-        if (tid == 0 && s + 2 <= p_last) issue(s + 2);
+        // The slot refilled now held plane s - T - 1, whose last reads and
+        // writes (half sweep T of the step before) every thread ordered before
+        // the asynchronous proxy (fence) and the barrier that closed that step.
+        if (tid == 0 && s + 1 + PF <= p_last) issue(s + 1 + PF);
         wait_prep(s + 1);
-        __syncthreads();
-        if (s_abort) break;
+        if (prep) __syncthreads();
 #pragma unroll
         for (int t = 1; t <= T; t++) {
             const int p = s - t + 1;
@@ -189,24 +209,28 @@ tb_smooth_kernel(const __grid_constant__ CUtensorMap map_x, const __grid_constan
                 float *X = ring_x + slot_of(p) * PLANE;
                 const float *Xm = ring_x + slot_of(p - 1) * PLANE;
                 const float *Xp = ring_x + slot_of(p + 1) * PLANE;
-                const float *B = ring_b + slot_of(p) * PLANE;
+                const float *B = BG ? nullptr : ring_b + slot_of(p) * PLANE;
+                const float *Bg = BG ? bgc + (size_t)p * d * d : nullptr;
                 const int ya = max(0, y0 - T + t), yb = min(d, y0 + TY + T - t);
                 const int xa = max(0, x0 - T + t), xb = min(d, x0 + TX + T - t);
-                constexpr int PAIRS = BX / 2;
-                for (int q = tid; q < BY * PAIRS; q += NT) {
-                    const int sy = q / PAIRS;
+#pragma unroll
+                for (int i = 0; i < ITEMS; i++) {
+                    const int sy = it_sy[i];
                     const int gy = y0 - T + sy;
                     // box x origin x0 - H is even, so box and grid parities agree
-                    const int sx = 2 * (q % PAIRS) + ((c - gy - p) & 1);
+                    const int sx = 2 * it_px[i] + ((c - gy - p) & 1);
                     const int gx = x0 - H + sx;
-                    if (gy < ya || gy >= yb || gx < xa || gx >= xb) continue;
+                    if (sy < 0 || gy < ya || gy >= yb || gx < xa || gx >= xb) continue;
                     const int o = sy * BX + sx;
                     const float nb = ((X[o - 1] + X[o + 1]) + (X[o + BX] + X[o - BX])) + (Xm[o] + Xp[o]);
-                    X[o] = sor(X[o], nb, B[o]);
+                    X[o] = sor(X[o], nb, BG ? __ldg(Bg + (size_t)gy * d + gx) : B[o]);
                 }
             }
+            if (t == T) fence_proxy_async();
             __syncthreads();
+            if (t == 1 && s_abort) break;
         }
+        if (s_abort) break;
         const int p = s - T + 1;
         if (p >= zc0 && p < zc1) {
             // 128-bit stores of the final TX x TY interior (x0, d multiples of 4)
@@ -223,10 +247,13 @@ tb_smooth_kernel(const __grid_constant__ CUtensorMap map_x, const __grid_constan
         }
     }
     if (s_abort && tid == 0) {
-        // let copies still in flight land before the CTA's shared memory goes away
+        // let copies still in flight land before the CTA's shared memory goes
+        // away: the last phase of every slot that was loaded, bounded again
         for (int r = 0; r < R; r++) {
+            if (!s_issued[r]) continue;
+            const uint32_t parity = (s_issued[r] - 1u) & 1u;
             uint32_t it = 0;
-            while (!mbar_try_wait(&bars[r], 0) && !mbar_try_wait(&bars[r], 1) && ++it < kWaitLimit) {
+            while (!mbar_try_wait(&bars[r], parity) && ++it < kWaitLimit) {
             }
         }
     }
@@ -250,22 +277,27 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 // The configurations built; TbConfig::variant indexes this table.
 struct TbVariant {
-    int T, TX, TY, NT;
+    int T, TX, TY, NT, PF;
+    bool BG;
     size_t smem;
     const void *kernel;
 };
 
-template <int T, int TX, int TY, int NT>
+template <int T, int TX, int TY, int NT, int PF, bool BG>
 TbVariant make_variant() {
-    return TbVariant{T, TX, TY, NT, TbShape<T, TX, TY>::SMEM, (const void *)tb_smooth_kernel<T, TX, TY, NT>};
+    return TbVariant{T, TX, TY, NT, PF, BG, TbShape<T, TX, TY, PF, BG>::SMEM,
+                     (const void *)tb_smooth_kernel<T, TX, TY, NT, PF, BG>};
 }
 
 const TbVariant *variants(int *count) {
+    // Measured on B200 (256^3, three components, 8 half sweeps): 0.89 ms
+    // (T2 64x16), 0.81 ms (T2 128x32), 0.94 ms for the plain half sweeps;
+    // staging b through the ring beat reading it from global memory, and T = 4
+    // lost to its larger halo.
     static const TbVariant v[] = {
-        make_variant<2, 64, 16, 256>(),
-        make_variant<4, 64, 16, 256>(),
-        make_variant<8, 32, 16, 256>(),
-        make_variant<4, 32, 16, 256>(),
+        make_variant<2, 64, 16, 384, 4, false>(),
+        make_variant<2, 128, 32, 1024, 1, false>(),
+        make_variant<4, 64, 16, 384, 4, false>(),
     };
     *count = (int)(sizeof(v) / sizeof(v[0]));
     return v;
@@ -306,22 +338,28 @@ cudaError_t tb_make_map(CUtensorMap *map, float *base, int d, int comps, int var
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
+// Opts the variant's kernel into its dynamic shared memory (once, at set-up,
+// outside any stream capture) and returns how many of its CTAs fit on an SM.
+cudaError_t tb_prepare(int variant, int *blocks_per_sm) {
+    int c = 0;
+    const TbVariant &w = variants(&c)[variant];
+    PPPM_CUDA_TRY(cudaFuncSetAttribute(w.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w.smem));
+    PPPM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, w.kernel, w.NT, w.smem));
+    return cudaSuccess;
+}
+
 // One pass of T half sweeps over a level: x_out = S^T(x_in [+ P xc], b).
 // map_x describes x_in (ignored when load_x = 0, start from zero); xc is the
 // coarser level's x for a fused prolongation, or null.
-cudaError_t tb_smooth(int variant, const CUtensorMap &map_x, const CUtensorMap &map_b, int load_x, const float *xc,
-                      float *x_out, int d, int comps, int zchunk, uint32_t *err, cudaStream_t st) {
+cudaError_t tb_smooth(int variant, const CUtensorMap &map_x, const CUtensorMap &map_b, const float *b_dev, int load_x,
+                      const float *xc, float *x_out, int d, int comps, int zchunk, uint32_t *err, cudaStream_t st) {
     int c = 0;
     const TbVariant &w = variants(&c)[variant];
-    static bool attr_done[16] = {};
-    if (!attr_done[variant]) {
-        PPPM_CUDA_TRY(cudaFuncSetAttribute(w.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w.smem));
-        attr_done[variant] = true;
-    }
     const int zchunks = (d + zchunk - 1) / zchunk;
     const dim3 grid((d + w.TX - 1) / w.TX, (d + w.TY - 1) / w.TY, comps * zchunks);
+    const float *bg = b_dev;
     void *args[] = {(void *)&map_x, (void *)&map_b, &load_x, (void *)&xc, &x_out, &d, &zchunk, (void *)&zchunks,
-                    &err};
+                    &err, (void *)&bg};
     ::pppm::note_launch();
     return cudaLaunchKernel(w.kernel, grid, dim3(w.NT), args, w.smem, st);
 }

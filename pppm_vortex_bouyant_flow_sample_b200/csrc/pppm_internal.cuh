@@ -12,6 +12,7 @@
 //     FP64 [3][C].
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -62,12 +63,36 @@ struct Level {
     uint32_t cells;   // d^3
     float *x;         // [comps][cells]
     float *b;         // [comps][cells]
+    float *x2 = nullptr;  // [comps][cells] second copy of x for the blocked smoother (its levels only)
+};
+
+// Temporally blocked smoother (mg_tb.cu): T half sweeps per pass over a level.
+constexpr uint32_t kTbErrTimeout = 0x7B000001u;  // an mbarrier wait ran out
+int tb_variant_count();
+void tb_variant_shape(int variant, int *T, int *TX, int *TY);
+cudaError_t tb_make_map(CUtensorMap *map, float *base, int d, int comps, int variant);
+cudaError_t tb_prepare(int variant, int *blocks_per_sm);
+cudaError_t tb_smooth(int variant, const CUtensorMap &map_x, const CUtensorMap &map_b, const float *b_dev, int load_x,
+                      const float *xc, float *x_out, int d, int comps, int zchunk, uint32_t *err, cudaStream_t st);
+
+// Tensor maps of one level for the blocked smoother.
+struct TbMaps {
+    CUtensorMap x, x2, b;
 };
 
 // Everything one multigrid solve touches; comps independent right-hand sides.
 struct MGPlan {
     int levels = 0;
     Level lv[kMaxLevels];
+    // blocked smoother per level: its variant (-1 = plain half sweeps), tensor
+    // maps and z-chunk length (levels with edge >= tb_min_edge, x2 allocated),
+    // and the device error flag
+    int tb_var[kMaxLevels] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1};
+    uint32_t tb_min_edge = 256;  // smaller levels measured faster with the plain half sweeps
+    bool tb_fuse_prolong = false;  // prolongation inside the first post-smoothing pass
+    TbMaps tb_maps[kMaxLevels];
+    int tb_zchunk[kMaxLevels] = {};
+    uint32_t *err = nullptr;
     int comps = 3;
     cudaStream_t st = nullptr;
     double *psi = nullptr;          // [comps][C0] FP64 solution
@@ -141,6 +166,9 @@ struct pppm_scene {
     double *coarse_op = nullptr;          // coarsest-level operator (levels >= 2)
     cudaGraphExec_t mg_graph = nullptr;   // reference-schedule solve, captured once
     unsigned mg_graph_kernels = 0;
+    float *mg_x2_pool = nullptr;          // second x copies of the blocked-smoother levels
+    uint32_t *mg_err = nullptr;           // device error flag of the blocked smoother
+    pppm::MGPlan mg_tb;                   // its variant, tensor maps and z-chunks (lv[].x2 in lv)
 
     // evaluation side
     uint32_t *ekey[2] = {nullptr, nullptr};
@@ -226,11 +254,20 @@ cudaError_t launch_move3(pppm_scene *s, float4 *pos, const double *u, const doub
 cudaError_t mg_solve(const MGPlan &m, int mode, double tol, int max_cycles, int *cycles_out,
                      double *relres_out);
 cudaError_t mg_vcycle_update(const MGPlan &m, double *x64);
+// Second x copy per level for the blocked smoother: bytes to allocate (all of
+// a plan's levels that qualify), then tensor maps and z-chunks over them.
+size_t mg_tb_extra_floats(const MGPlan &m);
+cudaError_t mg_tb_setup(MGPlan &m, float *pool, int forced);
+size_t mg_tune_report(char *buf, size_t cap);
 
 cudaError_t radix_sort_pairs(cudaStream_t st, uint32_t N, uint32_t bits, uint32_t *key[2], uint32_t *idx[2],
                              uint32_t *hist, uint32_t **sorted_key, uint32_t **sorted_idx);
 
 int mg_level_count(uint32_t n);
+// Blocked-smoother choice for new multigrid objects: PPPM_MG_TB in the
+// environment (a variant index, or -1 for the plain half sweeps), else -2:
+// the autotuner picks per level.
+int mg_tb_default_variant();
 bool mg_shape_ok(uint32_t n);
 uint32_t key_bits(uint32_t n);
 size_t radix_hist_entries(uint32_t N);
