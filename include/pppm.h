@@ -254,10 +254,16 @@ pppm_status pppm_tuning_report(char *buf, size_t cap, size_t *written);
 /* ---- several independent scenes in one call -----------------------------
  * No reference counterpart (the reference drives one solver from one host
  * thread).  Each item is one scene's set_vortices + build_far_field + eval
- * (M = 0 skips the eval).  Every item runs on its own stream from a pool the
- * library keeps per device, ordered after the caller's earlier work on
- * `stream`; `stream` then waits for all items.  A scene may appear once per
- * batch.  Each scene's result is the one it gets alone. */
+ * (M = 0 skips the eval).  The builds and the evaluation points' sorts run on
+ * a set of streams the call borrows (longest predicted build first, each onto
+ * the least loaded stream), ordered after the caller's earlier work on
+ * `stream`; then all items' evaluations run as one launch on `stream` over a
+ * work list of (scene, block of 128 points), the scenes with the most
+ * particles per cell first (one launch per group of items that differ in
+ * smoothing series or segment mode).  `stream` has all the batch's work when
+ * the call returns.  A scene may appear once per batch.  Each scene's result
+ * is bit for bit the one it gets alone.  Concurrent calls from several
+ * threads borrow different stream sets and overlap on the device. */
 typedef struct pppm_batch_item {
     pppm_scene *scene;
     uint32_t N;

@@ -315,6 +315,32 @@ pppm_status eval_common(pppm_scene *s, uint32_t M, const float *ea, const float 
 
 }  // namespace
 
+// The first half of an evaluation for the batched path (pppm_batch_run):
+// the checks and buffer growth of pppm_eval, then the points' sort; the
+// evaluation itself runs later in one launch with the batch's other scenes.
+pppm_status pppm_eval_batch_prepare(pppm_scene *s, uint32_t M, const float *ea, const float *eb, int is_segment,
+                                    double *u, double *v, double *w, pppm::EvalArgs *args, pppm::EvalMode *mode) {
+    if (!s) { snprintf(g_err, sizeof(g_err), "pppm_eval: scene is NULL"); return PPPM_ERR_INVALID; }
+    if (!s->far_ready) {
+        snprintf(g_err, sizeof(g_err), "pppm_eval: call pppm_build_far_field after pppm_set_vortices first");
+        return PPPM_ERR_STATE;
+    }
+    if (M == 0) return PPPM_OK;
+    if (!ea || (is_segment == 1 && !eb) || !u || !v || !w) {
+        snprintf(g_err, sizeof(g_err), "pppm_eval: NULL pointer argument");
+        return PPPM_ERR_INVALID;
+    }
+    if (M > s->capM) {
+        cudaError_t e = alloc_eval_side(s, M);
+        if (e != cudaSuccess) return cuda_fail("pppm_eval (grow eval buffers)", e);
+    }
+    s->M = M;
+    cudaError_t e = pppm::eval_batch_prepare(s, reinterpret_cast<const float4 *>(ea), reinterpret_cast<const float4 *>(eb),
+                                             is_segment, M, u, v, w, args, mode);
+    if (e != cudaSuccess) return cuda_fail("pppm_eval", e);
+    return PPPM_OK;
+}
+
 extern "C" __attribute__((visibility("hidden"))) void pppm_set_error(const char *fmt, ...) {
     va_list ap;
     va_start(ap, fmt);

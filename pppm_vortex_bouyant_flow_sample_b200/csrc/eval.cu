@@ -25,6 +25,7 @@
 // error 2e-7, below that of the exp form near t = 0.25) and (1 - exp(-t)) / t
 // above t = 2.  No cancellation in either polynomial.
 #include <climits>
+#include <cstring>
 #include <cmath>
 #include <type_traits>
 #include <utility>
@@ -42,12 +43,15 @@ __device__ __forceinline__ float3 rel_pos(float4 p, const DevParams *__restrict_
                        (float)((double)p.z - P->origin[2]));
 }
 
-// Evaluation order: NGP cell * 8 + Gray rank of the point's octant inside its
-// cell (points outside the grid last).  A warp of consecutive points then shares
-// one cell octant, whose near-field boxes span 2K+2 cells per axis instead of
-// the reference's 2K+3.  The order is internal: results return in caller order.
+// Evaluation order: NGP cell, then the Gray rank of the point's octant inside
+// the cell, then (fine = 1) the Gray rank of its quarter-cell inside the
+// octant (points outside the grid last).  A warp of consecutive points then
+// covers about a quarter of a cell, so the union of its lanes' near-field
+// boxes, over which it walks, exceeds each lane's own box by little and few
+// staged candidates fail the lane's box test.  The order is internal: results
+// return in caller order.
 __global__ void eval_keys_kernel(const float4 *__restrict__ eval_a, uint32_t M, const DevParams *__restrict__ P,
-                                 uint32_t *__restrict__ key, uint32_t *__restrict__ idx) {
+                                 int fine, uint32_t *__restrict__ key, uint32_t *__restrict__ idx) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= M) return;
     const float3 r = rel_pos(eval_a[t], P);
@@ -56,14 +60,24 @@ __global__ void eval_keys_kernel(const float4 *__restrict__ eval_a, uint32_t M, 
     const double qx = (double)r.x * invh, qy = (double)r.y * invh, qz = (double)r.z * invh;
     const double fx = floor(qx), fy = floor(qy), fz = floor(qz);
     const double dn = (double)n;
-    uint32_t k = 8u * n * n * n;
+    const int sh = fine ? 6 : 3;
+    uint32_t k = (n * n * n) << sh;
     if (fx >= 0.0 && fx < dn && fy >= 0.0 && fy < dn && fz >= 0.0 && fz < dn) {
-        const uint32_t oct = (qx - fx >= 0.5 ? 1u : 0u) | (qy - fy >= 0.5 ? 2u : 0u) | (qz - fz >= 0.5 ? 4u : 0u);
-        // octants in Gray-code order (0,1,3,2,6,7,5,4): neighbouring groups differ
-        // along one axis, so a warp spanning two groups widens its walk by one
-        // half-cell on one axis only
+        // quarter-cell coordinates 0..3 per axis (clamped against rounding)
+        const uint32_t ux = min(3u, (uint32_t)(4.0 * (qx - fx))), uy = min(3u, (uint32_t)(4.0 * (qy - fy))),
+                       uz = min(3u, (uint32_t)(4.0 * (qz - fz)));
+        const uint32_t oct = (ux >> 1) | ((uy >> 1) << 1) | ((uz >> 1) << 2);
+        // groups in Gray-code order (0,1,3,2,6,7,5,4): neighbouring groups differ
+        // along one axis, so a warp spanning two groups widens its walk on one
+        // axis only
         const uint32_t rank = (0x54672310u >> (4 * oct)) & 7u;
-        k = ((((uint32_t)fz * n + (uint32_t)fy) * n + (uint32_t)fx) << 3) | rank;
+        const uint32_t cell = ((uint32_t)fz * n + (uint32_t)fy) * n + (uint32_t)fx;
+        if (fine) {
+            const uint32_t sub = (ux & 1u) | ((uy & 1u) << 1) | ((uz & 1u) << 2);
+            k = (cell << 6) | (rank << 3) | ((0x54672310u >> (4 * sub)) & 7u);
+        } else {
+            k = (cell << 3) | rank;
+        }
     }
     key[t] = k;
     idx[t] = t;
@@ -339,18 +353,32 @@ struct SmoothSeries {
     float t7;      // 2 in the packed polynomials' variable: where the exp form takes over
 };
 
+// One block of evaluation points (kEvalThreads consecutive points in the
+// evaluation order) of one scene.
 template <bool SEG, bool COUNT, bool FOLD>
-__global__ void __launch_bounds__(kEvalThreads, 8) eval_kernel(const SmoothSeries sc, const uint32_t *__restrict__ eidx, uint32_t M, const float4 *__restrict__ eval_a,
-            const float4 *__restrict__ eval_b, const float *__restrict__ far,
-            const uint32_t *__restrict__ start, const uint32_t *__restrict__ end,
-            const uint32_t *__restrict__ sub_start, const uint32_t *__restrict__ sub_end, const float4 *__restrict__ vrec,
-            const float4 *__restrict__ valf, const DevParams *__restrict__ P, int n, int K,
-            double *__restrict__ u, double *__restrict__ v, double *__restrict__ w, float *__restrict__ uf,
-            unsigned long long *__restrict__ pair_count) {
-    __shared__ float4 stage[(kEvalThreads / 32) * kPackPlanes * kPackSlots];
+__device__ __forceinline__ void eval_points(const SmoothSeries &sc, const EvalArgs &ea, uint32_t block,
+                                            float4 *__restrict__ stage) {
+    const uint32_t *__restrict__ eidx = ea.eidx;
+    const uint32_t M = ea.M;
+    const float4 *__restrict__ eval_a = ea.eval_a;
+    const float4 *__restrict__ eval_b = ea.eval_b;
+    const float *__restrict__ far = ea.far;
+    const uint32_t *__restrict__ start = ea.start;
+    const uint32_t *__restrict__ end = ea.end;
+    const uint32_t *__restrict__ sub_start = ea.sub_start;
+    const uint32_t *__restrict__ sub_end = ea.sub_end;
+    const float4 *__restrict__ vrec = ea.vrec;
+    const float4 *__restrict__ valf = ea.valf;
+    const DevParams *__restrict__ P = ea.P;
+    const int n = ea.n, K = ea.K;
+    double *__restrict__ u = ea.u;
+    double *__restrict__ v = ea.v;
+    double *__restrict__ w = ea.w;
+    float *__restrict__ uf = ea.uf;
+    unsigned long long *__restrict__ pair_count = ea.pair_count;
     const int lane = threadIdx.x & 31;
     float4 *pk = stage + (threadIdx.x >> 5) * (kPackPlanes * kPackSlots);
-    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t s = block * blockDim.x + threadIdx.x;
     const bool act = s < M;
     const uint32_t q = act ? eidx[s] : 0u;
     float3 ra = make_float3(0.f, 0.f, 0.f), rb = make_float3(0.f, 0.f, 0.f);
@@ -547,6 +575,29 @@ __global__ void __launch_bounds__(kEvalThreads, 8) eval_kernel(const SmoothSerie
     }
 }
 
+// One scene: block b evaluates points [128 b, 128 b + 128) of the order.
+template <bool SEG, bool COUNT, bool FOLD>
+__global__ void __launch_bounds__(kEvalThreads, 8) eval_kernel(const SmoothSeries sc, const EvalArgs ea) {
+    __shared__ float4 stage[(kEvalThreads / 32) * kPackPlanes * kPackSlots];
+    eval_points<SEG, COUNT, FOLD>(sc, ea, blockIdx.x, stage);
+}
+
+// Several scenes in one launch: block b takes work item work[b] = (scene,
+// block of that scene).  The host orders the list so that the blocks of the
+// scenes with the most pairs per point come first, which the block scheduler
+// then hands out first (longest work first); each point's arithmetic is the
+// one-scene kernel's, so results do not depend on the batch.
+template <bool SEG, bool COUNT, bool FOLD>
+__global__ void __launch_bounds__(kEvalThreads, 8)
+eval_batch_kernel(const SmoothSeries sc, const EvalArgs *__restrict__ scenes, const uint2 *__restrict__ work) {
+    __shared__ float4 stage[(kEvalThreads / 32) * kPackPlanes * kPackSlots];
+    __shared__ EvalArgs sa;  // the block's scene, read from shared memory where used
+    const uint2 it = work[blockIdx.x];
+    if (threadIdx.x == 0) sa = scenes[it.x];
+    __syncthreads();
+    eval_points<SEG, COUNT, FOLD>(sc, sa, it.y, stage);
+}
+
 // Monomial coefficients of the degree-deg polynomial that interpolates
 // phi(t) = (1 - e^-t) / t at the deg + 1 Chebyshev nodes of [0, T] (a near-best
 // uniform approximation: relative error 2.6e-9 for degree 4 on [0, 0.25],
@@ -577,70 +628,106 @@ void phi_chebyshev(int deg, double T, double *c) {
 
 }  // namespace
 
-cudaError_t launch_eval(pppm_scene *s, const float4 *eval_a, const float4 *eval_b, int is_segment, uint32_t M,
-                        double *u, double *v, double *w, float *uf, int count_pairs) {
+// Evaluation keys of M points and their radix sort (the order the eval
+// kernel walks); the sorted original indices land in s->esorted_idx.
+cudaError_t launch_eval_sort(pppm_scene *s, const float4 *eval_a, uint32_t M) {
     uint32_t *skey = nullptr, *sidx = nullptr;
     prof_begin(s, kStageEvalSort);
     ::pppm::note_launch();
-    eval_keys_kernel<<<(M + 255) / 256, 256, 0, s->stream>>>(eval_a, M, s->dparams, s->ekey[0], s->eidx[0]);
+    // quarter-cell order while the key fits 32 bits (n <= 256), else octants
+    const int fine = (64ull * s->C < (1ull << 32)) ? 1 : 0;
+    eval_keys_kernel<<<(M + 255) / 256, 256, 0, s->stream>>>(eval_a, M, s->dparams, fine, s->ekey[0], s->eidx[0]);
     PPPM_CUDA_TRY(cudaGetLastError());
     uint32_t bits = 1;
-    while (bits < 32 && (1ull << bits) <= 8ull * s->C) bits++;
+    while (bits < 32 && (1ull << bits) <= (fine ? 64ull : 8ull) * s->C) bits++;
     PPPM_CUDA_TRY(radix_sort_pairs(s->stream, M, bits, s->ekey, s->eidx, s->hist, &skey, &sidx));
     prof_end(s, kStageEvalSort);
     s->esorted_idx = sidx;
+    return cudaSuccess;
+}
+
+// The smoothing series of a scene and whether its coefficients are folded.
+// With an absolute a (known here) the packed polynomials are in r^3
+// (c_q / a^(3q), scaled by 1/(4 pi a^3)) while every coefficient stays a
+// normal float far from overflow.  Otherwise (a tied to the cell size of the
+// build, known only on the device, or extreme a) they are in t = (r/a)^3 with
+// unit scale, and the kernel applies 1/(4 pi a^3) from the device parameters
+// once per point.
+static bool make_series(const pppm_scene *s, SmoothSeries &sc) {
+    memset(&sc, 0, sizeof(sc));
+    bool fold = s->prm.a_cells <= 0.0;
+    double f4[5], f7[8], f5[6];
+    phi_chebyshev(4, 0.25, f4);
+    phi_chebyshev(7, 2.0, f7);
+    phi_chebyshev(5, 0.5, f5);
+    for (int q = 0; q < 6; q++) sc.p5[q] = make_float2((float)f5[q], (float)f5[q]);
+    double u4[5], u7[8], k = 1.0;
+    if (fold) {
+        const double a = s->prm.a;
+        k = 1.0 / (kFourPi * a * a * a);
+        const double ia3 = 1.0 / (a * a * a);
+        double pw = 1.0;
+        for (int q = 0; q < 8; q++, pw *= ia3) {
+            if (q < 5) u4[q] = k * f4[q] * pw;
+            u7[q] = k * f7[q] * pw;
+            for (double x : {q < 5 ? u4[q] : 1.0, u7[q]})
+                if (!(std::fabs(x) <= 1e30 && std::fabs(x) >= 1e-30)) fold = false;
+        }
+    }
+    if (!fold) k = 1.0;
+    for (int q = 0; q < 8; q++) {
+        if (q < 5) {
+            sc.c[q] = (float)(k * f4[q]);
+            const float v4 = fold ? (float)u4[q] : sc.c[q];
+            sc.p4[q] = make_float2(v4, v4);
+        }
+        const float v7 = fold ? (float)u7[q] : (float)(k * f7[q]);
+        sc.p7[q] = make_float2(v7, v7);
+    }
+    sc.t7 = fold ? (float)(2.0 * s->prm.a * s->prm.a * s->prm.a) : 2.0f;
+    return fold;
+}
+
+static EvalArgs make_args(pppm_scene *s, const float4 *eval_a, const float4 *eval_b, uint32_t M, double *u, double *v,
+                          double *w, float *uf, unsigned long long *pc) {
+    EvalArgs a;
+    a.eidx = s->esorted_idx;
+    a.M = M;
+    a.eval_a = eval_a;
+    a.eval_b = eval_b;
+    a.far = s->far;
+    a.start = s->cell_start;
+    a.end = s->cell_end;
+    a.sub_start = s->sub_start;
+    a.sub_end = s->sub_end;
+    a.vrec = s->vrec;
+    a.valf = s->valf;
+    a.P = s->dparams;
+    a.n = (int)s->n;
+    a.K = s->prm.K;
+    a.u = u;
+    a.v = v;
+    a.w = w;
+    a.uf = uf;
+    a.pair_count = pc;
+    return a;
+}
+
+cudaError_t launch_eval(pppm_scene *s, const float4 *eval_a, const float4 *eval_b, int is_segment, uint32_t M,
+                        double *u, double *v, double *w, float *uf, int count_pairs) {
+    PPPM_CUDA_TRY(launch_eval_sort(s, eval_a, M));
     if (count_pairs) PPPM_CUDA_TRY(cudaMemsetAsync(s->pair_count, 0, sizeof(unsigned long long), s->stream));
     prof_begin(s, kStageEval);
     ::pppm::note_launch();
     const bool seg = (is_segment == 1) && (eval_b != eval_a);
     const unsigned grid = (M + kEvalThreads - 1) / kEvalThreads;
-    unsigned long long *pc = count_pairs ? s->pair_count : nullptr;
     SmoothSeries sc;
-    // With an absolute a (known here) the packed polynomials are in r^3
-    // (c_q / a^(3q), scaled by 1/(4 pi a^3)) while every coefficient stays a
-    // normal float far from overflow.  Otherwise (a tied to the cell size of
-    // the build, known only on the device, or extreme a) they are in
-    // t = (r/a)^3 with unit scale, and the kernel applies 1/(4 pi a^3) from
-    // the device parameters once per point.
-    bool fold = s->prm.a_cells <= 0.0;
-    {
-        double f4[5], f7[8], f5[6];
-        phi_chebyshev(4, 0.25, f4);
-        phi_chebyshev(7, 2.0, f7);
-        phi_chebyshev(5, 0.5, f5);
-        for (int q = 0; q < 6; q++) sc.p5[q] = make_float2((float)f5[q], (float)f5[q]);
-        double u4[5], u7[8], k = 1.0;
-        if (fold) {
-            const double a = s->prm.a;
-            k = 1.0 / (kFourPi * a * a * a);
-            const double ia3 = 1.0 / (a * a * a);
-            double pw = 1.0;
-            for (int q = 0; q < 8; q++, pw *= ia3) {
-                if (q < 5) u4[q] = k * f4[q] * pw;
-                u7[q] = k * f7[q] * pw;
-                for (double x : {q < 5 ? u4[q] : 1.0, u7[q]})
-                    if (!(std::fabs(x) <= 1e30 && std::fabs(x) >= 1e-30)) fold = false;
-            }
-        }
-        if (!fold) k = 1.0;
-        for (int q = 0; q < 8; q++) {
-            if (q < 5) {
-                sc.c[q] = (float)(k * f4[q]);
-                const float v4 = fold ? (float)u4[q] : sc.c[q];
-                sc.p4[q] = make_float2(v4, v4);
-            }
-            const float v7 = fold ? (float)u7[q] : (float)(k * f7[q]);
-            sc.p7[q] = make_float2(v7, v7);
-        }
-        sc.t7 = fold ? (float)(2.0 * s->prm.a * s->prm.a * s->prm.a) : 2.0f;
-    }
-#define PPPM_EVAL_ARGS sc, sidx, M, eval_a, eval_b, s->far, s->cell_start, s->cell_end, s->sub_start, s->sub_end, \
-                       s->vrec, s->valf, s->dparams, \
-                       (int)s->n, s->prm.K, u, v, w, uf, pc
+    const bool fold = make_series(s, sc);
+    const EvalArgs ea = make_args(s, eval_a, eval_b, M, u, v, w, uf, count_pairs ? s->pair_count : nullptr);
 #define PPPM_EVAL_LAUNCH(SEG_, COUNT_)                                                              \
     do {                                                                                              \
-        if (fold) eval_kernel<SEG_, COUNT_, true><<<grid, kEvalThreads, 0, s->stream>>>(PPPM_EVAL_ARGS); \
-        else eval_kernel<SEG_, COUNT_, false><<<grid, kEvalThreads, 0, s->stream>>>(PPPM_EVAL_ARGS);    \
+        if (fold) eval_kernel<SEG_, COUNT_, true><<<grid, kEvalThreads, 0, s->stream>>>(sc, ea);      \
+        else eval_kernel<SEG_, COUNT_, false><<<grid, kEvalThreads, 0, s->stream>>>(sc, ea);         \
     } while (0)
     if (seg) {
         if (count_pairs) PPPM_EVAL_LAUNCH(true, true);
@@ -650,8 +737,40 @@ cudaError_t launch_eval(pppm_scene *s, const float4 *eval_a, const float4 *eval_
         else PPPM_EVAL_LAUNCH(false, false);
     }
 #undef PPPM_EVAL_LAUNCH
-#undef PPPM_EVAL_ARGS
     prof_end(s, kStageEval);
+    return cudaGetLastError();
+}
+
+// Batched evaluation (pppm_batch_run): the arguments of each item's scene
+// after its sort, and whether all items can share one launch (the same
+// series, segment mode and folding).
+cudaError_t eval_batch_prepare(pppm_scene *s, const float4 *eval_a, const float4 *eval_b, int is_segment, uint32_t M,
+                               double *u, double *v, double *w, EvalArgs *args, EvalMode *mode) {
+    PPPM_CUDA_TRY(launch_eval_sort(s, eval_a, M));
+    SmoothSeries sc;
+    mode->fold = make_series(s, sc);
+    static_assert(sizeof(SmoothSeries) <= sizeof(mode->series), "series bytes");
+    memcpy(mode->series, &sc, sizeof(sc));
+    mode->seg = (is_segment == 1) && (eval_b != eval_a);
+    *args = make_args(s, eval_a, eval_b, M, u, v, w, nullptr, nullptr);
+    return cudaSuccess;
+}
+
+// One launch over a device work list of `blocks` (scene, block) items for
+// scenes that share `mode`.
+cudaError_t launch_eval_batch(const EvalMode &mode, const EvalArgs *args_dev, const uint2 *work_dev, uint32_t blocks,
+                              cudaStream_t st) {
+    if (!blocks) return cudaSuccess;
+    SmoothSeries sc;
+    memcpy(&sc, mode.series, sizeof(sc));
+    ::pppm::note_launch();
+    if (mode.seg) {
+        if (mode.fold) eval_batch_kernel<true, false, true><<<blocks, kEvalThreads, 0, st>>>(sc, args_dev, work_dev);
+        else eval_batch_kernel<true, false, false><<<blocks, kEvalThreads, 0, st>>>(sc, args_dev, work_dev);
+    } else {
+        if (mode.fold) eval_batch_kernel<false, false, true><<<blocks, kEvalThreads, 0, st>>>(sc, args_dev, work_dev);
+        else eval_batch_kernel<false, false, false><<<blocks, kEvalThreads, 0, st>>>(sc, args_dev, work_dev);
+    }
     return cudaGetLastError();
 }
 

@@ -235,6 +235,37 @@ cudaError_t run_multigrid(pppm_scene *s);
 cudaError_t launch_farfield(pppm_scene *s);
 cudaError_t launch_eval(pppm_scene *s, const float4 *eval_a, const float4 *eval_b, int is_segment,
                         uint32_t M, double *u, double *v, double *w, float *uf, int count_pairs);
+
+// Everything the evaluation of one scene's points reads and writes.
+struct EvalArgs {
+    const uint32_t *eidx;          // sorted original indices of the points
+    uint32_t M;
+    const float4 *eval_a, *eval_b;
+    const float *far;
+    const uint32_t *start, *end, *sub_start, *sub_end;
+    const float4 *vrec, *valf;
+    const DevParams *P;
+    int n, K;
+    double *u, *v, *w;
+    float *uf;
+    unsigned long long *pair_count;
+};
+// What items of one batched evaluation launch must share: the smoothing
+// series (bytes), its folding and the segment mode.
+struct EvalMode {
+    bool fold = false, seg = false;
+    unsigned char series[192] = {};
+    bool same(const EvalMode &o) const {
+        if (fold != o.fold || seg != o.seg) return false;
+        for (int i = 0; i < 192; i++)
+            if (series[i] != o.series[i]) return false;
+        return true;
+    }
+};
+cudaError_t eval_batch_prepare(pppm_scene *s, const float4 *eval_a, const float4 *eval_b, int is_segment, uint32_t M,
+                               double *u, double *v, double *w, EvalArgs *args, EvalMode *mode);
+cudaError_t launch_eval_batch(const EvalMode &mode, const EvalArgs *args_dev, const uint2 *work_dev, uint32_t blocks,
+                              cudaStream_t st);
 cudaError_t launch_gather_sorted(pppm_scene *s, float4 *pos_out, double *alpha_out);
 cudaError_t launch_move(pppm_scene *s, const float4 *base, const double *u, size_t stride, double dt, uint32_t N,
                         float4 *out);
