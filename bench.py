@@ -110,7 +110,7 @@ def parse():
                     help="plume: radius of the heated sphere")
     ap.add_argument("--scenes", type=int, default=64)
     ap.add_argument("--rate", type=float, default=200.0, help="serve: mean arrivals per second")
-    ap.add_argument("--duration", type=float, default=4.0, help="serve: seconds of arrivals")
+    ap.add_argument("--duration", type=float, default=6.0, help="serve: seconds of arrivals per swept rate")
     ap.add_argument("--slots", type=int, default=8, help="serve: concurrent request slots")
     return ap.parse_args()
 
@@ -521,14 +521,16 @@ def run_mix(args, world, rank, local):
     mine = R.partition_scenes([R.scene_cost(n, N) for n, N, _, _ in mix], world)[rank]
     total_all = sum(N for _, N, _, _ in mix)
     mix = [mix[i] for i in mine]
-    scenes, data = [], []
+    scenes, data, host = [], [], []
     for n, N, kind, seed in mix:
         pos, al = W.make_scene(kind, N, seed)
         dpos = torch.from_numpy(pos).cuda()
         dal = torch.from_numpy(np.ascontiguousarray(al.T)).cuda()
         out = torch.empty((3, N), dtype=torch.float64, device="cuda")
-        scenes.append(pb.Scene(n, cap_vort=N, cap_eval=N))
+        scenes.append(pb.Scene(n, cap_vort=N, cap_eval=N, **PRESETS["configured"]))
         data.append((dpos, dal, out))
+        host.append((torch.from_numpy(pos).pin_memory(), torch.from_numpy(np.ascontiguousarray(al.T)).pin_memory(),
+                     torch.empty((3, N), dtype=torch.float64).pin_memory()))
     total = sum(N for _, N, _, _ in mix)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream()
@@ -564,6 +566,37 @@ def run_mix(args, world, rank, local):
 
     seq_ms = timed(sequential)
     bat_ms = timed(batched)
+
+    # the plain path a caller without device buffers takes: each scene through
+    # pppm_solve_host in turn (copies in, build, evaluate, copies out, sync)
+    def host_sequential():
+        for sc, (hp, ha, ho) in zip(scenes, host):
+            sc.solve_host(hp, ha, None, None, 1, out_host=ho)
+
+    host_sequential()
+    host_ms = []
+    for _ in range(max(2, min(args.steps, 3))):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        host_sequential()
+        host_ms.append((time.perf_counter() - t0) * 1000.0)
+    host_seq_ms = R.max_over_ranks(statistics.median(host_ms), device="cuda")
+
+    # every scene's error against the FP64 direct sum on its every 100th
+    # particle (velocities of the last batched step)
+    batched()
+    torch.cuda.synchronize()
+    num = den = 0.0
+    errs = []
+    for sc, (dpos, dal, out) in zip(scenes, data):
+        sub = dpos[::100].contiguous()
+        ref = pb.direct_sum_fp64(dpos, dal, sub, sc.smoothing(), sub, 1).cpu().numpy()
+        got = out.t()[::100].cpu().numpy()
+        d2, r2 = float(np.sum((got - ref) ** 2)), float(np.sum(ref ** 2))
+        num += d2
+        den += r2
+        errs.append((d2 / r2) ** 0.5 if r2 > 0 else 0.0)
     total = total_all
     if rank == 0:
         print(json.dumps({
@@ -571,75 +604,142 @@ def run_mix(args, world, rank, local):
             "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": bat_ms, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f32 (multigrid residual/accumulation f64)",
             "data": "synthetic",
-            "config": {"workload": f"{args.scenes}-scene mix (grid 32..128, 1e4..1e6 particles, clouds + rings), "
-                                   "each scene evaluated at its particles", "scenes": args.scenes,
+            "config": {"workload": f"{args.scenes}-scene mix (grid 32..128, 1e4..1e6 particles, clouds + rings, "
+                                   "radius one cell, K=1), each scene evaluated at its particles",
+                       "scenes": args.scenes,
                        "particles_total": total, "l2": "flushed before each timed step",
                        "parallelism": f"scenes split over {world} GPUs (whole scenes per rank)" if world > 1
                        else "one GPU"},
             "sequential_ms": seq_ms, "batched_ms": bat_ms, "batch_speedup": seq_ms / bat_ms,
-            "sequential_evals_per_s": total / (seq_ms / 1000.0)}), flush=True)
+            "sequential_evals_per_s": total / (seq_ms / 1000.0),
+            "host_sequential_ms": host_seq_ms, "speedup_vs_host_sequential": host_seq_ms / bat_ms,
+            "err_vs_direct_fp64": (num / den) ** 0.5 if den > 0 else None,
+            "err_vs_direct_fp64_per_scene": {"max": max(errs), "median": statistics.median(errs),
+                                             "min": min(errs)},
+            "error_sample": "every 100th particle of every scene (this rank's scenes)"}), flush=True)
     for sc in scenes:
         sc.close()
     R.finish()
 
 
 def run_serve(args, world, rank, local):
-    """Serving mix: open-loop Poisson arrivals (mean --rate per second, seed 3)
-    over the 64-scene mix, half velocity evaluations and half 10-step RK2
-    advances (dt 1e-3), served by the request loop under a 150 GB HBM budget
-    with scenes resident across requests.  Throughput counts particle
-    evaluations (an advance step evaluates twice); latency is completion minus
-    arrival."""
-    import threading
+    """Serving mix: open-loop Poisson arrivals (seed 3) over the 64-scene mix,
+    half velocity evaluations and half 10-step RK2 advances (dt 1e-3), served
+    by the request loop under a 150 GB HBM budget with scenes resident across
+    requests.  Throughput counts particle evaluations (an advance step
+    evaluates twice); latency is completion minus arrival.
+
+    The configured arrival rate (--rate, 200 req/s) is far above what one GPU
+    serves for this mix, so the run first measures the capacity (a closed
+    loop that keeps every slot busy), then sweeps open-loop rates below it
+    (p50 / p99 where the queue stays bounded), and finally offers the
+    configured rate for a short window.  Accuracy: every scene is evaluated
+    through the server at the end, and its velocities on every 100th particle
+    are compared with the FP64 direct sum at the positions it was served at."""
     import torch
+    import pppm_vortex_bouyant_flow_sample_b200 as pb
     from pppm_vortex_bouyant_flow_sample_b200 import server as S
     from pppm_vortex_bouyant_flow_sample_b200 import workloads as W
     torch.cuda.set_device(local)
     mix = W.scene_mix(args.scenes, seed=2)
     srv = S.Server(hbm_budget_bytes=150 << 30, slots=args.slots)
-    ids, sizes = [], []
+    ids, sizes, grids, alphas = [], [], [], []
     for n, N, kind, seed in mix:
         pos, al = W.make_scene(kind, N, seed)
-        ids.append(srv.add_scene(n, pos, al))
+        ids.append(srv.add_scene(n, pos, al, **PRESETS["configured"]))
         sizes.append(N)
+        grids.append(n)
+        alphas.append(al)
     for sid in ids:  # make every scene resident once (state kept across requests)
         srv.wait(srv.submit_eval(sid))
     g = W.SplitMix64(3)
-    count = max(1, int(args.rate * args.duration))
-    gaps = -np.log1p(-g.uniform(count)) / args.rate
-    arrivals = np.cumsum(gaps)
-    pick = (g.uniform(count) * len(ids)).astype(int)
-    kinds = g.uniform(count) < 0.5
-    tickets, evals = [], 0
-    t0 = time.perf_counter()
-    for a, q, is_eval in zip(arrivals, pick, kinds):
-        d = t0 + a - time.perf_counter()
-        if d > 0:
-            time.sleep(d)
+
+    def draw(count):
+        pick = (g.uniform(count) * len(ids)).astype(int)
+        kinds = g.uniform(count) < 0.5
+        return pick, kinds
+
+    def submit(q, is_eval):
         if is_eval:
-            tickets.append(srv.submit_eval(ids[q]))
-            evals += sizes[q]
-        else:
-            tickets.append(srv.submit_advance(ids[q], 10, 1e-3))
-            evals += 20 * sizes[q]
-    lat, first, last = [], None, None
-    for t in tickets:
-        info, _ = srv.wait(t)
-        lat.append(info["latency_s"])
-        first = info["submit_s"] if first is None else min(first, info["submit_s"])
-        last = info["end_s"] if last is None else max(last, info["end_s"])
-    wall = last - first
-    lat_ms = np.array(lat) * 1000.0
+            return srv.submit_eval(ids[q]), sizes[q]
+        return srv.submit_advance(ids[q], 10, 1e-3), 20 * sizes[q]
+
+    def collect(tickets):
+        lat, first, last = [], None, None
+        for t in tickets:
+            info, _ = srv.wait(t)
+            lat.append(info["latency_s"])
+            first = info["submit_s"] if first is None else min(first, info["submit_s"])
+            last = info["end_s"] if last is None else max(last, info["end_s"])
+        return np.array(lat) * 1000.0, last - first
+
+    # capacity: a closed loop with every slot busy
+    cap_n = max(2 * args.slots, 48)
+    pick, kinds = draw(cap_n)
+    tickets, evals = [], 0
+    for q, is_eval in zip(pick, kinds):
+        t, e = submit(q, is_eval)
+        tickets.append(t)
+        evals += e
+    lat_c, wall_c = collect(tickets)
+    capacity = cap_n / wall_c
+
+    def open_loop(rate, count):
+        gaps = -np.log1p(-g.uniform(count)) / rate
+        arrivals = np.cumsum(gaps)
+        pick, kinds = draw(count)
+        tickets, ev = [], 0
+        t0 = time.perf_counter()
+        for a, q, is_eval in zip(arrivals, pick, kinds):
+            d = t0 + a - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            t, e = submit(q, is_eval)
+            tickets.append(t)
+            ev += e
+        lat, wall = collect(tickets)
+        return {"rate_req_s": rate, "requests": count, "p50_ms": float(np.percentile(lat, 50)),
+                "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
+                "evals_per_s": ev / wall, "wall_s": wall}
+
+    sweep = [open_loop(f * capacity, max(24, int(f * capacity * args.duration))) for f in (0.3, 0.6, 0.9)]
+    over = open_loop(args.rate, max(24, int(args.rate * 0.25)))
+
+    # accuracy of served evaluations: every scene, every 100th particle
+    num = den = 0.0
+    errs = []
+    for sid, n, al in zip(ids, grids, alphas):
+        _, v = srv.wait(srv.submit_eval(sid))
+        p = srv.positions(sid)
+        ext = (p[:, :3].max(axis=0).astype(np.float64) - p[:, :3].min(axis=0).astype(np.float64)).max()
+        a = PRESETS["configured"]["a_cells"] * float(np.float32(3.0 * ext / n))
+        dp = torch.from_numpy(p).cuda()
+        dal = torch.from_numpy(np.ascontiguousarray(al)).cuda()
+        sub = dp[::100].contiguous()
+        ref = pb.direct_sum_fp64(dp, dal, sub, a, sub, 1).cpu().numpy()
+        got = v[::100]
+        d2, r2 = float(np.sum((got - ref) ** 2)), float(np.sum(ref ** 2))
+        num += d2
+        den += r2
+        errs.append((d2 / r2) ** 0.5)
+    # headline of the line: the highest swept rate below capacity
+    top = sweep[-1]
     if rank == 0:
         print(json.dumps({
-            "metric": METRIC, "value": evals / wall, "unit": UNIT, "n_gpus": 1, "steps": count, "warmup": len(ids),
-            "ms_per_step": 1000.0 * wall / count, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 (multigrid residual/accumulation f64)", "data": "synthetic",
-            "config": {"workload": f"serving mix: Poisson {args.rate:g} req/s for {args.duration:g} s over the "
-                                   f"{len(ids)}-scene mix, half eval / half 10-step RK2 advance, HBM budget 150 GB",
-                       "slots": args.slots, "requests": count},
-            "p50_ms": float(np.percentile(lat_ms, 50)), "p99_ms": float(np.percentile(lat_ms, 99)),
-            "mean_ms": float(lat_ms.mean()), "wall_s": wall, "evaluations": evals}), flush=True)
+            "metric": METRIC, "value": top["evals_per_s"], "unit": UNIT, "n_gpus": 1, "steps": top["requests"],
+            "warmup": len(ids), "ms_per_step": 1000.0 * top["wall_s"] / top["requests"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (multigrid residual/accumulation f64)",
+            "data": "synthetic",
+            "config": {"workload": f"serving mix: Poisson arrivals over the {len(ids)}-scene mix (radius one cell, "
+                                   "K=1), half eval / half 10-step RK2 advance, HBM budget 150 GB",
+                       "slots": args.slots, "line_rate": "0.9 x measured capacity"},
+            "capacity_req_s": capacity, "capacity_evals_per_s": evals / wall_c,
+            "p50_ms": top["p50_ms"], "p99_ms": top["p99_ms"], "sweep": sweep,
+            "configured_rate": dict(over, note="offered load above capacity: the queue grows, so latency "
+                                              "measures the backlog"),
+            "err_vs_direct_fp64": (num / den) ** 0.5, "err_vs_direct_fp64_per_scene_max": max(errs),
+            "error_sample": "every scene evaluated through the server; every 100th particle vs the FP64 direct sum"}),
+            flush=True)
     srv.close()
 
 

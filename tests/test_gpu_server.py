@@ -68,3 +68,67 @@ def test_eviction_keeps_advanced_positions(srvmod):
         scene.advect(dpos, dal, 2e-3, method="rk2")
     assert np.array_equal(got, dpos.cpu().numpy())
     scene.close()
+
+
+def test_admission_near_the_budget_under_concurrent_requests(srvmod):
+    """Six scenes whose footprints together exceed the HBM budget about
+    threefold, requested from three threads at once over four slots: every
+    request completes, each EVAL equals the scene's result alone, and the
+    resident footprint never exceeds the budget (the loop evicts idle scenes,
+    least recently used first, to admit the next)."""
+    import threading
+    import time
+    from pppm_vortex_bouyant_flow_sample_b200 import workloads as W
+    specs = [(32, "cloud", 9000, 51), (48, "ring", 25000, 52), (64, "cloud", 18000, 53), (32, "ring", 12000, 54),
+             (48, "cloud", 15000, 55), (64, "ring", 22000, 56)]
+    scenes = [(n,) + W.make_scene(kind, N, seed) for n, kind, N, seed in specs]
+    # alone: each scene's EVAL with a budget that holds everything
+    ref = {}
+    srv = srvmod.Server(hbm_budget_bytes=8 << 30, slots=1)
+    try:
+        for q, (n, pos, al) in enumerate(scenes):
+            _, v = srv.wait(srv.submit_eval(srv.add_scene(n, pos, al)))
+            ref[q] = v.copy()
+    finally:
+        srv.close()
+    budget = 110 << 20
+    srv = srvmod.Server(hbm_budget_bytes=budget, slots=4)
+    try:
+        ids = [srv.add_scene(n, pos, al) for n, pos, al in scenes]
+        results, errors, peak = [], [], [0]
+        lock = threading.Lock()
+        stop = threading.Event()
+
+        def sampler():
+            while not stop.is_set():
+                peak[0] = max(peak[0], srv.stats()["resident_bytes"])
+                time.sleep(0.001)
+
+        def client(offset):
+            try:
+                for rep in range(4):
+                    for k in range(len(ids)):
+                        q = (k + offset + rep) % len(ids)
+                        info, v = srv.wait(srv.submit_eval(ids[q]))
+                        with lock:
+                            results.append((q, v.copy()))
+            except Exception as exc:  # reported below
+                errors.append(exc)
+
+        th = [threading.Thread(target=client, args=(o,)) for o in range(3)]
+        sm = threading.Thread(target=sampler)
+        sm.start()
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        stop.set()
+        sm.join()
+        assert not errors, errors
+        assert len(results) == 3 * 4 * len(ids)
+        for q, v in results:
+            assert np.array_equal(v, ref[q]), q
+        assert 0 < peak[0] <= budget
+        assert srv.stats()["completed"] == len(results)
+    finally:
+        srv.close()
