@@ -100,6 +100,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-variants", action="store_true",
+                    help="ring: skip the reference-constant / accurate variants and the RK2 / vortex-step extras "
+                         "(short runs for profiling)")
     ap.add_argument("--particles", type=int, default=N_PART)
     ap.add_argument("--grid", type=int, default=GRID)
     ap.add_argument("--workload", default="ring", choices=["ring", "mix", "serve", "render", "plume", "potential"],
@@ -320,6 +323,52 @@ def read_profile_traffic():
     return None
 
 
+def _extras(scene, dpos, dal, flush, stream):
+    """One RK2 (midpoint) advection step of the scene (two far-field builds and
+    two evaluations) and one vortex-segment time step (the reference's
+    solveTimeStep without boundary or heat: 2N end evaluations, segment
+    update, rehash, smoothing), each device-timed (median of 3) with its
+    stage split; reported beside the headline, not in it."""
+    import torch
+    rk_pos = dpos.clone()
+    scene.advect(rk_pos, dal, 1e-3, method="rk2")
+    torch.cuda.synchronize()
+    rk_ms = []
+    for _ in range(3):
+        rk_pos.copy_(dpos)
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        scene.advect(rk_pos, dal, 1e-3, method="rk2")
+        e1.record(stream)
+        torch.cuda.synchronize()
+        rk_ms.append(e0.elapsed_time(e1))
+    del rk_pos
+    vs_pos, vs_al = dpos.clone(), dal.clone()
+    scene.vortex_step(vs_pos, vs_al, 1e-3)
+    torch.cuda.synchronize()
+    vs_ms, vs_stage = [], {}
+    scene.set_profiling(True)
+    for _ in range(3):
+        vs_pos.copy_(dpos)
+        vs_al.copy_(dal)
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        scene.vortex_step(vs_pos, vs_al, 1e-3)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        vs_ms.append(e0.elapsed_time(e1))
+        for k, v in scene.stage_times().items():
+            if v >= 0:
+                vs_stage.setdefault(k, []).append(v)
+    scene.set_profiling(False)
+    return (statistics.median(rk_ms), statistics.median(vs_ms),
+            {k: statistics.median(v) for k, v in vs_stage.items()})
+
+
 def run_b200(args, world, rank, local):
     import torch
     import torch.distributed as dist
@@ -404,50 +453,13 @@ def run_b200(args, world, rank, local):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_val = world * N / float(t.item())
 
-    # one RK2 (midpoint) advection step of the same scene: two far-field
-    # builds and two evaluations (reported beside the headline, not in it)
-    rk_pos = dpos.clone()
-    scene.advect(rk_pos, dal, 1e-3, method="rk2")
-    torch.cuda.synchronize()
-    rk_ms = []
-    for _ in range(3):
-        rk_pos.copy_(dpos)
-        flush.zero_()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        scene.advect(rk_pos, dal, 1e-3, method="rk2")
-        e1.record(stream)
-        torch.cuda.synchronize()
-        rk_ms.append(e0.elapsed_time(e1))
-    rk2_ms = statistics.median(rk_ms)
-    del rk_pos
-
-    # one vortex-segment time step (the reference's solveTimeStep without
-    # boundary or heat): 2N end evaluations, segment update, rehash, smoothing
-    vs_pos, vs_al = dpos.clone(), dal.clone()
-    scene.vortex_step(vs_pos, vs_al, 1e-3)
-    torch.cuda.synchronize()
-    vs_ms, vs_stage = [], {}
-    scene.set_profiling(True)
-    for _ in range(3):
-        vs_pos.copy_(dpos)
-        vs_al.copy_(dal)
-        flush.zero_()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        scene.vortex_step(vs_pos, vs_al, 1e-3)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        vs_ms.append(e0.elapsed_time(e1))
-        for k, v in scene.stage_times().items():
-            if v >= 0:
-                vs_stage.setdefault(k, []).append(v)
-    scene.set_profiling(False)
-    vortex_step_ms = statistics.median(vs_ms)
-    vortex_step_stages = {k: statistics.median(v) for k, v in vs_stage.items()}
-    del vs_pos, vs_al
+    # an RK2 step and a vortex-segment time step of the same scene, and (below)
+    # the reference-constant and accurate variants; --no-variants skips them
+    extras = not args.no_variants
+    rk2_ms = vortex_step_ms = None
+    vortex_step_stages = {}
+    if extras:
+        rk2_ms, vortex_step_ms, vortex_step_stages = _extras(scene, dpos, dal, flush, stream)
 
     # accuracy on a fixed 1% subsample (every 100th particle) vs the FP64 direct sum
     # with the same smoothing kernel (a as the build resolved it)
@@ -458,7 +470,7 @@ def run_b200(args, world, rank, local):
 
     # the same scene with the reference's constants and with the accurate preset
     variants = {}
-    for name in ("reference_constants", "accurate"):
+    for name in (("reference_constants", "accurate") if extras else ()):
         vs = pb.Scene(args.grid, cap_vort=N, cap_eval=N, stream=stream, **PRESETS[name])
         vout = torch.empty((3, N), dtype=torch.float64, device="cuda")
 
