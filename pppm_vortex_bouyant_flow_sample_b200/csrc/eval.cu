@@ -23,7 +23,11 @@
 // scene can reach t = 0.25, a degree-4 polynomial (Chebyshev interpolant on
 // [0, 0.25], relative error 5e-9); otherwise a degree-7 one on [0, 2] (relative
 // error 2e-7, below that of the exp form near t = 0.25) and (1 - exp(-t)) / t
-// above t = 2.  No cancellation in either polynomial.
+// above t = 2.  No cancellation in either polynomial.  When some pair can
+// reach t = 2 (a smoothing radius of about a cell or less), the warp-uniform
+// walk takes the exp form (1 - e^-t) / (4 pi r^3) for every pair, r^-1 from
+// rsqrt.approx and e^-t from ex2.approx, with a degree-5 polynomial of phi
+// below t = 1/64, where 1 - e^-t would cancel.
 #include <climits>
 #include <cstring>
 #include <cmath>
@@ -163,13 +167,22 @@ struct PairAcc2 {
     unsigned long long n = 0;
 };
 
-// Per-warp staging of 32 vortex records as 16 record pairs, so that one
-// Blackwell f32x2 instruction (FADD2 / FMUL2 / FFMA2) works on two records:
-// slot p holds records 2p (.x, .z halves) and 2p+1 (.y, .w halves) of the
-// chunk.  Planes: A {-x, -y}, B {-z, alpha_x}, C {alpha_y, alpha_z},
-// D {m_x, m_y}, E {m_z} with m = alpha x (r - o).
-constexpr int kPackSlots = 16;
+// Per-warp ring of staged vortex records: 64 records as 32 record pairs, so
+// that one Blackwell f32x2 instruction (FADD2 / FMUL2 / FFMA2) works on two
+// records: slot p holds records 2p (.x, .z halves) and 2p+1 (.y, .w halves).
+// Planes: A {-x, -y}, B {-z, alpha_x}, C {alpha_y, alpha_z}, D {m_x, m_y},
+// E {m_z} with m = alpha x (r - o).  Records kept from successive runs are
+// appended (record i at slot (i / 2) mod 32) and evaluated 32 at a time, so
+// the pair loop runs whole blocks of 16 slots whatever the lengths of the
+// runs; only the last block of a walk is partial.
+constexpr int kPackSlots = 32;
 constexpr int kPackPlanes = 5;
+constexpr uint32_t kBlockRecs = 32;  // records per block of the pair loop
+
+struct Ring {
+    uint32_t fill = 0;  // records staged so far
+    uint32_t head = 0;  // records evaluated so far (a multiple of kBlockRecs)
+};
 
 // max(|a|, |b|, |c|) in one instruction: the three-input max.abs of PTX ISA 8.8
 // (sm_100 and later).
@@ -206,7 +219,18 @@ struct ExpForm {
     float2 inv_a3;   // {1/a^3, 1/a^3}
     float2 nl2a3;    // {-log2(e)/a^3, ...}: the exponent of e^-t in base 2, per r^3
     float tsmall;    // below it phi comes from the polynomial (1 - e^-t cancels)
+    float r3small;   // r^3 above tsmall * a^3 by a margin: the warp's trigger
 };
+
+// Switch point of the exp form to the polynomial.  ex2.approx has a relative
+// error of about 2^-22 (the PTX ISA's bound), so near 1 the absolute error of
+// e^-t is about 2^-22 and 1 - e^-t carries a relative error of about
+// 2^-22 / t: 1.5e-5 at t = 1/64 (r = a / 4), falling as 1 / t, on pairs whose
+// terms are a small part of the sum.  A low switch point keeps the polynomial
+// branch rare: with a = h and K = 1 about 0.2 % of a lane's pairs have
+// t < 1/64, against 5 % below t = 0.5, where some lane of the warp needed the
+// branch on nearly every step.
+constexpr float kExpSmallT = 1.0f / 64.0f;
 
 __device__ __forceinline__ void stage_record(float *__restrict__ pk, int slot, int half, float4 r, float4 a,
                                              float3 o) {
@@ -221,92 +245,71 @@ __device__ __forceinline__ void stage_record(float *__restrict__ pk, int slot, i
     E[half] = fmaf(a.x, sy, -(a.y * sx));
 }
 
-// Warp-uniform walk over one run of vortex records: the warp stages them 32 at
-// a time (one coalesced load per stream), then every lane takes them two at a
-// time from shared memory (broadcast reads) and evaluates both pairs with
-// packed f32x2 arithmetic.  cr_lane is the box half-width, or -1 for a lane
-// whose hash-cell range excludes this run.  An odd chunk is padded with a
-// record at (-1e18, -1e18, -1e18) and zero strength, outside every box.  The
-// r = 0 exclusion needs no test: the pair's (ra - r_p) is zero.  SEG keeps the
-// other-end test.  phi is the degree-DEG polynomial cf (DEG 4: the scene never
-// leaves [0, 0.25]; DEG 7: valid on [0, 2], the exp form above tbig when
-// need_exp).  FOLD: the coefficients carry the powers of 1/a^3, so the
-// polynomial takes r^3 directly and tbig is in r^3 too.
-template <bool SEG, bool COUNT, bool FOLD, int DEG>
-__device__ __forceinline__ void cell_pairs_packed(const float4 *__restrict__ vrec, const float4 *__restrict__ valf,
-                                                  uint32_t ps, uint32_t pe, float cr_lane, const float3 ra,
-                                                  const float3 rb, float3 o, const float3 blo, const float3 bhi,
-                                                  float2 inv_a3, const float2 *cf, float tbig, float inv4pia3,
-                                                  bool need_exp, float4 *__restrict__ pk4, int lane,
-                                                  PairAcc2 &acc, const ExpForm &xf) {
-    float *pk = reinterpret_cast<float *>(pk4);
+// The pair loop over np slots of the ring from slot s0 (FULL: one whole block
+// of 16 slots, unrolled into straight-line code with constant offsets): every
+// lane takes the records two at a time from shared memory (broadcast reads)
+// and evaluates both pairs with packed f32x2 arithmetic.  cr_lane is the box
+// half-width, or -1 for an inactive lane.  The r = 0 exclusion needs no test:
+// the pair's (ra - r_p) is zero.  SEG keeps the other-end test.  phi is the
+// degree-DEG polynomial cf (DEG 4: the scene never leaves [0, 0.25]; DEG 7:
+// valid on [0, 2], the exp form above tbig when need_exp; DEG 0: the exp form,
+// the polynomial only for small t).  FOLD: the coefficients carry the powers
+// of 1/a^3, so the polynomial takes r^3 directly and tbig is in r^3 too.
+template <bool SEG, bool COUNT, bool FOLD, int DEG, bool FULL>
+__device__ __forceinline__ void pair_slots(const float4 *__restrict__ pk4, uint32_t s0, uint32_t np, float cr_lane,
+                                           const float3 ra, const float3 rb, float2 inv_a3, const float2 *cf,
+                                           float tbig, float inv4pia3, bool need_exp, PairAcc2 &acc,
+                                           const ExpForm &xf) {
     const float2 tx = make_float2(ra.x, ra.x), ty = make_float2(ra.y, ra.y), tz = make_float2(ra.z, ra.z);
-    for (uint32_t base = ps; base < pe; base += 32) {
-        const uint32_t cnt = min(32u, pe - base);
-        // records outside the warp's box [blo, bhi] (every lane's box, widened
-        // beyond float rounding) cannot pass any lane's test: the chunk keeps
-        // only the others, packed to the front
-        bool keep = false;
-        float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
-        if ((uint32_t)lane < cnt) {
-            r = vrec[base + lane];
-            keep = r.x >= blo.x && r.x <= bhi.x && r.y >= blo.y && r.y <= bhi.y && r.z >= blo.z && r.z <= bhi.z;
+    const uint32_t cnt = FULL ? kBlockRecs / 2 : np;
+#pragma unroll (FULL ? kBlockRecs / 2 : 2)
+    for (uint32_t i = 0; i < cnt; i++) {
+        const uint32_t p = s0 + i;
+        const float4 A = pk4[0 * kPackSlots + p], B = pk4[1 * kPackSlots + p], Cc = pk4[2 * kPackSlots + p];
+        const float4 D = pk4[3 * kPackSlots + p], E = pk4[4 * kPackSlots + p];
+        const float2 nx = make_float2(A.x, A.y), ny = make_float2(A.z, A.w), nz = make_float2(B.x, B.y);
+        const float2 dx = __fadd2_rn(tx, nx), dy = __fadd2_rn(ty, ny), dz = __fadd2_rn(tz, nz);
+        const float m0 = max3_abs(dx.x, dy.x, dz.x);
+        const float m1 = max3_abs(dx.y, dy.y, dz.y);
+        // (the exp form adds 1e-30 to r^2 in the chain, so that rsqrt stays
+        // finite at r = 0; that pair takes the polynomial below)
+        const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, make_float2(DEG == 0 ? 1e-30f : 0.f,
+                                                                                    DEG == 0 ? 1e-30f : 0.f))));
+        bool ok0 = m0 <= cr_lane, ok1 = m1 <= cr_lane;
+        if (COUNT) acc.n += (ok0 ? 1ull : 0ull) + (ok1 ? 1ull : 0ull);
+        if (SEG) {
+            const float2 ex = __fadd2_rn(make_float2(rb.x, rb.x), nx);
+            const float2 ey = __fadd2_rn(make_float2(rb.y, rb.y), ny);
+            const float2 ez = __fadd2_rn(make_float2(rb.z, rb.z), nz);
+            const float2 e2 = __ffma2_rn(ex, ex, __ffma2_rn(ey, ey, __fmul2_rn(ez, ez)));
+            ok0 = ok0 && !(e2.x < 1e-24f);
+            ok1 = ok1 && !(e2.y < 1e-24f);
         }
-        const unsigned kept = __ballot_sync(0xffffffffu, keep);
-        const uint32_t kc = (uint32_t)__popc(kept);
-        if (kc == 0) continue;
-        if (keep) {
-            const int dst = __popc(kept & ((1u << lane) - 1u));
-            stage_record(pk, dst >> 1, dst & 1, r, valf[base + lane], o);
-        }
-        if (lane == 0 && (kc & 1u))
-            stage_record(pk, (int)(kc >> 1), 1, make_float4(-1e18f, -1e18f, -1e18f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f),
-                         make_float3(0.f, 0.f, 0.f));
-        __syncwarp();
-        const uint32_t np = (kc + 1) >> 1;
-#pragma unroll 2
-        for (uint32_t p = 0; p < np; p++) {
-            const float4 A = pk4[0 * kPackSlots + p], B = pk4[1 * kPackSlots + p], Cc = pk4[2 * kPackSlots + p];
-            const float4 D = pk4[3 * kPackSlots + p], E = pk4[4 * kPackSlots + p];
-            const float2 nx = make_float2(A.x, A.y), ny = make_float2(A.z, A.w), nz = make_float2(B.x, B.y);
-            const float2 dx = __fadd2_rn(tx, nx), dy = __fadd2_rn(ty, ny), dz = __fadd2_rn(tz, nz);
-            const float m0 = max3_abs(dx.x, dy.x, dz.x);
-            const float m1 = max3_abs(dx.y, dy.y, dz.y);
-            const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
-            bool ok0 = m0 <= cr_lane, ok1 = m1 <= cr_lane;
-            if (COUNT) acc.n += (ok0 ? 1ull : 0ull) + (ok1 ? 1ull : 0ull);
-            if (SEG) {
-                const float2 ex = __fadd2_rn(make_float2(rb.x, rb.x), nx);
-                const float2 ey = __fadd2_rn(make_float2(rb.y, rb.y), ny);
-                const float2 ez = __fadd2_rn(make_float2(rb.z, rb.z), nz);
-                const float2 e2 = __ffma2_rn(ex, ex, __ffma2_rn(ey, ey, __fmul2_rn(ez, ez)));
-                ok0 = ok0 && !(e2.x < 1e-24f);
-                ok1 = ok1 && !(e2.y < 1e-24f);
-            }
-            float2 c;
-            if constexpr (DEG == 0) {
-                // exp form, c * 4 pi = (1 - e^-t) / r^3 with t = r^3 / a^3: r^-1
-                // from rsqrt, e^-t from ex2 (two special-function ops); where
-                // some lane has t < tsmall (1 - e^-t cancels, or r = 0) the
-                // degree-5 polynomial phi(t) / a^3 replaces it
-                const float2 r2c = make_float2(fmaxf(r2.x, 1e-30f), fmaxf(r2.y, 1e-30f));
-                const float2 rs = make_float2(rsqrt_approx(r2c.x), rsqrt_approx(r2c.y));
-                const float2 r3 = __fmul2_rn(r2c, __fmul2_rn(r2c, rs));
-                const float2 ri3 = __fmul2_rn(__fmul2_rn(rs, rs), rs);
-                const float2 ex = __fmul2_rn(r3, xf.nl2a3);
-                const float2 e = make_float2(ex2_approx(ex.x), ex2_approx(ex.y));
-                c = __ffma2_rn(make_float2(-e.x, -e.y), ri3, ri3);
+        float2 c;
+        if constexpr (DEG == 0) {
+            // exp form, c * 4 pi = (1 - e^-t) / r^3 with t = r^3 / a^3: r^-1
+            // from rsqrt, e^-t from ex2 (two special-function ops); where
+            // some lane has t < tsmall (1 - e^-t cancels, or r = 0) the
+            // degree-5 polynomial phi(t) / a^3 replaces it
+            const float2 rs = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+            const float2 r3 = __fmul2_rn(r2, __fmul2_rn(r2, rs));
+            const float2 ri3 = __fmul2_rn(__fmul2_rn(rs, rs), rs);
+            const float2 ex = __fmul2_rn(r3, xf.nl2a3);
+            const float2 e = make_float2(ex2_approx(ex.x), ex2_approx(ex.y));
+            c = __ffma2_rn(make_float2(-e.x, -e.y), ri3, ri3);
+            // the trigger r^3 < r3small is a superset of t < tsmall, and
+            // a lane outside its box may trigger it (its coefficient is
+            // dropped below either way)
+            if (__any_sync(0xffffffffu, fminf(r3.x, r3.y) < xf.r3small)) {
                 const float2 t = __fmul2_rn(r3, xf.inv_a3);
-                const bool s0 = ok0 && t.x < xf.tsmall, s1 = ok1 && t.y < xf.tsmall;
-                if (__any_sync(0xffffffffu, s0 || s1)) {
-                    float2 p = __ffma2_rn(cf[5], t, cf[4]);
+                float2 p = __ffma2_rn(cf[5], t, cf[4]);
 #pragma unroll
-                    for (int q = 3; q >= 0; q--) p = __ffma2_rn(p, t, cf[q]);
-                    p = __fmul2_rn(p, xf.inv_a3);
-                    c.x = s0 ? p.x : c.x;
-                    c.y = s1 ? p.y : c.y;
-                }
-            } else {
+                for (int q = 3; q >= 0; q--) p = __ffma2_rn(p, t, cf[q]);
+                p = __fmul2_rn(p, xf.inv_a3);
+                c.x = t.x < xf.tsmall ? p.x : c.x;
+                c.y = t.y < xf.tsmall ? p.y : c.y;
+            }
+        } else {
             const float2 r3 = __fmul2_rn(r2, make_float2(sqrt_approx(r2.x), sqrt_approx(r2.y)));
             const float2 t = FOLD ? r3 : __fmul2_rn(r3, inv_a3);
             c = __ffma2_rn(cf[DEG], t, cf[DEG - 1]);
@@ -315,24 +318,81 @@ __device__ __forceinline__ void cell_pairs_packed(const float4 *__restrict__ vre
             if (DEG > 4 && need_exp) {
                 const bool big0 = ok0 && t.x >= tbig, big1 = ok1 && t.y >= tbig;
                 if (__any_sync(0xffffffffu, big0 || big1)) {
-                    const float s0 = FOLD ? t.x * inv_a3.x : t.x, s1 = FOLD ? t.y * inv_a3.y : t.y;
-                    const float e0 = __fdividef(1.0f - __expf(-s0), fmaxf(s0, 1.0f)) * inv4pia3;
-                    const float e1 = __fdividef(1.0f - __expf(-s1), fmaxf(s1, 1.0f)) * inv4pia3;
+                    const float v0 = FOLD ? t.x * inv_a3.x : t.x, v1 = FOLD ? t.y * inv_a3.y : t.y;
+                    const float e0 = __fdividef(1.0f - __expf(-v0), fmaxf(v0, 1.0f)) * inv4pia3;
+                    const float e1 = __fdividef(1.0f - __expf(-v1), fmaxf(v1, 1.0f)) * inv4pia3;
                     c.x = big0 ? e0 : c.x;
                     c.y = big1 ? e1 : c.y;
                 }
             }
-            }
-            const float2 coeff = make_float2(ok0 ? c.x : 0.0f, ok1 ? c.y : 0.0f);
-            acc.ax = __ffma2_rn(coeff, make_float2(B.z, B.w), acc.ax);
-            acc.ay = __ffma2_rn(coeff, make_float2(Cc.x, Cc.y), acc.ay);
-            acc.az = __ffma2_rn(coeff, make_float2(Cc.z, Cc.w), acc.az);
-            acc.bx = __ffma2_rn(coeff, make_float2(D.x, D.y), acc.bx);
-            acc.by = __ffma2_rn(coeff, make_float2(D.z, D.w), acc.by);
-            acc.bz = __ffma2_rn(coeff, make_float2(E.x, E.y), acc.bz);
         }
-        __syncwarp();
+        const float2 coeff = make_float2(ok0 ? c.x : 0.0f, ok1 ? c.y : 0.0f);
+        acc.ax = __ffma2_rn(coeff, make_float2(B.z, B.w), acc.ax);
+        acc.ay = __ffma2_rn(coeff, make_float2(Cc.x, Cc.y), acc.ay);
+        acc.az = __ffma2_rn(coeff, make_float2(Cc.z, Cc.w), acc.az);
+        acc.bx = __ffma2_rn(coeff, make_float2(D.x, D.y), acc.bx);
+        acc.by = __ffma2_rn(coeff, make_float2(D.z, D.w), acc.by);
+        acc.bz = __ffma2_rn(coeff, make_float2(E.x, E.y), acc.bz);
     }
+}
+
+// Appends one run of vortex records [ps, pe) to the ring, 32 at a time (one
+// coalesced load per stream).  Records outside the warp's box [blo, bhi]
+// (every lane's box, widened beyond float rounding) cannot pass any lane's
+// test and are dropped.  Whenever 32 records wait, the warp evaluates them.
+// The ring never overwrites a record still waiting: before a chunk fewer than
+// 32 wait, a chunk adds at most 32, and the ring holds 64.
+template <bool SEG, bool COUNT, bool FOLD, int DEG>
+__device__ __forceinline__ void stage_run(const float4 *__restrict__ vrec, const float4 *__restrict__ valf,
+                                          uint32_t ps, uint32_t pe, float cr_lane, const float3 ra,
+                                          const float3 rb, float3 o, const float3 blo, const float3 bhi,
+                                          float2 inv_a3, const float2 *cf, float tbig, float inv4pia3,
+                                          bool need_exp, float4 *__restrict__ pk4, int lane, Ring &ring,
+                                          PairAcc2 &acc, const ExpForm &xf) {
+    float *pk = reinterpret_cast<float *>(pk4);
+    for (uint32_t base = ps; base < pe; base += 32) {
+        const uint32_t cnt = min(32u, pe - base);
+        bool keep = false;
+        float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+        if ((uint32_t)lane < cnt) {
+            r = vrec[base + lane];
+            keep = r.x >= blo.x && r.x <= bhi.x && r.y >= blo.y && r.y <= bhi.y && r.z >= blo.z && r.z <= bhi.z;
+        }
+        const unsigned kept = __ballot_sync(0xffffffffu, keep);
+        if (kept == 0u) continue;
+        if (keep) {
+            const uint32_t dst = ring.fill + (uint32_t)__popc(kept & ((1u << lane) - 1u));
+            stage_record(pk, (int)((dst >> 1) & (kPackSlots - 1)), (int)(dst & 1u), r, valf[base + lane], o);
+        }
+        ring.fill += (uint32_t)__popc(kept);
+        if (ring.fill - ring.head >= kBlockRecs) {
+            __syncwarp();
+            pair_slots<SEG, COUNT, FOLD, DEG, true>(pk4, (ring.head >> 1) & (kPackSlots - 1), 0, cr_lane, ra, rb,
+                                                    inv_a3, cf, tbig, inv4pia3, need_exp, acc, xf);
+            ring.head += kBlockRecs;
+            __syncwarp();  // the next records may take the slots just read
+        }
+    }
+}
+
+// Evaluates the records left in the ring after the walk (fewer than 32); an
+// odd count is padded with a record at (-1e18, -1e18, -1e18) and zero
+// strength, outside every box.
+template <bool SEG, bool COUNT, bool FOLD, int DEG>
+__device__ __forceinline__ void finish_ring(float cr_lane, const float3 ra, const float3 rb, float2 inv_a3,
+                                            const float2 *cf, float tbig, float inv4pia3, bool need_exp,
+                                            float4 *__restrict__ pk4, int lane, const Ring &ring, PairAcc2 &acc,
+                                            const ExpForm &xf) {
+    const uint32_t rem = ring.fill - ring.head;
+    if (rem == 0) return;
+    if (lane == 0 && (rem & 1u))
+        stage_record(reinterpret_cast<float *>(pk4), (int)((ring.fill >> 1) & (kPackSlots - 1)), 1,
+                     make_float4(-1e18f, -1e18f, -1e18f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f),
+                     make_float3(0.f, 0.f, 0.f));
+    __syncwarp();
+    pair_slots<SEG, COUNT, FOLD, DEG, false>(pk4, (ring.head >> 1) & (kPackSlots - 1), (rem + 1) >> 1, cr_lane, ra,
+                                             rb, inv_a3, cf, tbig, inv4pia3, need_exp, acc, xf);
+    __syncwarp();
 }
 
 constexpr int kUniformMaxSub = 1000;  // warp-uniform walk up to 10^3 half-cells
@@ -425,7 +485,8 @@ __device__ __forceinline__ void eval_points(const SmoothSeries &sc, const EvalAr
         ExpForm xf;
         xf.inv_a3 = make_float2(inv_a3, inv_a3);
         xf.nl2a3 = make_float2(-1.4426950408889634f * inv_a3, -1.4426950408889634f * inv_a3);
-        xf.tsmall = 0.5f;
+        xf.tsmall = kExpSmallT;
+        xf.r3small = 1.001f * kExpSmallT / inv_a3;
         // warp origin of the packed accumulation: lane 0's position
         const float3 o = make_float3(__shfl_sync(0xffffffffu, ra.x, 0), __shfl_sync(0xffffffffu, ra.y, 0),
                                      __shfl_sync(0xffffffffu, ra.z, 0));
@@ -479,9 +540,18 @@ __device__ __forceinline__ void eval_points(const SmoothSeries &sc, const EvalAr
         for (int a = 0; a < 3; a++) vol *= (uhi[a] >= ulo[a]) ? (long long)(uhi[a] - ulo[a] + 1) : 0ll;
         // warp-uniform walk over half-cells: every lane sees the same vortex at
         // once; DEG picks phi's polynomial (one walk per polynomial, so that
-        // only one pair loop is live at a time)
+        // only one pair loop is live at a time).  The walk does not test a
+        // lane's hash-cell range [i-K-1, i+K+1]^3 per run: a vortex inside the
+        // lane's box, (K+0.5)h either side of a point of cell i, lies in that
+        // range whenever its hash cell differs from its coordinate by less
+        // than half a cell, which the rounding bound prune_cells < 1/4 (far
+        // beyond float rounding of the relative coordinates) guarantees;
+        // otherwise every lane takes its own walk below.
+        const float cr_lane = act ? cr : -1.0f;
         auto uniform_walk = [&](auto deg) {
             constexpr int D = decltype(deg)::value;
+            const float2 *cfd = D == 0 ? sc.p5 : (D == 7 ? sc.p7 : sc.p4);
+            Ring ring;
             for (int k2 = ulo[2]; k2 <= uhi[2]; k2++)
                 for (int j2 = ulo[1]; j2 <= uhi[1]; j2++)
                     for (int i2 = ulo[0]; i2 <= uhi[0];) {
@@ -501,15 +571,14 @@ __device__ __forceinline__ void eval_points(const SmoothSeries &sc, const EvalAr
                         }
                         i2 += both ? 2 : 1;
                         if (ps == kEmpty) continue;
-                        const bool lane_ok = act && ci >= rlo[0] && ci <= rhi[0] && cj >= rlo[1] && cj <= rhi[1] &&
-                                             ck >= rlo[2] && ck <= rhi[2];
-                        cell_pairs_packed<SEG, COUNT, FOLD, D>(
-                            vrec, valf, ps, pe, lane_ok ? cr : -1.0f, ra, rb, o, blo, bhi, inv_a3_2,
-                            D == 0 ? sc.p5 : (D == 7 ? sc.p7 : sc.p4), sc.t7, inv4pia3, D == 7 && need_exp2, pk,
-                            lane, acc2, xf);
+                        stage_run<SEG, COUNT, FOLD, D>(vrec, valf, ps, pe, cr_lane, ra, rb, o, blo, bhi, inv_a3_2,
+                                                       cfd, sc.t7, inv4pia3, D == 7 && need_exp2, pk, lane, ring,
+                                                       acc2, xf);
                     }
+            finish_ring<SEG, COUNT, FOLD, D>(cr_lane, ra, rb, inv_a3_2, cfd, sc.t7, inv4pia3, D == 7 && need_exp2, pk,
+                                             lane, ring, acc2, xf);
         };
-        if (vol > 0 && vol <= kUniformMaxSub) {
+        if (vol > 0 && vol <= kUniformMaxSub && P->prune_cells < 0.25) {
             if (tier0) uniform_walk(std::integral_constant<int, 0>{});
             else if (tier7) uniform_walk(std::integral_constant<int, 7>{});
             else uniform_walk(std::integral_constant<int, 4>{});
