@@ -182,6 +182,7 @@ constexpr uint32_t kBlockRecs = 32;  // records per block of the pair loop
 struct Ring {
     uint32_t fill = 0;  // records staged so far
     uint32_t head = 0;  // records evaluated so far (a multiple of kBlockRecs)
+    bool near = false;  // a waiting record may lie within a / 4 of a lane (exp form)
 };
 
 // max(|a|, |b|, |c|) in one instruction: the three-input max.abs of PTX ISA 8.8
@@ -253,9 +254,10 @@ __device__ __forceinline__ void stage_record(float *__restrict__ pk, int slot, i
 // the pair's (ra - r_p) is zero.  SEG keeps the other-end test.  phi is the
 // degree-DEG polynomial cf (DEG 4: the scene never leaves [0, 0.25]; DEG 7:
 // valid on [0, 2], the exp form above tbig when need_exp; DEG 0: the exp form,
-// the polynomial only for small t).  FOLD: the coefficients carry the powers
-// of 1/a^3, so the polynomial takes r^3 directly and tbig is in r^3 too.
-template <bool SEG, bool COUNT, bool FOLD, int DEG, bool FULL>
+// the polynomial only for small t, looked for only when CHECK).  FOLD: the
+// coefficients carry the powers of 1/a^3, so the polynomial takes r^3
+// directly and tbig is in r^3 too.
+template <bool SEG, bool COUNT, bool FOLD, int DEG, bool FULL, bool CHECK>
 __device__ __forceinline__ void pair_slots(const float4 *__restrict__ pk4, uint32_t s0, uint32_t np, float cr_lane,
                                            const float3 ra, const float3 rb, float2 inv_a3, const float2 *cf,
                                            float tbig, float inv4pia3, bool need_exp, PairAcc2 &acc,
@@ -300,7 +302,7 @@ __device__ __forceinline__ void pair_slots(const float4 *__restrict__ pk4, uint3
             // the trigger r^3 < r3small is a superset of t < tsmall, and
             // a lane outside its box may trigger it (its coefficient is
             // dropped below either way)
-            if (__any_sync(0xffffffffu, fminf(r3.x, r3.y) < xf.r3small)) {
+            if (CHECK && __any_sync(0xffffffffu, fminf(r3.x, r3.y) < xf.r3small)) {
                 const float2 t = __fmul2_rn(r3, xf.inv_a3);
                 float2 p = __ffma2_rn(cf[5], t, cf[4]);
 #pragma unroll
@@ -326,7 +328,12 @@ __device__ __forceinline__ void pair_slots(const float4 *__restrict__ pk4, uint3
                 }
             }
         }
-        const float2 coeff = make_float2(ok0 ? c.x : 0.0f, ok1 ? c.y : 0.0f);
+        // the exp form's c is finite for every pair of an active lane (r = 0
+        // lies inside the box and takes the polynomial), so the box mask can
+        // multiply it; the polynomials can overflow on the padding record
+        const float2 coeff = (DEG == 0 && !SEG && !COUNT)
+                                 ? __fmul2_rn(c, make_float2(ok0 ? 1.0f : 0.0f, ok1 ? 1.0f : 0.0f))
+                                 : make_float2(ok0 ? c.x : 0.0f, ok1 ? c.y : 0.0f);
         acc.ax = __ffma2_rn(coeff, make_float2(B.z, B.w), acc.ax);
         acc.ay = __ffma2_rn(coeff, make_float2(Cc.x, Cc.y), acc.ay);
         acc.az = __ffma2_rn(coeff, make_float2(Cc.z, Cc.w), acc.az);
@@ -342,13 +349,19 @@ __device__ __forceinline__ void pair_slots(const float4 *__restrict__ pk4, uint3
 // test and are dropped.  Whenever 32 records wait, the warp evaluates them.
 // The ring never overwrites a record still waiting: before a chunk fewer than
 // 32 wait, a chunk adds at most 32, and the ring holds 64.
+// Exp form: a record farther than dnear inside the warp's box [blo, bhi] on
+// some axis is more than a / 4 (with a margin) from every lane's point, so no
+// pair with it needs the small-t polynomial; a block of 32 records with no
+// other record skips the warp's test for it.  The records still waiting after
+// a block all come from the chunk just staged (fewer than 32 waited before
+// it), so that chunk's flag carries over.
 template <bool SEG, bool COUNT, bool FOLD, int DEG>
 __device__ __forceinline__ void stage_run(const float4 *__restrict__ vrec, const float4 *__restrict__ valf,
                                           uint32_t ps, uint32_t pe, float cr_lane, const float3 ra,
                                           const float3 rb, float3 o, const float3 blo, const float3 bhi,
-                                          float2 inv_a3, const float2 *cf, float tbig, float inv4pia3,
-                                          bool need_exp, float4 *__restrict__ pk4, int lane, Ring &ring,
-                                          PairAcc2 &acc, const ExpForm &xf) {
+                                          float dnear, float2 inv_a3, const float2 *cf, float tbig,
+                                          float inv4pia3, bool need_exp, float4 *__restrict__ pk4, int lane,
+                                          Ring &ring, PairAcc2 &acc, const ExpForm &xf) {
     float *pk = reinterpret_cast<float *>(pk4);
     for (uint32_t base = ps; base < pe; base += 32) {
         const uint32_t cnt = min(32u, pe - base);
@@ -360,16 +373,29 @@ __device__ __forceinline__ void stage_run(const float4 *__restrict__ vrec, const
         }
         const unsigned kept = __ballot_sync(0xffffffffu, keep);
         if (kept == 0u) continue;
+        bool near_chunk = true;
+        if (DEG == 0) {
+            const bool nr = keep && r.x >= blo.x + dnear && r.x <= bhi.x - dnear && r.y >= blo.y + dnear &&
+                            r.y <= bhi.y - dnear && r.z >= blo.z + dnear && r.z <= bhi.z - dnear;
+            near_chunk = __any_sync(0xffffffffu, nr);
+        }
         if (keep) {
             const uint32_t dst = ring.fill + (uint32_t)__popc(kept & ((1u << lane) - 1u));
             stage_record(pk, (int)((dst >> 1) & (kPackSlots - 1)), (int)(dst & 1u), r, valf[base + lane], o);
         }
         ring.fill += (uint32_t)__popc(kept);
+        ring.near = ring.near || near_chunk;
         if (ring.fill - ring.head >= kBlockRecs) {
             __syncwarp();
-            pair_slots<SEG, COUNT, FOLD, DEG, true>(pk4, (ring.head >> 1) & (kPackSlots - 1), 0, cr_lane, ra, rb,
-                                                    inv_a3, cf, tbig, inv4pia3, need_exp, acc, xf);
+            const uint32_t s0 = (ring.head >> 1) & (kPackSlots - 1);
+            if (DEG != 0 || ring.near)
+                pair_slots<SEG, COUNT, FOLD, DEG, true, true>(pk4, s0, 0, cr_lane, ra, rb, inv_a3, cf, tbig,
+                                                              inv4pia3, need_exp, acc, xf);
+            else
+                pair_slots<SEG, COUNT, FOLD, DEG, true, false>(pk4, s0, 0, cr_lane, ra, rb, inv_a3, cf, tbig,
+                                                               inv4pia3, need_exp, acc, xf);
             ring.head += kBlockRecs;
+            ring.near = near_chunk && ring.fill != ring.head;
             __syncwarp();  // the next records may take the slots just read
         }
     }
@@ -390,8 +416,8 @@ __device__ __forceinline__ void finish_ring(float cr_lane, const float3 ra, cons
                      make_float4(-1e18f, -1e18f, -1e18f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f),
                      make_float3(0.f, 0.f, 0.f));
     __syncwarp();
-    pair_slots<SEG, COUNT, FOLD, DEG, false>(pk4, (ring.head >> 1) & (kPackSlots - 1), (rem + 1) >> 1, cr_lane, ra,
-                                             rb, inv_a3, cf, tbig, inv4pia3, need_exp, acc, xf);
+    pair_slots<SEG, COUNT, FOLD, DEG, false, true>(pk4, (ring.head >> 1) & (kPackSlots - 1), (rem + 1) >> 1, cr_lane,
+                                                   ra, rb, inv_a3, cf, tbig, inv4pia3, need_exp, acc, xf);
     __syncwarp();
 }
 
@@ -548,6 +574,9 @@ __device__ __forceinline__ void eval_points(const SmoothSeries &sc, const EvalAr
         // beyond float rounding of the relative coordinates) guarantees;
         // otherwise every lane takes its own walk below.
         const float cr_lane = act ? cr : -1.0f;
+        // exp form: records inside [blo + dnear, bhi - dnear] may lie within
+        // a / 4 of a lane (1 % margin on a / 4, far above the trigger's)
+        const float dnear = cr - (float)(0.2525 * P->a);
         auto uniform_walk = [&](auto deg) {
             constexpr int D = decltype(deg)::value;
             const float2 *cfd = D == 0 ? sc.p5 : (D == 7 ? sc.p7 : sc.p4);
@@ -571,9 +600,9 @@ __device__ __forceinline__ void eval_points(const SmoothSeries &sc, const EvalAr
                         }
                         i2 += both ? 2 : 1;
                         if (ps == kEmpty) continue;
-                        stage_run<SEG, COUNT, FOLD, D>(vrec, valf, ps, pe, cr_lane, ra, rb, o, blo, bhi, inv_a3_2,
-                                                       cfd, sc.t7, inv4pia3, D == 7 && need_exp2, pk, lane, ring,
-                                                       acc2, xf);
+                        stage_run<SEG, COUNT, FOLD, D>(vrec, valf, ps, pe, cr_lane, ra, rb, o, blo, bhi, dnear,
+                                                       inv_a3_2, cfd, sc.t7, inv4pia3, D == 7 && need_exp2, pk, lane,
+                                                       ring, acc2, xf);
                     }
             finish_ring<SEG, COUNT, FOLD, D>(cr_lane, ra, rb, inv_a3_2, cfd, sc.t7, inv4pia3, D == 7 && need_exp2, pk,
                                              lane, ring, acc2, xf);
