@@ -690,9 +690,9 @@ size_t mg_tune_report(char *buf, size_t cap) {
         put("edge %d comps %d: chosen %d; ms per 8 half sweeps: plain %.4f", t.key.d, t.key.comps, t.variant,
             (double)t.ms[0]);
         for (int v = 0; v + 1 < 16 && v < tb_variant_count(); v++) {
-            int T = 0, TX = 0, TY = 0;
-            tb_variant_shape(v, &T, &TX, &TY);
-            put(", v%d(T%d %dx%d) %.4f", v, T, TX, TY, (double)t.ms[v + 1]);
+            int T = 0, TX = 0, TY = 0, G4 = 0;
+            tb_variant_shape(v, &T, &TX, &TY, &G4);
+            put(", v%d(T%d %dx%d%s) %.4f", v, T, TX, TY, G4 ? " g4" : "", (double)t.ms[v + 1]);
         }
         put("\n");
     }

@@ -102,7 +102,15 @@ struct TbShape {
     static_assert(T % 2 == 0, "whole red-black iterations only");
 };
 
-template <int T, int TX, int TY, int NT, int PF, bool BG>
+// G4: a thread takes a group of 4 consecutive cells of a row (a 16-byte word of
+// the slot) and, in a half sweep, updates the 2 of them that have the sweep's
+// colour, reading its own row, the rows above and below and the planes before
+// and after with 128-bit shared loads (conflict free) plus one scalar either
+// side; the group is written back whole, the other colour's cells with the
+// values just read (no other thread writes them in that half sweep, and the
+// half sweep's readers of them read the same value either way).  Otherwise a
+// thread takes a pair of cells and updates the one of the sweep's colour.
+template <int T, int TX, int TY, int NT, int PF, bool BG, bool G4>
 __global__ void __launch_bounds__(NT)
 tb_smooth_kernel(const __grid_constant__ CUtensorMap map_x, const __grid_constant__ CUtensorMap map_b,
                  int load_x, const float *__restrict__ xc, float *__restrict__ x_out, int d, int zchunk,
@@ -137,8 +145,10 @@ tb_smooth_kernel(const __grid_constant__ CUtensorMap map_x, const __grid_constan
     }
     __syncthreads();
 
-    // this thread's (row, pair) slots of the box, the same for every half sweep
-    constexpr int PAIRS = BX / 2;
+    // this thread's (row, pair) or (row, group of 4) slots of the box, the same
+    // for every half sweep
+    static_assert(!G4 || (!BG && BX % 4 == 0), "groups of 4 need b in the ring and whole words");
+    constexpr int PAIRS = G4 ? BX / 4 : BX / 2;
     constexpr int ITEMS = (BY * PAIRS + NT - 1) / NT;
     int it_sy[ITEMS], it_px[ITEMS];
 #pragma unroll
@@ -213,6 +223,49 @@ tb_smooth_kernel(const __grid_constant__ CUtensorMap map_x, const __grid_constan
                 const float *Bg = BG ? bgc + (size_t)p * d * d : nullptr;
                 const int ya = max(0, y0 - T + t), yb = min(d, y0 + TY + T - t);
                 const int xa = max(0, x0 - T + t), xb = min(d, x0 + TX + T - t);
+                if constexpr (G4) {
+#pragma unroll
+                    for (int i = 0; i < ITEMS; i++) {
+                        const int sy = it_sy[i];
+                        const int gy = y0 - T + sy;
+                        // rows outside [ya, yb) include the box's first and
+                        // last, so the rows above and below stay in the slot
+                        if (sy < 0 || gy < ya || gy >= yb) continue;
+                        const int sx = 4 * it_px[i];
+                        const int gx = x0 - H + sx;  // a multiple of 4
+                        const int a = (c - gy - p) & 1;  // the colour's cells: sx + a, sx + a + 2
+                        const bool m_lo = gx + a >= xa && gx + a < xb;
+                        const bool m_hi = gx + a + 2 >= xa && gx + a + 2 < xb;
+                        if (!m_lo && !m_hi) continue;
+                        const int o = sy * BX + sx;
+                        const float4 v = *reinterpret_cast<const float4 *>(X + o);
+                        const float4 un = *reinterpret_cast<const float4 *>(X + o + BX);
+                        const float4 dn = *reinterpret_cast<const float4 *>(X + o - BX);
+                        const float4 zm = *reinterpret_cast<const float4 *>(Xm + o);
+                        const float4 zp = *reinterpret_cast<const float4 *>(Xp + o);
+                        const float4 bb = *reinterpret_cast<const float4 *>(B + o);
+                        const float xl = sx > 0 ? X[o - 1] : 0.0f;
+                        const float xr = sx + 4 < BX ? X[o + 4] : 0.0f;
+                        const bool odd = a != 0;
+                        // the same sums in the same order as one cell of the
+                        // pair mapping (left + right) + (y+1 + y-1) + (z-1 + z+1)
+                        const float nb_lo = (((odd ? v.x : xl) + (odd ? v.z : v.y)) + ((odd ? un.y : un.x) + (odd ? dn.y : dn.x))) +
+                                            ((odd ? zm.y : zm.x) + (odd ? zp.y : zp.x));
+                        const float nb_hi = (((odd ? v.z : v.y) + (odd ? xr : v.w)) + ((odd ? un.w : un.z) + (odd ? dn.w : dn.z))) +
+                                            ((odd ? zm.w : zm.z) + (odd ? zp.w : zp.z));
+                        const float n_lo = sor(odd ? v.y : v.x, nb_lo, odd ? bb.y : bb.x);
+                        const float n_hi = sor(odd ? v.w : v.z, nb_hi, odd ? bb.w : bb.z);
+                        float4 w = v;
+                        if (odd) {
+                            if (m_lo) w.y = n_lo;
+                            if (m_hi) w.w = n_hi;
+                        } else {
+                            if (m_lo) w.x = n_lo;
+                            if (m_hi) w.z = n_hi;
+                        }
+                        *reinterpret_cast<float4 *>(X + o) = w;
+                    }
+                } else {
 #pragma unroll
                 for (int i = 0; i < ITEMS; i++) {
                     const int sy = it_sy[i];
@@ -224,6 +277,7 @@ tb_smooth_kernel(const __grid_constant__ CUtensorMap map_x, const __grid_constan
                     const int o = sy * BX + sx;
                     const float nb = ((X[o - 1] + X[o + 1]) + (X[o + BX] + X[o - BX])) + (Xm[o] + Xp[o]);
                     X[o] = sor(X[o], nb, BG ? __ldg(Bg + (size_t)gy * d + gx) : B[o]);
+                }
                 }
             }
             if (t == T) fence_proxy_async();
@@ -278,15 +332,15 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 // The configurations built; TbConfig::variant indexes this table.
 struct TbVariant {
     int T, TX, TY, NT, PF;
-    bool BG;
+    bool BG, G4;
     size_t smem;
     const void *kernel;
 };
 
-template <int T, int TX, int TY, int NT, int PF, bool BG>
+template <int T, int TX, int TY, int NT, int PF, bool BG, bool G4 = false>
 TbVariant make_variant() {
-    return TbVariant{T, TX, TY, NT, PF, BG, TbShape<T, TX, TY, PF, BG>::SMEM,
-                     (const void *)tb_smooth_kernel<T, TX, TY, NT, PF, BG>};
+    return TbVariant{T, TX, TY, NT, PF, BG, G4, TbShape<T, TX, TY, PF, BG>::SMEM,
+                     (const void *)tb_smooth_kernel<T, TX, TY, NT, PF, BG, G4>};
 }
 
 const TbVariant *variants(int *count) {
@@ -298,6 +352,11 @@ const TbVariant *variants(int *count) {
         make_variant<2, 64, 16, 384, 4, false>(),
         make_variant<2, 128, 32, 1024, 1, false>(),
         make_variant<4, 64, 16, 384, 4, false>(),
+        // groups of 4 cells per thread (one item per thread, or two for 128 x 32)
+        make_variant<2, 64, 16, 384, 4, false, true>(),
+        make_variant<2, 128, 16, 704, 1, false, true>(),
+        make_variant<2, 128, 32, 640, 1, false, true>(),
+        make_variant<4, 64, 16, 448, 4, false, true>(),
     };
     *count = (int)(sizeof(v) / sizeof(v[0]));
     return v;
@@ -311,13 +370,14 @@ int tb_variant_count() {
     return c;
 }
 
-void tb_variant_shape(int variant, int *T, int *TX, int *TY) {
+void tb_variant_shape(int variant, int *T, int *TX, int *TY, int *G4) {
     int c = 0;
     const TbVariant *v = variants(&c);
     const TbVariant &w = v[(variant >= 0 && variant < c) ? variant : 0];
     *T = w.T;
     *TX = w.TX;
     *TY = w.TY;
+    if (G4) *G4 = w.G4 ? 1 : 0;
 }
 
 // 4-D tensor map {d, d, d, comps} of FP32 over `base`, box {BX, BY, 1, 1}.

@@ -69,7 +69,7 @@ struct Level {
 // Temporally blocked smoother (mg_tb.cu): T half sweeps per pass over a level.
 constexpr uint32_t kTbErrTimeout = 0x7B000001u;  // an mbarrier wait ran out
 int tb_variant_count();
-void tb_variant_shape(int variant, int *T, int *TX, int *TY);
+void tb_variant_shape(int variant, int *T, int *TX, int *TY, int *G4 = nullptr);  // G4: groups of 4 cells
 cudaError_t tb_make_map(CUtensorMap *map, float *base, int d, int comps, int variant);
 cudaError_t tb_prepare(int variant, int *blocks_per_sm);
 cudaError_t tb_smooth(int variant, const CUtensorMap &map_x, const CUtensorMap &map_b, const float *b_dev, int load_x,
