@@ -899,6 +899,41 @@ def plume_cpu_rate(N: int, n: int, radius: float):
                       f"{Ns:,} particles on {ns}^3 ({sec:.1f} s): the same particles per cell"}
 
 
+def plume_scale_check(scene, pos, al, temp, n, sample=4096):
+    """The first plume step at full scale against the oracle, untimed: the
+    baroclinic source of every particle (orc_baroclinic), and the velocity
+    (self pair excluded) at `sample` particles with the oracle's FP64 PPPM at
+    the same multigrid tolerance (orc_pppm) for the vortices after that
+    source.  The rest of the step (segments, stretching, smoothing) is
+    checked against the oracle on smaller plumes by the tests."""
+    import torch
+    from oracle import pyoracle as O
+    O.build()
+    N = len(pos)
+    dpos = torch.from_numpy(pos).cuda()
+    dal = torch.from_numpy(np.ascontiguousarray(al.T)).cuda()
+    dtemp = torch.from_numpy(temp.astype(np.float32)).cuda()
+    scene.baroclinic(dpos, dtemp, dpos, dal, PLUME_DT)
+    al1 = dal.cpu().numpy().T.copy()
+    ref1 = O.baroclinic(pos, temp.astype(np.float32), pos, al, PLUME_DT, cap=0)[0]
+    rng = np.random.default_rng(11)
+    sub = np.ascontiguousarray(pos[np.sort(rng.choice(N, min(sample, N), replace=False))])
+    scene.set_vortices(dpos, dal)
+    scene.build_far_field()
+    dsub = torch.from_numpy(sub).cuda()
+    u = scene.eval(dsub, dsub, 1).cpu().numpy()
+    uref, d = O.pppm(O.params(n, mg_mode=1, mg_tol=1e-10), pos, al1, sub, sub, 1, dump=True)
+
+    def rel(a, b):
+        return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+    return {"baroclinic_rel_l2_all_particles": rel(al1, ref1), "velocity_rel_l2": rel(u, uref),
+            "velocity_points": int(len(sub)), "oracle_mg_cycles": [int(c) for c in d["mg_cycles"]],
+            "what": "step 1 from the initial state: baroclinic source of every particle vs orc_baroclinic; "
+                    "velocity at the sampled particles vs orc_pppm (FP64, multigrid to 1e-10) for the "
+                    "vortices after that source"}
+
+
 def run_plume(args, world, rank, local):
     """Buoyant plume time steps: N particles uniform in a sphere at
     (0.5, 0.15, 0.5) carrying a temperature N(1, 0.05^2) and no vorticity
@@ -930,6 +965,12 @@ def run_plume(args, world, rank, local):
     dpos, dal = pos0.clone(), al0.clone()
     dtemp = torch.from_numpy(temp.astype(np.float32)).cuda()
     stream = torch.cuda.current_stream()
+    check = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            check = plume_scale_check(scene, pos, al, temp, n)
+        except Exception as exc:  # reported, not fatal
+            check = {"failed": str(exc)}
     warm = max(args.warmup, 3)
     for _ in range(warm):
         scene.solve_time_step(dpos, dal, PLUME_DT, dtemp)
@@ -998,6 +1039,7 @@ def run_plume(args, world, rank, local):
             "step1_baroclinic_ms": ms_baro[0],
             "baroclinic_ms": statistics.median(ms_baro), "vortex_step_stages_ms": st,
             "mg_cycles_last": mg["mg_cycles"], "mg_relres_last": mg["mg_relres"],
+            "step1_vs_oracle": check,
             "state_after": {"steps": args.steps, "mean_y": float(p[:, 1].astype(np.float64).mean()),
                             "alpha_rms": float(np.sqrt((a * a).sum(axis=0).mean())),
                             "finite": bool(np.isfinite(p).all() and np.isfinite(a).all())}}), flush=True)
