@@ -112,3 +112,35 @@ def test_plume_with_separate_heat_particles(pb, oracle):
     gc = dpos.cpu().numpy()
     assert rel_l2(gc[:, :3] - pos[:, :3], rc[:, :3].astype(np.float64) - pos[:, :3]) <= 1e-4
     scene.close()
+
+
+def test_plume_step_one_at_full_scale(pb, oracle):
+    """The configured plume (4,194,304 particles, 256^3, multigrid to 1e-10),
+    step 1 from the initial state: the baroclinic source of every particle
+    against orc_baroclinic, and the velocity at 2,048 sampled particles (self
+    pair excluded) against the oracle's FP64 PPPM for the vortices after that
+    source.  The segment step's remaining parts are covered above on the
+    smaller plume."""
+    import torch
+    from pppm_vortex_bouyant_flow_sample_b200 import workloads as W
+    N, n = 1 << 22, 256
+    pos, al, temp = W.plume_sphere(N, seed=3, radius=0.5)
+    scene = pb.Scene(n, cap_vort=N, cap_eval=N, mg="converged", mg_tol=1e-10, mg_max_cycles=50)
+    try:
+        dpos = torch.from_numpy(pos).cuda()
+        dal = torch.from_numpy(np.ascontiguousarray(al.T)).cuda()
+        scene.baroclinic(dpos, torch.from_numpy(temp.astype(np.float32)).cuda(), dpos, dal, DT)
+        al1 = dal.cpu().numpy().T.copy()
+        ref1 = oracle.baroclinic(pos, temp.astype(np.float32), pos, al, DT, cap=0)[0]
+        assert np.linalg.norm(ref1) > 0
+        assert rel_l2(al1, ref1) <= 1e-12
+        rng = np.random.default_rng(11)
+        sub = np.ascontiguousarray(pos[np.sort(rng.choice(N, 2048, replace=False))])
+        scene.set_vortices(dpos, dal)
+        scene.build_far_field()
+        dsub = torch.from_numpy(sub).cuda()
+        u = scene.eval(dsub, dsub, 1).cpu().numpy()
+    finally:
+        scene.close()
+    uref, _ = oracle.pppm(oracle.params(n, mg_mode=1, mg_tol=1e-10), pos, al1, sub, sub, 1)
+    assert rel_l2(u, uref) <= 1e-5
