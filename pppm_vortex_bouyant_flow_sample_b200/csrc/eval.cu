@@ -365,10 +365,13 @@ __device__ __forceinline__ void stage_run(const float4 *__restrict__ vrec, const
     float *pk = reinterpret_cast<float *>(pk4);
     for (uint32_t base = ps; base < pe; base += 32) {
         const uint32_t cnt = min(32u, pe - base);
+        // the strength is loaded with the position (one latency per chunk,
+        // not two), also for records the box test then drops
         bool keep = false;
-        float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+        float4 r = make_float4(0.f, 0.f, 0.f, 0.f), al = r;
         if ((uint32_t)lane < cnt) {
             r = vrec[base + lane];
+            al = valf[base + lane];
             keep = r.x >= blo.x && r.x <= bhi.x && r.y >= blo.y && r.y <= bhi.y && r.z >= blo.z && r.z <= bhi.z;
         }
         const unsigned kept = __ballot_sync(0xffffffffu, keep);
@@ -381,7 +384,7 @@ __device__ __forceinline__ void stage_run(const float4 *__restrict__ vrec, const
         }
         if (keep) {
             const uint32_t dst = ring.fill + (uint32_t)__popc(kept & ((1u << lane) - 1u));
-            stage_record(pk, (int)((dst >> 1) & (kPackSlots - 1)), (int)(dst & 1u), r, valf[base + lane], o);
+            stage_record(pk, (int)((dst >> 1) & (kPackSlots - 1)), (int)(dst & 1u), r, al, o);
         }
         ring.fill += (uint32_t)__popc(kept);
         ring.near = ring.near || near_chunk;
