@@ -622,6 +622,22 @@ def run_mix(args, world, rank, local):
     seq_ms = timed(sequential)
     bat_ms = timed(batched)
 
+    # untimed: the sequential path's stages summed over the scenes (CUDA
+    # events per stage), and the near-field pairs; the evaluations' share is
+    # work that batching cannot shorten, only overlap with other scenes' builds
+    stage_sum = {}
+    pairs_total = 0
+    for sc, (dpos, dal, out) in zip(scenes, data):
+        sc.set_profiling(True)
+        sc.set_vortices(dpos, dal)
+        sc.build_far_field()
+        sc.eval(dpos, dpos, 1, out=out)
+        for k, v in sc.stage_times().items():
+            if v >= 0:
+                stage_sum[k] = stage_sum.get(k, 0.0) + v
+        sc.set_profiling(False)
+        pairs_total += sc.count_pairs(dpos)
+
     # the plain path a caller without device buffers takes: each scene through
     # pppm_solve_host in turn (copies in, build, evaluate, copies out, sync)
     def host_sequential():
@@ -666,6 +682,8 @@ def run_mix(args, world, rank, local):
                        "parallelism": f"scenes split over {world} GPUs (whole scenes per rank)" if world > 1
                        else "one GPU"},
             "sequential_ms": seq_ms, "batched_ms": bat_ms, "batch_speedup": seq_ms / bat_ms,
+            "sequential_stage_sum_ms": {k: round(v, 3) for k, v in stage_sum.items()},
+            "near_field_pairs": pairs_total,
             "sequential_evals_per_s": total / (seq_ms / 1000.0),
             "host_sequential_ms": host_seq_ms, "speedup_vs_host_sequential": host_seq_ms / bat_ms,
             "err_vs_direct_fp64": (num / den) ** 0.5 if den > 0 else None,
