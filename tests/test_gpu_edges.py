@@ -142,6 +142,26 @@ def test_eval_points_outside_the_grid(pb, oracle):
     scene.close()
 
 
+def test_far_vortex_sends_every_lane_on_its_own_walk(pb, oracle):
+    """The warp-uniform walk drops a lane's hash-cell range test, which is
+    sound while the hash cells and the coordinates differ by far less than half
+    a cell (the build's rounding bound prune_cells < 1/4).  One vortex 20,000
+    units out in a fixed unit-cube domain on 32^3 lifts that bound to about
+    0.6, and every lane then walks its own cells; the result is the oracle's."""
+    from pppm_vortex_bouyant_flow_sample_b200 import workloads as W
+    pos, al = W.uniform_cloud(12000, seed=31)
+    pos[:, :3] = 0.1 + 0.8 * (pos[:, :3] - pos[:, :3].min(0)) / np.ptp(pos[:, :3], axis=0)
+    pos[0, :3] = (20000.0, 0.5, 0.5)
+    box = dict(domain_mode=1, fixed_origin=(0.0, 0.0, 0.0), fixed_length=1.0)
+    ev = np.ascontiguousarray(pos[1:])
+    scene, u = _velocity(pb, 32, pos, al, ev, ev, 1, domain="fixed", fixed_origin=(0.0, 0.0, 0.0),
+                         fixed_length=1.0)
+    ref, _ = oracle.pppm(oracle.params(32, **box), pos, al, ev, ev, 1, dump=True)
+    assert np.linalg.norm(ref) > 0
+    assert rel_l2(u, ref) <= VEL_TOL
+    scene.close()
+
+
 def test_grid_96(pb, oracle):
     from pppm_vortex_bouyant_flow_sample_b200 import workloads as W
     pos, al = W.vortex_ring(40000, seed=3)
