@@ -41,7 +41,7 @@ def _dev(a):
     return torch.from_numpy(np.ascontiguousarray(a)).cuda()
 
 
-def _gpu(pb, n, pos, al, ev, **kw):
+def _gpu(pb, n, pos, al, ev, pairs=None, **kw):
     scene = pb.Scene(n, cap_vort=len(pos), cap_eval=len(ev), **kw)
     dpos, dal, dev = _dev(pos), _dev(al), _dev(ev)
     scene.set_vortices(dpos, dal)
@@ -49,6 +49,8 @@ def _gpu(pb, n, pos, al, ev, **kw):
     u = scene.eval(dev, dev, 1).cpu().numpy()
     a = scene.smoothing()
     (o, L, h) = scene.domain()
+    if pairs is not None:
+        pairs.append(scene.count_pairs(dev))
     ds = pb.direct_sum_fp64(dpos, dal, dev, a, dev, 1).cpu().numpy()
     scene.close()
     return u, ds, a, h
@@ -92,9 +94,11 @@ def test_ring_128_radius_one_cell(pb, oracle, preset, bound):
     else:
         kw = dict(K=1, a_cells=1.0)
         okw = dict(K=1, mg_mode=0)
-    u, ds, a, h = _gpu(pb, n, pos, al, sub, **kw)
+    pairs = []
+    u, ds, a, h = _gpu(pb, n, pos, al, sub, pairs=pairs, **kw)
     assert a == h
-    ref = oracle.pppm(oracle.params(n, a=a, **okw), pos, al, sub, sub, 1)[0]
+    ref, d = oracle.pppm(oracle.params(n, a=a, **okw), pos, al, sub, sub, 1, dump=True)
+    assert pairs[0] == int(d["pairs"][0])
     assert rel_l2(u, ref) <= VEL_TOL
     err, err_ref = rel_l2(u, ds), rel_l2(ref, ds)
     assert abs(err - err_ref) <= 1e-3 * err_ref
@@ -141,4 +145,30 @@ def test_exp_form_accuracy_pair_by_pair(pb, oracle):
                       pos, al, ev, None, 0)[0]
     err = np.linalg.norm(u - ref, axis=1) / np.linalg.norm(ref, axis=1)
     assert err.max() <= 5e-6, (float(err.max()), float(t[np.argmax(err) % len(t)]))
+    assert rel_l2(u, ref) <= VEL_TOL
+
+
+def test_segments_radius_one_cell(pb, oracle):
+    """Segment evaluation (is_segment = 1 with distinct other ends, the time
+    step's form) at a radius of one cell: a pair counts only where both ends
+    are apart from the vortex, as in the oracle."""
+    import torch
+    from pppm_vortex_bouyant_flow_sample_b200 import workloads as W
+    pos, al = W.vortex_ring(60000, seed=12)
+    rng = np.random.default_rng(13)
+    ea = np.ascontiguousarray(pos[::3])
+    eb = ea.copy()
+    eb[:, :3] += rng.normal(0, 0.01, (len(eb), 3)).astype(np.float32)
+    eb[::7] = pos[1::21][: len(eb[::7])]   # some other ends on vortices
+    n = 64
+    scene = pb.Scene(n, cap_vort=len(pos), cap_eval=len(ea), a_cells=1.0)
+    try:
+        scene.set_vortices(_dev(pos), _dev(al))
+        scene.build_far_field()
+        a = scene.smoothing()
+        u = scene.eval(_dev(ea), _dev(eb), 1).cpu().numpy()
+    finally:
+        scene.close()
+    ref = oracle.pppm(oracle.params(n, a=a), pos, al, ea, eb, 1)[0]
+    assert np.linalg.norm(ref) > 0
     assert rel_l2(u, ref) <= VEL_TOL
