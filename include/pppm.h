@@ -240,15 +240,16 @@ const char *pppm_stage_name(int stage);
 pppm_status pppm_get_stage_times(pppm_scene *s, double *ms, int cap, int *count);
 /* Number of kernels this library has launched in the process so far. */
 uint64_t pppm_kernel_launches(void);
-/* The multigrid smoother's autotuner (no reference counterpart): each level
- * of edge >= 256 runs either the plain red-black half sweeps or one of the
- * temporally blocked variants (T half sweeps per pass, TX x TY tiles, TMA
- * plane staging), whichever measured fastest for that edge and component
- * count on this device the first time a scene or multigrid object needed it
- * (every choice gives the same values bit for bit).  The environment variable
- * PPPM_MG_TB forces one variant (an index, or -1 for the plain sweeps).
- * Writes a text table of the measurements, one line per edge, into buf
- * (NUL-terminated, truncated to cap); *written receives its length. */
+/* The multigrid smoother's autotuner (no reference counterpart).  By default
+ * every level runs the plain red-black half sweeps.  With PPPM_MG_TB=auto in
+ * the environment when a scene or multigrid object is created, each level of
+ * edge >= 256 runs either the plain half sweeps or one of the temporally
+ * blocked variants (T half sweeps per pass, TX x TY tiles, TMA plane
+ * staging), whichever measured fastest for that edge and component count on
+ * this device; PPPM_MG_TB=<index> forces one variant.  Every choice gives the
+ * same values bit for bit.  Writes a text table of the autotuner's
+ * measurements, one line per edge, into buf (NUL-terminated, truncated to
+ * cap; empty when it has not run); *written receives its length. */
 pppm_status pppm_tuning_report(char *buf, size_t cap, size_t *written);
 
 /* ---- several independent scenes in one call -----------------------------

@@ -22,6 +22,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstdio>
+#include <cstring>
 #include <mutex>
 
 #include "pppm_internal.cuh"
@@ -79,6 +80,14 @@ __device__ __forceinline__ void split3(uint32_t t, int a, int d, int la, int ld,
     }
 }
 
+// The SOR update of one cell from its neighbour sum and right-hand side
+// (MG/MultiGrid_kernel.cu:766, omega = 1.43f), one expression for every
+// smoother kernel so that they round alike.
+__device__ __forceinline__ float sor_update(float x, float nb, float b) {
+    const float r = nb - b;
+    return kOneMinusOmegaF * x + (kOmegaF * r) * (1.0f / 6.0f);
+}
+
 // One half sweep over the cells with (i+j+k) % 2 == color.
 __global__ void __launch_bounds__(kMGThreads)
 rbsor_kernel(float *__restrict__ x, const float *__restrict__ b, int d, int color, int ld) {
@@ -94,8 +103,48 @@ rbsor_kernel(float *__restrict__ x, const float *__restrict__ b, int d, int colo
     split3(t, half, d, ld > 0 ? ld - 1 : -1, ld, ih, j, k);
     const int i = 2 * ih + ((j + k + color) & 1);
     const size_t c = ((size_t)k * d + j) * d + i;
-    const float r = nb_sum(xc, i, j, k, d, c) - bc[c];
-    xc[c] = kOneMinusOmegaF * xc[c] + (kOmegaF * r) * (1.0f / 6.0f);
+    xc[c] = sor_update(xc[c], nb_sum(xc, i, j, k, d, c), bc[c]);
+}
+
+__device__ __forceinline__ float4 ld4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+
+// The same half sweep with a thread per group of 4 consecutive cells of a
+// row (edge a multiple of 4): it updates the group's 2 cells of the colour
+// from 128-bit loads of its row, the rows and planes either side and b, plus
+// one scalar either side, with nb_sum's terms in nb_sum's order (the values
+// equal rbsor_kernel's bit for bit).  Half the threads of rbsor_kernel, and
+// every loaded sector fully used.
+__global__ void __launch_bounds__(kMGThreads)
+rbsor4_kernel(float *__restrict__ x, const float *__restrict__ b, int d, int color, int ld) {
+    const int q = d >> 2;  // groups per row
+    const uint32_t per = (uint32_t)q * d * d;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= per) return;
+    const size_t comp = blockIdx.y;
+    const size_t cells = (size_t)d * d * d, dd = (size_t)d * d;
+    float *xc = x + comp * cells;
+    const float *bc = b + comp * cells;
+    int g, j, k;
+    split3(t, q, d, ld >= 2 ? ld - 2 : -1, ld, g, j, k);
+    const int i0 = 4 * g;
+    const size_t c = ((size_t)k * d + j) * d + i0;
+    const bool odd = ((j + k + color) & 1) != 0;  // the colour's cells: i0 + odd, i0 + odd + 2
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 v = ld4(xc + c);
+    const float xl = i0 > 0 ? xc[c - 1] : 0.f;
+    const float xr = i0 + 4 < d ? xc[c + 4] : 0.f;
+    const float4 up = (j < d - 1) ? ld4(xc + c + d) : z4;
+    const float4 dn = (j > 0) ? ld4(xc + c - d) : z4;
+    const float4 fr = (k > 0) ? ld4(xc + c - dd) : z4;
+    const float4 bk = (k < d - 1) ? ld4(xc + c + dd) : z4;
+    const float4 bb = ld4(bc + c);
+    const float nb_lo = (((odd ? v.x : xl) + (odd ? v.z : v.y)) + ((odd ? up.y : up.x) + (odd ? dn.y : dn.x))) +
+                        ((odd ? fr.y : fr.x) + (odd ? bk.y : bk.x));
+    const float nb_hi = (((odd ? v.z : v.y) + (odd ? xr : v.w)) + ((odd ? up.w : up.z) + (odd ? dn.w : dn.z))) +
+                        ((odd ? fr.w : fr.z) + (odd ? bk.w : bk.z));
+    const int o = odd ? 1 : 0;
+    xc[c + o] = sor_update(odd ? v.y : v.x, nb_lo, odd ? bb.y : bb.x);
+    xc[c + o + 2] = sor_update(odd ? v.w : v.z, nb_hi, odd ? bb.w : bb.z);
 }
 
 // Residual at the fine level restricted to the coarse level in one pass:
@@ -351,12 +400,22 @@ static cudaError_t smooth(const MGPlan &m, int j, XAt in, const float *xc, XAt *
         ::pppm::note_launch();
         prolong_kernel<<<grid_for(L.cells, m.comps), kMGThreads, 0, m.st>>>(L.x, xc, d, edge_log2(d));
     }
-    const dim3 g = grid_for((uint32_t)(d / 2) * d * d, m.comps);
-    for (int it = 0; it < 4; it++) {
-        ::pppm::note_launch();
-        rbsor_kernel<<<g, kMGThreads, 0, m.st>>>(L.x, L.b, d, 1, edge_log2(d));
-        ::pppm::note_launch();
-        rbsor_kernel<<<g, kMGThreads, 0, m.st>>>(L.x, L.b, d, 0, edge_log2(d));
+    if ((d % 4) == 0) {
+        const dim3 g = grid_for((uint32_t)(d / 4) * d * d, m.comps);
+        for (int it = 0; it < 4; it++) {
+            ::pppm::note_launch();
+            rbsor4_kernel<<<g, kMGThreads, 0, m.st>>>(L.x, L.b, d, 1, edge_log2(d));
+            ::pppm::note_launch();
+            rbsor4_kernel<<<g, kMGThreads, 0, m.st>>>(L.x, L.b, d, 0, edge_log2(d));
+        }
+    } else {
+        const dim3 g = grid_for((uint32_t)(d / 2) * d * d, m.comps);
+        for (int it = 0; it < 4; it++) {
+            ::pppm::note_launch();
+            rbsor_kernel<<<g, kMGThreads, 0, m.st>>>(L.x, L.b, d, 1, edge_log2(d));
+            ::pppm::note_launch();
+            rbsor_kernel<<<g, kMGThreads, 0, m.st>>>(L.x, L.b, d, 0, edge_log2(d));
+        }
     }
     *out = kXMain;
     return cudaGetLastError();
@@ -620,7 +679,8 @@ cudaError_t mg_tb_setup(MGPlan &m, float *pool, int forced) {
         static std::once_flag once;
         static cudaError_t carve = cudaSuccess;
         std::call_once(once, [] {
-            const void *k[] = {(const void *)rbsor_kernel, (const void *)resid_restrict_kernel,
+            const void *k[] = {(const void *)rbsor_kernel, (const void *)rbsor4_kernel,
+                               (const void *)resid_restrict_kernel,
                                (const void *)prolong_kernel, (const void *)dc_residual_kernel,
                                (const void *)dc_update_kernel};
             for (const void *f : k)
@@ -699,13 +759,20 @@ size_t mg_tune_report(char *buf, size_t cap) {
     return w < cap ? w : cap;
 }
 
+// The plain half sweeps (rbsor4_kernel) measured faster inside a whole solve
+// than every blocked variant at 96^3 to 256^3 (256^3: 5.67 ms against 5.85 ms
+// with the autotuner's pick), and once a blocked pass has run, its large
+// shared-memory split slows the plain stencil kernels that follow.  So the
+// plain sweeps are the default; PPPM_MG_TB=auto runs the autotuner, an index
+// forces a variant.
 int mg_tb_default_variant() {
     const char *e = getenv("PPPM_MG_TB");
     if (e && *e) {
+        if (strcmp(e, "auto") == 0) return -2;
         const int v = atoi(e);
         return (v >= 0 && v < tb_variant_count()) ? v : -1;
     }
-    return -2;  // autotune
+    return -1;
 }
 
 static MGPlan scene_plan(pppm_scene *s) {

@@ -295,9 +295,9 @@ cudaError_t radix_sort_pairs(cudaStream_t st, uint32_t N, uint32_t bits, uint32_
                              uint32_t *hist, uint32_t **sorted_key, uint32_t **sorted_idx);
 
 int mg_level_count(uint32_t n);
-// Blocked-smoother choice for new multigrid objects: PPPM_MG_TB in the
-// environment (a variant index, or -1 for the plain half sweeps), else -2:
-// the autotuner picks per level.
+// Blocked-smoother choice for new multigrid objects: -1 (the plain half
+// sweeps) unless PPPM_MG_TB in the environment names a variant index, or
+// "auto" (-2: the autotuner picks per level).
 int mg_tb_default_variant();
 bool mg_shape_ok(uint32_t n);
 uint32_t key_bits(uint32_t n);

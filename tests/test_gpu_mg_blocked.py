@@ -2,7 +2,8 @@
 red-black half sweeps (MG/Multigrid.cu:202-239) T at a time; every variant
 must give the plain half sweeps' multigrid result bit for bit.  The blocked
 path serves levels of edge >= 256, so the scene is 256^3.  PPPM_MG_TB forces a
-variant (-1: the plain half sweeps) when a scene is created."""
+variant (-1: the plain half sweeps, the default) and "auto" runs the
+autotuner when a scene is created."""
 import re
 
 import numpy as np
@@ -35,12 +36,13 @@ def test_every_blocked_variant_matches_the_plain_half_sweeps(monkeypatch):
     pos, al = W.vortex_ring(1 << 16, seed=7)
     n = 256
     # a scene with the autotuner: its report lists every variant it timed
-    _psi(pb, n, pos, al, None, monkeypatch)
+    _psi(pb, n, pos, al, "auto", monkeypatch)
     report = pb.tuning_report()
     variants = sorted({int(v) for v in re.findall(r"v(\d+)\(", report)})
     assert variants == list(range(len(variants))) and len(variants) >= 4, report
     plain = _psi(pb, n, pos, al, -1, monkeypatch)
     assert np.isfinite(plain).all()
+    assert np.array_equal(_psi(pb, n, pos, al, None, monkeypatch), plain)  # the default
     for v in variants:
         got = _psi(pb, n, pos, al, v, monkeypatch)
         assert np.array_equal(got, plain), (v, float(np.abs(got - plain).max()))
