@@ -174,6 +174,61 @@ resid_restrict_kernel(const float *__restrict__ xf, const float *__restrict__ bf
     bc[comp * per + t] = sum * 0.5f;
 }
 
+// The same with a thread per pair of coarse cells along x (coarse edge even):
+// their 16 fine children, 4 consecutive cells in each of the 4 fine rows
+// (j, k) in {2jc, 2jc+1} x {2kc, 2kc+1}, read with 128-bit loads of the rows,
+// their neighbour rows and b.  The rows are taken in the children's order
+// (x fastest, then y, then z), so each coarse sum adds the same terms in the
+// same order as resid_restrict_kernel.
+__global__ void __launch_bounds__(kMGThreads)
+resid_restrict2_kernel(const float *__restrict__ xf, const float *__restrict__ bf, float *__restrict__ bc,
+                       int dc, int x_zero, int ldc) {
+    const int h = dc >> 1;  // coarse pairs per row
+    const uint32_t per2 = (uint32_t)h * dc * dc;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= per2) return;
+    const size_t comp = blockIdx.y;
+    const int df = 2 * dc;
+    const size_t fcells = (size_t)df * df * df, dd = (size_t)df * df;
+    const float *x = xf + comp * fcells;
+    const float *b = bf + comp * fcells;
+    int ip, jc, kc;
+    split3(t, h, dc, ldc >= 1 ? ldc - 1 : -1, ldc, ip, jc, kc);
+    const int i0 = 4 * ip;
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    float s0 = 0.f, s1 = 0.f;
+#pragma unroll
+    for (int rrow = 0; rrow < 4; rrow++) {
+        const int j = 2 * jc + (rrow & 1), k = 2 * kc + (rrow >> 1);
+        const size_t c = ((size_t)k * df + j) * df + i0;
+        const float4 bb = ld4(b + c);
+        float r[4] = {bb.x, bb.y, bb.z, bb.w};
+        if (!x_zero) {
+            const float4 v = ld4(x + c);
+            const float xl = i0 > 0 ? x[c - 1] : 0.f;
+            const float xr = i0 + 4 < df ? x[c + 4] : 0.f;
+            const float4 up = (j < df - 1) ? ld4(x + c + df) : z4;
+            const float4 dn = (j > 0) ? ld4(x + c - df) : z4;
+            const float4 fr = (k > 0) ? ld4(x + c - dd) : z4;
+            const float4 bk = (k < df - 1) ? ld4(x + c + dd) : z4;
+            const float xs[6] = {xl, v.x, v.y, v.z, v.w, xr};
+            const float us[4] = {up.x, up.y, up.z, up.w}, ds[4] = {dn.x, dn.y, dn.z, dn.w};
+            const float fs[4] = {fr.x, fr.y, fr.z, fr.w}, bs[4] = {bk.x, bk.y, bk.z, bk.w};
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const float nb = ((xs[e] + xs[e + 2]) + (us[e] + ds[e])) + (fs[e] + bs[e]);
+                r[e] -= nb - 6.f * xs[e + 1];
+            }
+        }
+        s0 += r[0];
+        s0 += r[1];
+        s1 += r[2];
+        s1 += r[3];
+    }
+    *reinterpret_cast<float2 *>(bc + comp * (size_t)dc * dc * dc + ((size_t)kc * dc + jc) * dc + 2 * ip) =
+        make_float2(s0 * 0.5f, s1 * 0.5f);
+}
+
 __global__ void __launch_bounds__(kMGThreads)
 prolong_kernel(float *__restrict__ xf, const float *__restrict__ xc, int df, int ldf) {
     const uint32_t per = (uint32_t)df * df * df;
@@ -184,6 +239,31 @@ prolong_kernel(float *__restrict__ xf, const float *__restrict__ xc, int df, int
     int i, j, k;
     split3(t, df, df, ldf, ldf, i, j, k);
     xf[comp * per + t] += xc[comp * (size_t)dc * dc * dc + ((size_t)(k >> 1) * dc + (j >> 1)) * dc + (i >> 1)];
+}
+
+// The same prolongation by injection with a thread per group of 4 fine cells
+// of a row (fine edge a multiple of 4): one 128-bit read-modify-write of the
+// fine cells and the 2 coarse cells under them (each cell gets the same single
+// addition as in prolong_kernel).
+__global__ void __launch_bounds__(kMGThreads)
+prolong4_kernel(float *__restrict__ xf, const float *__restrict__ xc, int df, int ldf) {
+    const int q = df >> 2;
+    const uint32_t per = (uint32_t)q * df * df;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= per) return;
+    const size_t comp = blockIdx.y;
+    const int dc = df >> 1;
+    int g, j, k;
+    split3(t, q, df, ldf >= 2 ? ldf - 2 : -1, ldf, g, j, k);
+    float4 *f = reinterpret_cast<float4 *>(xf + comp * (size_t)df * df * df + ((size_t)k * df + j) * df + 4 * g);
+    const float *cr = xc + comp * (size_t)dc * dc * dc + ((size_t)(k >> 1) * dc + (j >> 1)) * dc + 2 * g;
+    const float c0 = cr[0], c1 = cr[1];
+    float4 v = *f;
+    v.x += c0;
+    v.y += c0;
+    v.z += c1;
+    v.w += c1;
+    *f = v;
 }
 
 // Coarsest level: 100 Jacobi sweeps x <- (sum_nbr(x) - b) / 6 in FP64
@@ -367,6 +447,27 @@ static float *x_ptr(const MGPlan &m, int j, XAt at) { return at == kXAlt ? m.lv[
 // a pre-smoothing from zero ends in the main copy for an even pass count and
 // in the second copy for an odd one, a post-smoothing from there always ends
 // in the main copy.
+// bc = the restricted residual of the level above (a pair of coarse cells per
+// thread where the coarse edge is even).
+static void launch_restrict(const MGPlan &m, const float *xf, const float *bf, float *bc, int dc, int x_zero) {
+    if ((dc % 2) == 0)
+        resid_restrict2_kernel<<<grid_for((uint32_t)(dc / 2) * dc * dc, m.comps), kMGThreads, 0, m.st>>>(
+            xf, bf, bc, dc, x_zero, edge_log2(dc));
+    else
+        resid_restrict_kernel<<<grid_for((uint32_t)dc * dc * dc, m.comps), kMGThreads, 0, m.st>>>(
+            xf, bf, bc, dc, x_zero, edge_log2(dc));
+}
+
+// x += the coarser level's xc injected (a group of 4 cells per thread where
+// the edge allows).
+static void launch_prolong(const MGPlan &m, float *x, const float *xc, int d) {
+    if ((d % 4) == 0)
+        prolong4_kernel<<<grid_for((uint32_t)(d / 4) * d * d, m.comps), kMGThreads, 0, m.st>>>(x, xc, d,
+                                                                                                edge_log2(d));
+    else
+        prolong_kernel<<<grid_for((uint32_t)d * d * d, m.comps), kMGThreads, 0, m.st>>>(x, xc, d, edge_log2(d));
+}
+
 static cudaError_t smooth(const MGPlan &m, int j, XAt in, const float *xc, XAt *out) {
     const Level &L = m.lv[j];
     const int d = (int)L.d;
@@ -380,7 +481,7 @@ static cudaError_t smooth(const MGPlan &m, int j, XAt in, const float *xc, XAt *
             float *dst = x_ptr(m, j, at);
             if (in == kXZero) PPPM_CUDA_TRY(cudaMemsetAsync(dst, 0, sizeof(float) * m.comps * (size_t)L.cells, m.st));
             ::pppm::note_launch();
-            prolong_kernel<<<grid_for(L.cells, m.comps), kMGThreads, 0, m.st>>>(dst, xc, d, edge_log2(d));
+            launch_prolong(m, dst, xc, d);
             in = at;
             xc = nullptr;
         }
@@ -398,7 +499,7 @@ static cudaError_t smooth(const MGPlan &m, int j, XAt in, const float *xc, XAt *
     if (in == kXZero) PPPM_CUDA_TRY(cudaMemsetAsync(L.x, 0, sizeof(float) * m.comps * (size_t)L.cells, m.st));
     if (xc) {
         ::pppm::note_launch();
-        prolong_kernel<<<grid_for(L.cells, m.comps), kMGThreads, 0, m.st>>>(L.x, xc, d, edge_log2(d));
+        launch_prolong(m, L.x, xc, d);
     }
     if ((d % 4) == 0) {
         const dim3 g = grid_for((uint32_t)(d / 4) * d * d, m.comps);
@@ -432,8 +533,7 @@ static cudaError_t vcycle32(const MGPlan &m, int level, const float *xc = nullpt
     for (int j = level; j < L - 1; j++) {
         PPPM_CUDA_TRY(smooth(m, j, kXZero, j == level ? xc : nullptr, &at[j]));
         ::pppm::note_launch();
-        resid_restrict_kernel<<<grid_for(m.lv[j + 1].cells, m.comps), kMGThreads, 0, m.st>>>(
-            x_ptr(m, j, at[j]), m.lv[j].b, m.lv[j + 1].b, (int)m.lv[j + 1].d, 0, edge_log2((int)m.lv[j + 1].d));
+        launch_restrict(m, x_ptr(m, j, at[j]), m.lv[j].b, m.lv[j + 1].b, (int)m.lv[j + 1].d, 0);
     }
     // the coarsest solve starts from zero (a cycle on the coarsest level alone
     // included: it is only ever asked for from a zero start)
@@ -454,8 +554,7 @@ static cudaError_t fmg32(const MGPlan &m) {
     const int L = m.levels;
     for (int j = 0; j < L - 1; j++) {
         ::pppm::note_launch();
-        resid_restrict_kernel<<<grid_for(m.lv[j + 1].cells, m.comps), kMGThreads, 0, m.st>>>(
-            m.lv[j].x, m.lv[j].b, m.lv[j + 1].b, (int)m.lv[j + 1].d, 1, edge_log2((int)m.lv[j + 1].d));
+        launch_restrict(m, m.lv[j].x, m.lv[j].b, m.lv[j + 1].b, (int)m.lv[j + 1].d, 1);
     }
     PPPM_CUDA_TRY(cudaMemsetAsync(m.lv[L - 1].x, 0, sizeof(float) * m.comps * (size_t)m.lv[L - 1].cells, m.st));
     coarse_solve(m);
@@ -680,7 +779,8 @@ cudaError_t mg_tb_setup(MGPlan &m, float *pool, int forced) {
         static cudaError_t carve = cudaSuccess;
         std::call_once(once, [] {
             const void *k[] = {(const void *)rbsor_kernel, (const void *)rbsor4_kernel,
-                               (const void *)resid_restrict_kernel,
+                               (const void *)prolong4_kernel, (const void *)resid_restrict_kernel,
+                               (const void *)resid_restrict2_kernel,
                                (const void *)prolong_kernel, (const void *)dc_residual_kernel,
                                (const void *)dc_update_kernel};
             for (const void *f : k)
