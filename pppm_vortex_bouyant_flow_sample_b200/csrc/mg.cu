@@ -18,6 +18,12 @@
 // V(psi, b) in exact arithmetic because the V-cycle is a consistent linear
 // iteration.  The coarsest solve is FP64.  Every kernel handles the three
 // potential components of a scene in one launch (grid y = component).
+//
+// Where the level's edge allows, the half sweeps and the prolongation take a
+// group of 4 consecutive cells of a row per thread and the restriction a pair
+// of coarse cells, with 128-bit loads; their values equal the one-cell
+// kernels' bit for bit.  The temporally blocked smoother of mg_tb.cu is
+// opt-in (PPPM_MG_TB), as it measured slower inside a whole solve.
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>

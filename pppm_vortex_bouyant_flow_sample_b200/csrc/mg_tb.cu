@@ -1,5 +1,7 @@
 // Temporally blocked red-black SOR smoother for the multigrid levels that
-// stream from HBM or L2 (edge >= kTbMinEdge): T half sweeps — T/2 of the
+// stream from HBM (edge >= 256; opt-in through PPPM_MG_TB, since the plain
+// half sweeps on groups of 4 cells measured faster inside a whole solve):
+// T half sweeps — T/2 of the
 // reference's red-black iterations (MG/Multigrid.cu:202-239, odd cells first,
 // omega = 1.43f) — in one pass over the level, optionally fused with the
 // prolongation by injection that precedes the post-smoothing
