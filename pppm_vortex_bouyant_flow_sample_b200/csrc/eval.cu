@@ -41,6 +41,11 @@ namespace pppm {
 namespace {
 
 constexpr int kEvalThreads = 128;
+// Resident blocks per SM the evaluation kernels are compiled for: 9 (56
+// registers, a few bytes of spill outside the pair loop) measured 12.85 ms on
+// the 1M-ring headline against 13.05 ms with 8 (64 registers) and 13.77 ms
+// with 10 (48 registers).
+constexpr int kEvalBlocksPerSM = 9;
 
 __device__ __forceinline__ float3 rel_pos(float4 p, const DevParams *__restrict__ P) {
     return make_float3((float)((double)p.x - P->origin[0]), (float)((double)p.y - P->origin[1]),
@@ -678,7 +683,7 @@ __device__ __forceinline__ void eval_points(const SmoothSeries &sc, const EvalAr
 
 // One scene: block b evaluates points [128 b, 128 b + 128) of the order.
 template <bool SEG, bool COUNT, bool FOLD>
-__global__ void __launch_bounds__(kEvalThreads, 8) eval_kernel(const SmoothSeries sc, const EvalArgs ea) {
+__global__ void __launch_bounds__(kEvalThreads, kEvalBlocksPerSM) eval_kernel(const SmoothSeries sc, const EvalArgs ea) {
     __shared__ float4 stage[(kEvalThreads / 32) * kPackPlanes * kPackSlots];
     eval_points<SEG, COUNT, FOLD>(sc, ea, blockIdx.x, stage);
 }
@@ -689,7 +694,7 @@ __global__ void __launch_bounds__(kEvalThreads, 8) eval_kernel(const SmoothSerie
 // then hands out first (longest work first); each point's arithmetic is the
 // one-scene kernel's, so results do not depend on the batch.
 template <bool SEG, bool COUNT, bool FOLD>
-__global__ void __launch_bounds__(kEvalThreads, 8)
+__global__ void __launch_bounds__(kEvalThreads, kEvalBlocksPerSM)
 eval_batch_kernel(const SmoothSeries sc, const EvalArgs *__restrict__ scenes, const uint2 *__restrict__ work) {
     __shared__ float4 stage[(kEvalThreads / 32) * kPackPlanes * kPackSlots];
     __shared__ EvalArgs sa;  // the block's scene, read from shared memory where used
