@@ -28,6 +28,9 @@ __device__ __forceinline__ float warp_sum(float v) {
 __device__ __forceinline__ void run_sum(const float4 *__restrict__ vrec, const float4 *__restrict__ valf,
                                         uint32_t s, uint32_t e, uint32_t cell, int lane, float &ax, float &ay,
                                         float &az) {
+    // unrolled so that a dense cell's loads are in flight together (each
+    // lane's records are still added in order)
+#pragma unroll 4
     for (uint32_t p = s + lane; p < e; p += 32) {
         const float4 r = vrec[p];
         if (__float_as_uint(r.w) == cell) {
