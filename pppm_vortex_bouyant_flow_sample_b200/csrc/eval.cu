@@ -238,8 +238,11 @@ struct ExpForm {
 // branch on nearly every step.
 constexpr float kExpSmallT = 1.0f / 64.0f;
 
+// WIDX: the record's index into the sorted vortices goes to E's spare half
+// (the index test of segment evaluation).
+template <bool WIDX = false>
 __device__ __forceinline__ void stage_record(float *__restrict__ pk, int slot, int half, float4 r, float4 a,
-                                             float3 o) {
+                                             float3 o, uint32_t ridx = 0xFFFFFFFFu) {
     float *A = pk + 4 * (0 * kPackSlots + slot), *B = pk + 4 * (1 * kPackSlots + slot);
     float *Cc = pk + 4 * (2 * kPackSlots + slot), *D = pk + 4 * (3 * kPackSlots + slot);
     float *E = pk + 4 * (4 * kPackSlots + slot);
@@ -249,6 +252,7 @@ __device__ __forceinline__ void stage_record(float *__restrict__ pk, int slot, i
     Cc[half] = a.y; Cc[2 + half] = a.z;
     D[half] = fmaf(a.y, sz, -(a.z * sy)); D[2 + half] = fmaf(a.z, sx, -(a.x * sz));
     E[half] = fmaf(a.x, sy, -(a.y * sx));
+    if (WIDX) E[2 + half] = __uint_as_float(ridx);
 }
 
 // The pair loop over np slots of the ring from slot s0 (FULL: one whole block
@@ -256,17 +260,19 @@ __device__ __forceinline__ void stage_record(float *__restrict__ pk, int slot, i
 // lane takes the records two at a time from shared memory (broadcast reads)
 // and evaluates both pairs with packed f32x2 arithmetic.  cr_lane is the box
 // half-width, or -1 for an inactive lane.  The r = 0 exclusion needs no test:
-// the pair's (ra - r_p) is zero.  SEG keeps the other-end test.  phi is the
+// the pair's (ra - r_p) is zero.  SEG: the other-end test, 1 by position
+// (|rb - r_p|^2 < 1e-24), 2 by record index (the one vortex at rb, pstar, found
+// beforehand), 0 none.  phi is the
 // degree-DEG polynomial cf (DEG 4: the scene never leaves [0, 0.25]; DEG 7:
 // valid on [0, 2], the exp form above tbig when need_exp; DEG 0: the exp form,
 // the polynomial only for small t, looked for only when CHECK).  FOLD: the
 // coefficients carry the powers of 1/a^3, so the polynomial takes r^3
 // directly and tbig is in r^3 too.
-template <bool SEG, bool COUNT, bool FOLD, int DEG, bool FULL, bool CHECK>
+template <int SEG, bool COUNT, bool FOLD, int DEG, bool FULL, bool CHECK>
 __device__ __forceinline__ void pair_slots(const float4 *__restrict__ pk4, uint32_t s0, uint32_t np, float cr_lane,
-                                           const float3 ra, const float3 rb, float2 inv_a3, const float2 *cf,
-                                           float tbig, float inv4pia3, bool need_exp, PairAcc2 &acc,
-                                           const ExpForm &xf) {
+                                           const float3 ra, const float3 rb, uint32_t pstar, float2 inv_a3,
+                                           const float2 *cf, float tbig, float inv4pia3, bool need_exp,
+                                           PairAcc2 &acc, const ExpForm &xf) {
     const float2 tx = make_float2(ra.x, ra.x), ty = make_float2(ra.y, ra.y), tz = make_float2(ra.z, ra.z);
     const uint32_t cnt = FULL ? kBlockRecs / 2 : np;
 #pragma unroll (FULL ? kBlockRecs / 2 : 2)
@@ -284,7 +290,11 @@ __device__ __forceinline__ void pair_slots(const float4 *__restrict__ pk4, uint3
                                                                                     DEG == 0 ? 1e-30f : 0.f))));
         bool ok0 = m0 <= cr_lane, ok1 = m1 <= cr_lane;
         if (COUNT) acc.n += (ok0 ? 1ull : 0ull) + (ok1 ? 1ull : 0ull);
-        if (SEG) {
+        if (SEG == 2) {
+            ok0 = ok0 && __float_as_uint(E.z) != pstar;
+            ok1 = ok1 && __float_as_uint(E.w) != pstar;
+        }
+        if (SEG == 1) {
             const float2 ex = __fadd2_rn(make_float2(rb.x, rb.x), nx);
             const float2 ey = __fadd2_rn(make_float2(rb.y, rb.y), ny);
             const float2 ez = __fadd2_rn(make_float2(rb.z, rb.z), nz);
@@ -336,7 +346,7 @@ __device__ __forceinline__ void pair_slots(const float4 *__restrict__ pk4, uint3
         // the exp form's c is finite for every pair of an active lane (r = 0
         // lies inside the box and takes the polynomial), so the box mask can
         // multiply it; the polynomials can overflow on the padding record
-        const float2 coeff = (DEG == 0 && !SEG && !COUNT)
+        const float2 coeff = (DEG == 0 && SEG != 1 && !COUNT)
                                  ? __fmul2_rn(c, make_float2(ok0 ? 1.0f : 0.0f, ok1 ? 1.0f : 0.0f))
                                  : make_float2(ok0 ? c.x : 0.0f, ok1 ? c.y : 0.0f);
         acc.ax = __ffma2_rn(coeff, make_float2(B.z, B.w), acc.ax);
@@ -360,10 +370,11 @@ __device__ __forceinline__ void pair_slots(const float4 *__restrict__ pk4, uint3
 // other record skips the warp's test for it.  The records still waiting after
 // a block all come from the chunk just staged (fewer than 32 waited before
 // it), so that chunk's flag carries over.
-template <bool SEG, bool COUNT, bool FOLD, int DEG>
+template <int SEG, bool COUNT, bool FOLD, int DEG>
 __device__ __forceinline__ void stage_run(const float4 *__restrict__ vrec, const float4 *__restrict__ valf,
                                           uint32_t ps, uint32_t pe, float cr_lane, const float3 ra,
-                                          const float3 rb, float3 o, const float3 blo, const float3 bhi,
+                                          const float3 rb, uint32_t pstar, float3 o, const float3 blo,
+                                          const float3 bhi,
                                           float dnear, float2 inv_a3, const float2 *cf, float tbig,
                                           float inv4pia3, bool need_exp, float4 *__restrict__ pk4, int lane,
                                           Ring &ring, PairAcc2 &acc, const ExpForm &xf) {
@@ -389,7 +400,7 @@ __device__ __forceinline__ void stage_run(const float4 *__restrict__ vrec, const
         }
         if (keep) {
             const uint32_t dst = ring.fill + (uint32_t)__popc(kept & ((1u << lane) - 1u));
-            stage_record(pk, (int)((dst >> 1) & (kPackSlots - 1)), (int)(dst & 1u), r, al, o);
+            stage_record<SEG == 2>(pk, (int)((dst >> 1) & (kPackSlots - 1)), (int)(dst & 1u), r, al, o, base + lane);
         }
         ring.fill += (uint32_t)__popc(kept);
         ring.near = ring.near || near_chunk;
@@ -397,11 +408,11 @@ __device__ __forceinline__ void stage_run(const float4 *__restrict__ vrec, const
             __syncwarp();
             const uint32_t s0 = (ring.head >> 1) & (kPackSlots - 1);
             if (DEG != 0 || ring.near)
-                pair_slots<SEG, COUNT, FOLD, DEG, true, true>(pk4, s0, 0, cr_lane, ra, rb, inv_a3, cf, tbig,
+                pair_slots<SEG, COUNT, FOLD, DEG, true, true>(pk4, s0, 0, cr_lane, ra, rb, pstar, inv_a3, cf, tbig,
                                                               inv4pia3, need_exp, acc, xf);
             else
-                pair_slots<SEG, COUNT, FOLD, DEG, true, false>(pk4, s0, 0, cr_lane, ra, rb, inv_a3, cf, tbig,
-                                                               inv4pia3, need_exp, acc, xf);
+                pair_slots<SEG, COUNT, FOLD, DEG, true, false>(pk4, s0, 0, cr_lane, ra, rb, pstar, inv_a3, cf,
+                                                               tbig, inv4pia3, need_exp, acc, xf);
             ring.head += kBlockRecs;
             ring.near = near_chunk && ring.fill != ring.head;
             __syncwarp();  // the next records may take the slots just read
@@ -412,20 +423,21 @@ __device__ __forceinline__ void stage_run(const float4 *__restrict__ vrec, const
 // Evaluates the records left in the ring after the walk (fewer than 32); an
 // odd count is padded with a record at (-1e18, -1e18, -1e18) and zero
 // strength, outside every box.
-template <bool SEG, bool COUNT, bool FOLD, int DEG>
-__device__ __forceinline__ void finish_ring(float cr_lane, const float3 ra, const float3 rb, float2 inv_a3,
+template <int SEG, bool COUNT, bool FOLD, int DEG>
+__device__ __forceinline__ void finish_ring(float cr_lane, const float3 ra, const float3 rb, uint32_t pstar,
+                                            float2 inv_a3,
                                             const float2 *cf, float tbig, float inv4pia3, bool need_exp,
                                             float4 *__restrict__ pk4, int lane, const Ring &ring, PairAcc2 &acc,
                                             const ExpForm &xf) {
     const uint32_t rem = ring.fill - ring.head;
     if (rem == 0) return;
     if (lane == 0 && (rem & 1u))
-        stage_record(reinterpret_cast<float *>(pk4), (int)((ring.fill >> 1) & (kPackSlots - 1)), 1,
+        stage_record<SEG == 2>(reinterpret_cast<float *>(pk4), (int)((ring.fill >> 1) & (kPackSlots - 1)), 1,
                      make_float4(-1e18f, -1e18f, -1e18f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f),
                      make_float3(0.f, 0.f, 0.f));
     __syncwarp();
     pair_slots<SEG, COUNT, FOLD, DEG, false, true>(pk4, (ring.head >> 1) & (kPackSlots - 1), (rem + 1) >> 1, cr_lane,
-                                                   ra, rb, inv_a3, cf, tbig, inv4pia3, need_exp, acc, xf);
+                                                   ra, rb, pstar, inv_a3, cf, tbig, inv4pia3, need_exp, acc, xf);
     __syncwarp();
 }
 
@@ -585,8 +597,57 @@ __device__ __forceinline__ void eval_points(const SmoothSeries &sc, const EvalAr
         // exp form: records inside [blo + dnear, bhi - dnear] may lie within
         // a / 4 of a lane (1 % margin on a / 4, far above the trigger's)
         const float dnear = cr - (float)(0.2525 * P->a);
-        auto uniform_walk = [&](auto deg) {
+        // Segments: the pair test on the other end only ever drops a vortex
+        // that sits at this lane's other end (|rb - r_p|^2 < 1e-24).  Each lane
+        // looks for them among the records of the hash cells its other end can
+        // fall in (widened by the rounding bound prune_cells), with the pair
+        // loop's own arithmetic.  None: the walk needs no test.  Exactly one
+        // (the time step's segments: the other end is the segment's own
+        // centre): the pair loop drops that record by its index.  More, or an
+        // other end near or beyond the grid's faces (vortices hashed from
+        // outside wrap around): the position test.
+        int seg_mode = 0;
+        uint32_t pstar = 0xFFFFFFFFu;
+        if (SEG) {
+            int found = 0;
+            if (act) {
+                const double pr = P->prune_cells + 1e-6;
+                const double qb[3] = {(double)rb.x * invh, (double)rb.y * invh, (double)rb.z * invh};
+                int clo[3], chi[3];
+                bool edge = false;
+#pragma unroll
+                for (int a = 0; a < 3; a++) {
+                    // inside: floor(qb - pr) >= 0 and floor(qb + pr) <= n - 1
+                    edge = edge || !(qb[a] >= pr && qb[a] < (double)n - pr);
+                    clo[a] = (int)floor(qb[a] - pr);
+                    chi[a] = (int)floor(qb[a] + pr);
+                }
+                if (edge) {
+                    found = 2;
+                } else {
+                    for (int kk = clo[2]; kk <= chi[2] && found < 2; kk++)
+                        for (int jj = clo[1]; jj <= chi[1] && found < 2; jj++)
+                            for (int ii = clo[0]; ii <= chi[0] && found < 2; ii++) {
+                                const uint32_t cell = ((uint32_t)kk * n + (uint32_t)jj) * n + (uint32_t)ii;
+                                const uint32_t ps = start[cell];
+                                if (ps == kEmpty) continue;
+                                const uint32_t pe = end[cell];
+                                for (uint32_t p = ps; p < pe && found < 2; p++) {
+                                    const float4 r = vrec[p];
+                                    const float ex = rb.x + (-r.x), ey = rb.y + (-r.y), ez = rb.z + (-r.z);
+                                    if (fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < 1e-24f) {
+                                        found++;
+                                        pstar = p;
+                                    }
+                                }
+                            }
+                }
+            }
+            seg_mode = __any_sync(0xffffffffu, found >= 2) ? 1 : (__any_sync(0xffffffffu, found == 1) ? 2 : 0);
+        }
+        auto uniform_walk = [&](auto deg, auto segc) {
             constexpr int D = decltype(deg)::value;
+            constexpr int S = decltype(segc)::value;
             const float2 *cfd = D == 0 ? sc.p5 : (D == 7 ? sc.p7 : sc.p4);
             Ring ring;
             for (int k2 = ulo[2]; k2 <= uhi[2]; k2++)
@@ -608,17 +669,26 @@ __device__ __forceinline__ void eval_points(const SmoothSeries &sc, const EvalAr
                         }
                         i2 += both ? 2 : 1;
                         if (ps == kEmpty) continue;
-                        stage_run<SEG, COUNT, FOLD, D>(vrec, valf, ps, pe, cr_lane, ra, rb, o, blo, bhi, dnear,
-                                                       inv_a3_2, cfd, sc.t7, inv4pia3, D == 7 && need_exp2, pk, lane,
-                                                       ring, acc2, xf);
+                        stage_run<S, COUNT, FOLD, D>(vrec, valf, ps, pe, cr_lane, ra, rb, pstar, o, blo, bhi,
+                                                     dnear, inv_a3_2, cfd, sc.t7, inv4pia3, D == 7 && need_exp2, pk,
+                                                     lane, ring, acc2, xf);
                     }
-            finish_ring<SEG, COUNT, FOLD, D>(cr_lane, ra, rb, inv_a3_2, cfd, sc.t7, inv4pia3, D == 7 && need_exp2, pk,
-                                             lane, ring, acc2, xf);
+            finish_ring<S, COUNT, FOLD, D>(cr_lane, ra, rb, pstar, inv_a3_2, cfd, sc.t7, inv4pia3,
+                                           D == 7 && need_exp2, pk, lane, ring, acc2, xf);
+        };
+        auto walk = [&](auto deg) {
+            if constexpr (SEG) {
+                if (seg_mode == 1) uniform_walk(deg, std::integral_constant<int, 1>{});
+                else if (seg_mode == 2) uniform_walk(deg, std::integral_constant<int, 2>{});
+                else uniform_walk(deg, std::integral_constant<int, 0>{});
+            } else {
+                uniform_walk(deg, std::integral_constant<int, 0>{});
+            }
         };
         if (vol > 0 && vol <= kUniformMaxSub && P->prune_cells < 0.25) {
-            if (tier0) uniform_walk(std::integral_constant<int, 0>{});
-            else if (tier7) uniform_walk(std::integral_constant<int, 7>{});
-            else uniform_walk(std::integral_constant<int, 4>{});
+            if (tier0) walk(std::integral_constant<int, 0>{});
+            else if (tier7) walk(std::integral_constant<int, 7>{});
+            else walk(std::integral_constant<int, 4>{});
         } else if (act && lo[0] <= hi[0]) {
             // scattered warp (points outside the grid, sparse regions): own walk
             for (int kk = lo[2] >> 1; kk <= (hi[2] >> 1); kk++)
