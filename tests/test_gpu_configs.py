@@ -148,18 +148,26 @@ def test_exp_form_accuracy_pair_by_pair(pb, oracle):
     assert rel_l2(u, ref) <= VEL_TOL
 
 
-def test_segments_radius_one_cell(pb, oracle):
+@pytest.mark.parametrize("duplicates", [False, True])
+def test_segments_radius_one_cell(pb, oracle, duplicates):
     """Segment evaluation (is_segment = 1 with distinct other ends, the time
     step's form) at a radius of one cell: a pair counts only where both ends
-    are apart from the vortex, as in the oracle."""
+    are apart from the vortex, as in the oracle.  Some other ends sit on a
+    vortex (the kernel then drops that record by index), the rest on none (no
+    test needed); with duplicates, some sit on two vortices at one position
+    (the position test)."""
     import torch
     from pppm_vortex_bouyant_flow_sample_b200 import workloads as W
     pos, al = W.vortex_ring(60000, seed=12)
+    if duplicates:
+        pos[30000:30400] = pos[40000:40400]
     rng = np.random.default_rng(13)
     ea = np.ascontiguousarray(pos[::3])
     eb = ea.copy()
     eb[:, :3] += rng.normal(0, 0.01, (len(eb), 3)).astype(np.float32)
     eb[::7] = pos[1::21][: len(eb[::7])]   # some other ends on vortices
+    if duplicates:
+        eb[1::11][:400] = pos[40000:40400]  # other ends on two vortices each
     n = 64
     scene = pb.Scene(n, cap_vort=len(pos), cap_eval=len(ea), a_cells=1.0)
     try:
