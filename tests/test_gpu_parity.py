@@ -303,3 +303,34 @@ def test_full_scale_ring_subsample(pb, oracle):
     assert pairs == int(d["pairs"][0])
     assert rel_l2(u, ref) <= VEL_TOL
     scene.close()
+
+
+def test_solve_host_equals_the_device_path(pb, oracle):
+    """pppm_solve_host, the end-to-end entry point on (pinned) host buffers
+    (copies in, build, evaluation, copies out), gives bit for bit the device
+    path's velocities on the same inputs, both for the vortices themselves and
+    for separate points, and the oracle's within the velocity tolerance."""
+    import torch
+    from pppm_vortex_bouyant_flow_sample_b200 import workloads as W
+    pos, al = W.vortex_ring(20000, seed=61)
+    ev, _ = W.uniform_cloud(5000, seed=62)
+    n = 32
+    scene = pb.Scene(n, cap_vort=len(pos), cap_eval=len(pos), a_cells=1.0)
+    try:
+        dpos, dal = _dev(pos), _dev(al)
+        scene.set_vortices(dpos, dal)
+        scene.build_far_field()
+        u_self = scene.eval(dpos, dpos, 1).cpu().numpy()
+        u_pts = scene.eval(_dev(ev)).cpu().numpy()
+        a = scene.smoothing()
+        hpos = torch.from_numpy(np.ascontiguousarray(pos)).pin_memory()
+        hal = torch.from_numpy(np.ascontiguousarray(np.asarray(al).T)).pin_memory()
+        h_self = scene.solve_host(hpos, hal).numpy().T.copy()
+        hev = torch.from_numpy(np.ascontiguousarray(ev)).pin_memory()
+        h_pts = scene.solve_host(hpos, hal, hev, None, 0).numpy().T.copy()
+    finally:
+        scene.close()
+    assert np.array_equal(h_self, u_self)
+    assert np.array_equal(h_pts, u_pts)
+    ref = oracle.pppm(oracle.params(n, a=a), pos, al, pos, pos, 1)[0]
+    assert rel_l2(h_self, ref) <= VEL_TOL
